@@ -1,0 +1,234 @@
+/*
+ * vxl_sph.h — C ABI of the B200 (sm_100a) WCSPH fluid step.
+ *
+ * Drop-in for the fluid GPU tier of bfxh/RUST-WL. The reference's seam is the Rust
+ * trait `FluidStepper` (crates/vxl-phys-core/src/interop.rs:293-316), implemented by
+ * `GpuFluidStepper` (crates/vxl-phys-gpu/src/pipeline/stepper.rs:22-147) and
+ * registered with `World::set_fluid_stepper` (crates/vxl-phys/src/world_step/
+ * fluid_stepper.rs:46-58). A Rust shim implements that trait over these entry points.
+ *
+ * Conventions follow crates/vxl-phys-ffi/src/lib.rs:
+ *   - every struct that crosses the boundary starts with {u32 size; u32 version}
+ *     (BlockHeader, lib.rs:18-21), checked against VXL_SPH_ABI_VERSION (lib.rs:13);
+ *   - status codes extend FfiError (lib.rs:26-33): the first six values are identical;
+ *   - calls are batch-only (whole particle arrays, never one particle at a time);
+ *   - no C++ exception or CUDA error crosses the boundary: both become a status code
+ *     and a message readable through vxl_sph_last_error().
+ *
+ * Arrays of vectors are AoS float triples (x, y, z) — the reference's `Vec3` layout
+ * (#[repr(C)] { f32 x, y, z }, crates/vxl-phys-core/src/math.rs:8-14) — in the
+ * reference's particle index order: fluid prefix [0, n_fluid) then boundary suffix.
+ * Host pointers are borrowed for the duration of the call only.
+ *
+ * Threading: one handle must not be driven from two threads at once (the reference's
+ * FluidStepper is used through &mut self). Distinct handles are independent.
+ */
+#ifndef VXL_SPH_H
+#define VXL_SPH_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define VXL_SPH_ABI_VERSION 1u
+
+/* crates/vxl-phys-ffi/src/lib.rs:26-33 (FfiError); values 6.. are additions. */
+typedef enum vxl_status {
+  VXL_OK = 0,
+  VXL_NULL_POINTER = 1,
+  VXL_VERSION_MISMATCH = 2,
+  VXL_SIZE_MISMATCH = 3,
+  VXL_NOT_READY = 4,
+  VXL_PANIC_CAUGHT = 5,
+  VXL_INVALID_ARGUMENT = 6,
+  VXL_CUDA_ERROR = 7,
+  VXL_OUT_OF_MEMORY = 8,
+  VXL_DEVICE_FAULT_FLAG = 9 /* a kernel raised its error flag (see vxl_sph_last_error) */
+} vxl_status;
+
+/* crates/vxl-phys-ffi/src/lib.rs:18-21 (BlockHeader). */
+typedef struct vxl_block_header {
+  uint32_t size;
+  uint32_t version;
+} vxl_block_header;
+
+/* crates/vxl-phys-fluid/src/config.rs:6-68 (FluidConfig; field meaning and defaults
+ * identical). particle_mass is the fluid particle mass `FluidSystem::mass`
+ * (fluid_access.rs:27-42, see vxl_sph_lattice_mass); max_bins is the cell budget of
+ * crates/vxl-phys-core/src/grid.rs:20 (0 = 1<<21). */
+typedef struct vxl_sph_params {
+  vxl_block_header hdr;
+  float rest_density;
+  float smoothing_radius;
+  float xsph_viscosity;
+  uint32_t tensile_instability_suppression;
+  float sound_speed;
+  float gamma_tait;
+  uint32_t substeps;
+  uint32_t boundary_layers;
+  float gravity[3];
+  float max_speed_frac;
+  float artificial_viscosity;
+  float particle_mass;
+  uint32_t max_bins;
+} vxl_sph_params;
+
+/* Full particle set at creation: `FluidStepper::step`'s pos/vel/pmass
+ * (crates/vxl-phys-core/src/interop.rs:296-304), fluid prefix + boundary suffix. */
+typedef struct vxl_sph_desc {
+  vxl_block_header hdr;
+  vxl_sph_params params;
+  uint64_t n_fluid;
+  uint64_t n_boundary;
+  const float* pos_xyz;  /* 3 * (n_fluid + n_boundary) */
+  const float* vel_xyz;  /* 3 * (n_fluid + n_boundary) */
+  const float* pmass;    /* n_fluid + n_boundary; fluid entries must equal particle_mass */
+  int32_t device;        /* CUDA device ordinal */
+} vxl_sph_desc;
+
+/* One boundary segment (crates/vxl-phys-fluid/src/system.rs:41-42): body id, body
+ * origin (torque pivot), [start, end) in global particle index. */
+typedef struct vxl_sph_span {
+  uint32_t body;
+  float origin[3];
+  uint32_t start;
+  uint32_t end;
+} vxl_sph_span;
+
+/* Per-body reaction (crates/vxl-phys-fluid/src/fluid_access.rs:109-113):
+ * tick-averaged force and torque about the body origin. */
+typedef struct vxl_sph_reaction {
+  uint32_t body;
+  float force[3];
+  float torque[3];
+} vxl_sph_reaction;
+
+/* Grid description of the last substep (crates/vxl-phys-fluid/src/grid.rs:168-175,
+ * NeighborGrid): min corner, 1/bin, bin, dims, cell count. */
+typedef struct vxl_sph_grid_info {
+  vxl_block_header hdr;
+  float min[3];
+  float inv;
+  float bin;
+  uint32_t dims[3];
+  uint64_t total;
+} vxl_sph_grid_info;
+
+typedef struct vxl_sph_handle vxl_sph_handle;
+
+/* crates/vxl-phys-ffi/src/lib.rs:13 (ABI_VERSION). */
+uint32_t vxl_sph_abi_version(void);
+
+/* Thread-local message for the last non-OK status returned on this thread. */
+const char* vxl_sph_last_error(void);
+
+/* PhysGpuBackend::name / ::available (crates/vxl-phys-gpu/src/lib.rs:20-29):
+ * backend name, and 1 when a device with compute capability 10.x is present. */
+const char* vxl_sph_backend_name(void);
+int vxl_sph_backend_available(void);
+
+/* Lattice mass calibration m = rho0 / sum_lattice W
+ * (crates/vxl-phys-fluid/src/fluid_access.rs:27-42). Host-only arithmetic. */
+vxl_status vxl_sph_lattice_mass(const vxl_sph_params* params, float spacing, float* out_mass);
+
+/* Two-layer Akinci boundary lattice of a box (half extents) or sphere (radius) in body
+ * space (crates/vxl-phys-fluid/src/boundary.rs:67-88, box_faces :208-232,
+ * sphere_shell :237-258, volume_from_self_sum :95-129). shape: 0 = box, 1 = sphere.
+ * Writes min(count, cap) points (xyz) and the calibrated per-particle volume; *out_count
+ * receives the full count (call with cap = 0 to size the buffer). */
+vxl_status vxl_sph_boundary_lattice(uint32_t shape, const float half[3], float radius, float spacing,
+                                    float h, uint32_t layers, float* out_pts_xyz, uint64_t cap,
+                                    uint64_t* out_count, float* out_volume);
+
+/* Create a resident scene (the reference builds its `Packet` once from the full set,
+ * crates/vxl-phys-gpu/src/pipeline/stepper.rs:36-61). */
+vxl_status vxl_sph_create(const vxl_sph_desc* desc, vxl_sph_handle** out);
+vxl_status vxl_sph_destroy(vxl_sph_handle* h);
+
+/* Re-upload the boundary segment (positions/velocities of boundary particles
+ * [n_fluid, n_fluid + nb)), as GpuFluidStepper::step does each tick through
+ * upload_boundary_segment (crates/vxl-phys-gpu/src/pipeline/coupling.rs:20-50).
+ * A length mismatch is VXL_SIZE_MISMATCH, never truncation (coupling.rs:22-33). */
+vxl_status vxl_sph_upload_boundary(vxl_sph_handle* h, uint64_t n_fluid, const float* pos_xyz,
+                                   const float* vel_xyz, uint64_t nb);
+
+/* Advance one tick of `substeps` substeps (FluidSystem::step, crates/vxl-phys-fluid/
+ * src/fluid_step.rs:75-89) and return the tick-averaged per-span reactions
+ * (aggregate_reactions, fluid_boundary.rs:10-28). out_reactions may be NULL when
+ * nspans == 0. Synchronous: returns after the reactions are on the host. */
+vxl_status vxl_sph_step_tick(vxl_sph_handle* h, float dt_tick, const vxl_sph_span* spans,
+                             uint32_t nspans, vxl_sph_reaction* out_reactions);
+
+/* Enqueue one tick without waiting (the reference's run_deferred,
+ * crates/vxl-phys-gpu/src/pipeline.rs:607-609); vxl_sph_sync waits and, when
+ * out_reactions is given, copies the reactions of the last enqueued tick. */
+vxl_status vxl_sph_step_tick_async(vxl_sph_handle* h, float dt_tick, const vxl_sph_span* spans,
+                                   uint32_t nspans);
+vxl_status vxl_sph_sync(vxl_sph_handle* h, vxl_sph_reaction* out_reactions, uint32_t nspans);
+
+/* One substep only (FluidSystem::substep, fluid_step.rs:91-127): per-step parity. */
+vxl_status vxl_sph_substep(vxl_sph_handle* h, float dt);
+
+/* Tight AABB of the fluid particles (FluidStepper::bounds, interop.rs:306-309;
+ * the GPU tier reads it from the device, readback.rs:111-154). */
+vxl_status vxl_sph_bounds(vxl_sph_handle* h, float lo[3], float hi[3]);
+
+/* State in reference index order (Packet::read_state / snapshot / restore,
+ * crates/vxl-phys-gpu/src/pipeline.rs:768-776). Arrays are 3 * n_total floats;
+ * either pointer may be NULL. */
+vxl_status vxl_sph_read_state(vxl_sph_handle* h, float* pos_xyz, float* vel_xyz);
+vxl_status vxl_sph_write_state(vxl_sph_handle* h, const float* pos_xyz, const float* vel_xyz);
+
+/* Per-particle results of the last substep in reference index order (the
+ * reference's densities()/pressures()/accelerations()/boundary_forces() and xsph,
+ * fluid_access.rs:149-171). acc/xsph are recorded only while recording is on
+ * (vxl_sph_set_record); dens/press always. Any pointer may be NULL. */
+vxl_status vxl_sph_set_record(vxl_sph_handle* h, int on);
+vxl_status vxl_sph_read_fields(vxl_sph_handle* h, float* dens, float* press, float* acc_xyz,
+                               float* xsph_xyz, float* bforce_xyz);
+
+/* Neighbour table of the last substep (FluidSystem::neighbor_grid,
+ * crates/vxl-phys-fluid/src/fluid_access.rs:125-133): items[n_total] = particle
+ * index per cell-ordered slot, start[total+1], bins[n_total] = cell of each particle.
+ * start_cap is the capacity of start in entries. Any array may be NULL. */
+vxl_status vxl_sph_export_grid(vxl_sph_handle* h, uint32_t* items, uint32_t* start, uint64_t start_cap,
+                               uint32_t* bins, vxl_sph_grid_info* info);
+
+/* Counts for the caller's own accounting: particles, cells of the last substep,
+ * kernel launches of the last tick, bytes of device memory held. */
+typedef struct vxl_sph_stats {
+  vxl_block_header hdr;
+  uint64_t n_fluid;
+  uint64_t n_boundary;
+  uint64_t cells;
+  uint64_t launches_last_tick;
+  uint64_t device_bytes;
+  float last_tick_ms; /* device time of the last tick (CUDA events), 0 if unknown */
+} vxl_sph_stats;
+vxl_status vxl_sph_get_stats(vxl_sph_handle* h, vxl_sph_stats* out);
+
+/* Run the handle's work on a caller-owned CUDA stream (a cudaStream_t passed as
+ * void*; NULL returns to the handle's own stream). Lets a caller order the step with
+ * its own work and time it with events on that stream. */
+vxl_status vxl_sph_set_stream(vxl_sph_handle* h, void* cuda_stream);
+
+/* Per-kernel device timers, the device counterpart of the reference's phase
+ * accumulators (FluidSystem::phase_us, crates/vxl-phys-fluid/src/fluid_step.rs:
+ * 98-126, 129-138): with profiling on, every kernel launch of a tick is bracketed by
+ * CUDA events on the launching stream and the elapsed times are accumulated per kernel
+ * when the next tick starts or on vxl_sph_profile_read. Switching on resets the
+ * accumulators. */
+vxl_status vxl_sph_set_profile(vxl_sph_handle* h, int on);
+/* Kernel k of the accumulator table: name (static string), total device ms and
+ * launch count. Returns VXL_INVALID_ARGUMENT when k is past the last kernel. */
+vxl_status vxl_sph_profile_read(vxl_sph_handle* h, uint32_t k, const char** name, double* total_ms,
+                                uint64_t* launches);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* VXL_SPH_H */

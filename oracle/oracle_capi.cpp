@@ -1,0 +1,388 @@
+// C entry points over the WCSPH oracle — TEST INFRASTRUCTURE ONLY.
+//
+// tests/ (through ctypes), __graft_entry__.smoke() and bench.py's cpu_baseline leg load
+// this library as the checker. The shipped library never links it.
+//
+// Each handle holds an f32 restatement (bit-identical to the reference's Rust CPU path)
+// or its FP64 twin (same formulas and constants in double precision).
+#include <chrono>
+#include <cstring>
+#include <memory>
+#include <type_traits>
+
+#include "wcsph_oracle.hpp"
+
+using namespace oracle;
+
+extern "C" {
+
+struct orc_cfg {
+  float rest_density;
+  float smoothing_radius;
+  float xsph_viscosity;
+  uint32_t tensile_instability_suppression;
+  float sound_speed;
+  float gamma_tait;
+  uint32_t substeps;
+  uint32_t threads;
+  uint32_t boundary_layers;
+  float gravity[3];
+  float max_speed_frac;
+  float artificial_viscosity;
+  uint64_t max_bins;
+};
+
+struct orc_body {
+  uint32_t id;
+  uint32_t shape;   // 0 = box (half), 1 = sphere (radius)
+  float half[3];
+  float radius;
+  float pos[3];
+  float rot[4];     // x, y, z, w
+  float linvel[3];
+  float angvel[3];
+};
+
+struct orc_span {
+  uint32_t body;
+  float origin[3];
+  uint32_t start, end;
+};
+
+struct orc_reaction {
+  uint32_t body;
+  float force[3];
+  float torque[3];
+};
+}
+
+namespace {
+
+template <class R>
+FluidConfig<R> to_cfg(const orc_cfg* c) {
+  FluidConfig<R> f;
+  f.rest_density = (R)c->rest_density;
+  f.smoothing_radius = (R)c->smoothing_radius;
+  f.xsph_viscosity = (R)c->xsph_viscosity;
+  f.tensile_instability_suppression = c->tensile_instability_suppression != 0;
+  f.sound_speed = (R)c->sound_speed;
+  f.gamma_tait = (R)c->gamma_tait;
+  f.substeps = c->substeps;
+  f.threads = c->threads;
+  f.boundary_layers = c->boundary_layers;
+  f.gravity = V3<R>((R)c->gravity[0], (R)c->gravity[1], (R)c->gravity[2]);
+  f.max_speed_frac = (R)c->max_speed_frac;
+  f.artificial_viscosity = (R)c->artificial_viscosity;
+  f.max_bins = c->max_bins ? c->max_bins : GRID_MAX_BINS;
+  return f;
+}
+
+struct Handle {
+  std::unique_ptr<FluidSystem<float>> f;
+  std::unique_ptr<FluidSystem<double>> d;
+};
+
+template <class R, class Fn>
+void with(Handle* h, Fn&& fn) {
+  if (h->f) fn(*h->f);
+  else fn(*h->d);
+}
+
+template <class R>
+Body<R> to_body(const orc_body& b) {
+  Body<R> o;
+  o.id = b.id;
+  o.shape.kind = b.shape == 1 ? ShapeKind::Sphere : ShapeKind::Box;
+  o.shape.half = V3<R>(b.half[0], b.half[1], b.half[2]);
+  o.shape.radius = b.radius;
+  o.pose.pos = V3<R>(b.pos[0], b.pos[1], b.pos[2]);
+  o.pose.rot = Quat<R>(b.rot[0], b.rot[1], b.rot[2], b.rot[3]);
+  o.pose.linvel = V3<R>(b.linvel[0], b.linvel[1], b.linvel[2]);
+  o.pose.angvel = V3<R>(b.angvel[0], b.angvel[1], b.angvel[2]);
+  return o;
+}
+
+}  // namespace
+
+extern "C" {
+
+void* orc_create(const orc_cfg* cfg, const float origin[3], const uint64_t dims[3], float spacing,
+                 int fp64) {
+  auto* h = new Handle();
+  size_t d[3] = {(size_t)dims[0], (size_t)dims[1], (size_t)dims[2]};
+  if (fp64)
+    h->d.reset(new FluidSystem<double>(to_cfg<double>(cfg), V3<double>(origin[0], origin[1], origin[2]), d,
+                                       (double)spacing));
+  else
+    h->f.reset(new FluidSystem<float>(to_cfg<float>(cfg), V3<float>(origin[0], origin[1], origin[2]), d,
+                                      spacing));
+  return h;
+}
+
+void orc_destroy(void* p) { delete (Handle*)p; }
+
+uint64_t orc_n_total(void* p) {
+  uint64_t n = 0;
+  with<float>((Handle*)p, [&](auto& s) { n = s.n_total(); });
+  return n;
+}
+uint64_t orc_n_fluid(void* p) {
+  uint64_t n = 0;
+  with<float>((Handle*)p, [&](auto& s) { n = s.n_fluid; });
+  return n;
+}
+double orc_mass(void* p) {
+  double m = 0;
+  with<float>((Handle*)p, [&](auto& s) { m = (double)s.mass; });
+  return m;
+}
+void orc_set_threads(void* p, uint32_t t) {
+  with<float>((Handle*)p, [&](auto& s) { s.cfg.threads = t; });
+}
+
+// Lattice mass calibration without building a system (crates/vxl-phys-fluid/src/fluid_access.rs:27-42).
+float orc_lattice_mass(const orc_cfg* cfg, float spacing) {
+  return FluidSystem<float>::lattice_mass(to_cfg<float>(cfg), spacing);
+}
+
+// Overwrite positions/velocities of all n_total particles (harness-only: the reference
+// has no position setter; seeded jitter is applied through this after construction).
+int orc_set_state(void* p, const float* pos, const float* vel, uint64_t n) {
+  int rc = 0;
+  with<float>((Handle*)p, [&](auto& s) {
+    using R = std::decay_t<decltype(s.h)>;
+    if (n != s.n_total()) { rc = 3; return; }
+    for (size_t i = 0; i < n; ++i) {
+      if (pos) s.pos[i] = V3<R>(pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]);
+      if (vel) s.vel[i] = V3<R>(vel[3 * i], vel[3 * i + 1], vel[3 * i + 2]);
+    }
+  });
+  return rc;
+}
+
+// set_boundary_particles (crates/vxl-phys-fluid/src/fluid_step.rs:13-53); returns N_b.
+uint64_t orc_set_bodies(void* p, const orc_body* bodies, uint32_t n) {
+  uint64_t nb = 0;
+  with<float>((Handle*)p, [&](auto& s) {
+    using R = std::decay_t<decltype(s.h)>;
+    std::vector<Body<R>> v;
+    for (uint32_t i = 0; i < n; ++i) v.push_back(to_body<R>(bodies[i]));
+    nb = s.set_boundary_particles(v);
+  });
+  return nb;
+}
+
+// Replace the boundary suffix with explicit particles (the FluidStepper view: the
+// facade hands over pos/vel/pmass of the boundary segment plus the span table).
+int orc_set_boundary_raw(void* p, uint64_t nb, const float* pos, const float* vel, const float* pm,
+                         const orc_span* spans, uint32_t nspans) {
+  with<float>((Handle*)p, [&](auto& s) {
+    using R = std::decay_t<decltype(s.h)>;
+    s.truncate_to_fluid();
+    for (size_t k = 0; k < nb; ++k) {
+      s.pos.push_back(V3<R>(pos[3 * k], pos[3 * k + 1], pos[3 * k + 2]));
+      s.vel.push_back(V3<R>(vel[3 * k], vel[3 * k + 1], vel[3 * k + 2]));
+      s.pmass.push_back((R)pm[k]);
+      s.dens.push_back(R(0));
+      s.press.push_back(R(0));
+      s.acc.push_back(V3<R>());
+      s.xsph.push_back(V3<R>());
+    }
+    for (uint32_t q = 0; q < nspans; ++q)
+      s.spans.push_back(Span<R>{spans[q].body, V3<R>(spans[q].origin[0], spans[q].origin[1], spans[q].origin[2]),
+                                spans[q].start, spans[q].end});
+    s.bforce.resize(s.pos.size(), V3<R>());
+    s.breact.clear();
+  });
+  return 0;
+}
+
+void orc_step(void* p, float dt_tick) {
+  with<float>((Handle*)p, [&](auto& s) { s.step((decltype(s.h))dt_tick); });
+}
+void orc_substep(void* p, float dt) {
+  with<float>((Handle*)p, [&](auto& s) { s.substep((decltype(s.h))dt); });
+}
+
+// Timed ticks for the CPU baseline: returns wall seconds.
+double orc_run_ticks(void* p, float dt_tick, uint32_t ticks) {
+  auto t0 = std::chrono::steady_clock::now();
+  for (uint32_t t = 0; t < ticks; ++t) orc_step(p, dt_tick);
+  auto t1 = std::chrono::steady_clock::now();
+  return std::chrono::duration<double>(t1 - t0).count();
+}
+
+// Read any subset of the per-particle arrays (all n_total long; xyz arrays 3*n).
+// Values are converted to double so the FP64 twin loses nothing.
+void orc_read(void* p, double* pos, double* vel, double* dens, double* press, double* acc, double* xsph,
+              double* bforce, double* pmass) {
+  with<float>((Handle*)p, [&](auto& s) {
+    size_t n = s.n_total();
+    for (size_t i = 0; i < n; ++i) {
+      if (pos) { pos[3 * i] = s.pos[i].x; pos[3 * i + 1] = s.pos[i].y; pos[3 * i + 2] = s.pos[i].z; }
+      if (vel) { vel[3 * i] = s.vel[i].x; vel[3 * i + 1] = s.vel[i].y; vel[3 * i + 2] = s.vel[i].z; }
+      if (acc) { acc[3 * i] = s.acc[i].x; acc[3 * i + 1] = s.acc[i].y; acc[3 * i + 2] = s.acc[i].z; }
+      if (xsph) { xsph[3 * i] = s.xsph[i].x; xsph[3 * i + 1] = s.xsph[i].y; xsph[3 * i + 2] = s.xsph[i].z; }
+      if (bforce) { bforce[3 * i] = s.bforce[i].x; bforce[3 * i + 1] = s.bforce[i].y; bforce[3 * i + 2] = s.bforce[i].z; }
+      if (dens) dens[i] = s.dens[i];
+      if (press) press[i] = s.press[i];
+      if (pmass) pmass[i] = s.pmass[i];
+    }
+  });
+}
+
+// Same as orc_read for f32 handles, without conversion (bit patterns preserved).
+void orc_read_f32(void* p, float* pos, float* vel, float* dens, float* press, float* acc, float* xsph,
+                  float* bforce, float* pmass) {
+  auto* h = (Handle*)p;
+  if (!h->f) return;
+  auto& s = *h->f;
+  size_t n = s.n_total();
+  for (size_t i = 0; i < n; ++i) {
+    if (pos) std::memcpy(pos + 3 * i, &s.pos[i], 12);
+    if (vel) std::memcpy(vel + 3 * i, &s.vel[i], 12);
+    if (acc) std::memcpy(acc + 3 * i, &s.acc[i], 12);
+    if (xsph) std::memcpy(xsph + 3 * i, &s.xsph[i], 12);
+    if (bforce) std::memcpy(bforce + 3 * i, &s.bforce[i], 12);
+    if (dens) dens[i] = s.dens[i];
+    if (press) press[i] = s.press[i];
+    if (pmass) pmass[i] = s.pmass[i];
+  }
+}
+
+// Grid table of the last substep (the reference's neighbor_grid()). Returns the
+// number of cells; start must hold cells+1 entries, items n_total entries.
+uint64_t orc_grid(void* p, uint32_t* start, uint64_t start_cap, uint32_t* items, float* min3, float* inv_bin,
+                  uint32_t* dims3) {
+  auto* h = (Handle*)p;
+  if (!h->f) return 0;
+  auto& g = h->f->grid;
+  uint64_t total = (uint64_t)g.nx * g.ny * g.nz;
+  if (dims3) { dims3[0] = g.nx; dims3[1] = g.ny; dims3[2] = g.nz; }
+  if (min3) { min3[0] = g.min.x; min3[1] = g.min.y; min3[2] = g.min.z; }
+  if (inv_bin) { inv_bin[0] = g.inv; inv_bin[1] = g.bin; }
+  if (start && start_cap >= total + 1) std::memcpy(start, g.start.data(), (total + 1) * 4);
+  if (items) std::memcpy(items, g.items.data(), g.items.size() * 4);
+  return total;
+}
+
+uint32_t orc_reactions(void* p, orc_reaction* out, uint32_t cap) {
+  uint32_t n = 0;
+  with<float>((Handle*)p, [&](auto& s) {
+    n = (uint32_t)s.breact.size();
+    for (uint32_t k = 0; k < n && k < cap; ++k) {
+      out[k].body = s.breact[k].body;
+      out[k].force[0] = (float)s.breact[k].force.x;
+      out[k].force[1] = (float)s.breact[k].force.y;
+      out[k].force[2] = (float)s.breact[k].force.z;
+      out[k].torque[0] = (float)s.breact[k].torque.x;
+      out[k].torque[1] = (float)s.breact[k].torque.y;
+      out[k].torque[2] = (float)s.breact[k].torque.z;
+    }
+  });
+  return n;
+}
+
+// Run the aggregation alone on a given bforce suffix (the reference's C2 reaction
+// test drives aggregate_reactions directly: crates/vxl-phys-fluid/src/tests.rs:667-712).
+void orc_aggregate_with(void* p, const float* bforce_suffix, int clear) {
+  auto* h = (Handle*)p;
+  if (!h->f) return;
+  auto& s = *h->f;
+  if (clear) s.breact.clear();
+  for (size_t k = s.n_fluid; k < s.n_total(); ++k) {
+    size_t q = k - s.n_fluid;
+    s.bforce[k] = V3<float>(bforce_suffix[3 * q], bforce_suffix[3 * q + 1], bforce_suffix[3 * q + 2]);
+  }
+  s.aggregate_reactions();
+}
+void orc_scale_reactions(void* p, float inv) {
+  auto* h = (Handle*)p;
+  if (!h->f) return;
+  for (auto& e : h->f->breact) { e.force *= inv; e.torque *= inv; }
+}
+
+uint32_t orc_spans(void* p, orc_span* out, uint32_t cap) {
+  uint32_t n = 0;
+  with<float>((Handle*)p, [&](auto& s) {
+    n = (uint32_t)s.spans.size();
+    for (uint32_t k = 0; k < n && k < cap; ++k) {
+      out[k].body = s.spans[k].body;
+      out[k].origin[0] = (float)s.spans[k].origin.x;
+      out[k].origin[1] = (float)s.spans[k].origin.y;
+      out[k].origin[2] = (float)s.spans[k].origin.z;
+      out[k].start = s.spans[k].start;
+      out[k].end = s.spans[k].end;
+    }
+  });
+  return n;
+}
+
+// grid_box alone (crates/vxl-phys-core/src/grid.rs:34-50).
+void orc_grid_box(const float lo[3], const float hi[3], float h, uint64_t max_bins, float* min3, float* bin,
+                  uint32_t* dims3) {
+  GridBox<float> g = grid_box(V3<float>(lo[0], lo[1], lo[2]), V3<float>(hi[0], hi[1], hi[2]), h, max_bins);
+  min3[0] = g.min.x; min3[1] = g.min.y; min3[2] = g.min.z;
+  *bin = g.bin;
+  dims3[0] = g.dims[0]; dims3[1] = g.dims[1]; dims3[2] = g.dims[2];
+}
+
+// Grid rebuild alone over arbitrary positions (n points, xyz).
+uint64_t orc_rebuild_grid(const float* pos, uint64_t n, float h, uint64_t max_bins, uint32_t* start,
+                          uint64_t start_cap, uint32_t* items, uint32_t* dims3) {
+  std::vector<V3<float>> v(n);
+  for (size_t i = 0; i < n; ++i) v[i] = V3<float>(pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]);
+  UniformGrid<float> g;
+  g.rebuild(v, h, max_bins);
+  uint64_t total = (uint64_t)g.nx * g.ny * g.nz;
+  if (dims3) { dims3[0] = g.nx; dims3[1] = g.ny; dims3[2] = g.nz; }
+  if (start && start_cap >= total + 1) std::memcpy(start, g.start.data(), (total + 1) * 4);
+  if (items) std::memcpy(items, g.items.data(), n * 4);
+  return total;
+}
+
+// Boundary lattice of one shape (crates/vxl-phys-fluid/src/boundary.rs:67-88).
+// Returns the particle count; fills pts (3*cap floats) when cap suffices.
+uint64_t orc_lattice(uint32_t shape, const float half[3], float radius, float s, float h, uint32_t layers,
+                     float* pts, uint64_t cap, float* volume, uint64_t* n0) {
+  Shape<float> sh;
+  sh.kind = shape == 1 ? ShapeKind::Sphere : ShapeKind::Box;
+  sh.half = V3<float>(half[0], half[1], half[2]);
+  sh.radius = radius;
+  BoundaryLattice<float> l = lattice(sh, s, h, layers);
+  if (volume) *volume = l.volume;
+  if (n0) *n0 = l.n0;
+  if (pts && cap >= l.pts.size())
+    for (size_t i = 0; i < l.pts.size(); ++i) std::memcpy(pts + 3 * i, &l.pts[i], 12);
+  return l.pts.size();
+}
+
+// Self-sum used by the volume calibration (boundary.rs:104-129), for the
+// calibration-consistency test (boundary.rs:367-372).
+float orc_boundary_self_sum(const float* pts, uint64_t n, float h) {
+  std::vector<V3<float>> v(n);
+  for (size_t i = 0; i < n; ++i) v[i] = V3<float>(pts[3 * i], pts[3 * i + 1], pts[3 * i + 2]);
+  return boundary_self_sum(v, h);
+}
+
+// The reference grid probe scene (crates/vxl-phys-gpu/examples/gpu_grid_probe.rs:181-226):
+// n^3 lattice at spacing 0.05, origin (-n*s/2, 0.5, -n*s/2), default FluidConfig, no
+// providers; 5 ticks, snapshot, 1 more tick; FNV hash of the last substep's table.
+uint64_t orc_grid_probe_hash(uint64_t n, uint64_t max_bins, uint32_t threads) {
+  float spacing = 0.05f;
+  FluidConfig<float> cfg;
+  cfg.threads = threads;
+  cfg.max_bins = max_bins ? max_bins : GRID_MAX_BINS;
+  float nf = (float)n;
+  V3<float> origin(-nf * spacing * 0.5f, 0.5f, -nf * spacing * 0.5f);
+  size_t dims[3] = {(size_t)n, (size_t)n, (size_t)n};
+  FluidSystem<float> f(cfg, origin, dims, spacing);
+  for (int t = 0; t < 5; ++t) f.step(1.0f / 60.0f);
+  size_t np = f.n_fluid;
+  f.step(1.0f / 60.0f);
+  auto& g = f.grid;
+  size_t total = (size_t)g.nx * g.ny * g.nz;
+  return table_hash(g.start, g.items, total, np);
+}
+
+}  // extern "C"

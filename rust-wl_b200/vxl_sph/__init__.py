@@ -1,0 +1,444 @@
+"""Python binding of the B200 WCSPH C ABI (include/vxl_sph.h) through ctypes.
+
+This is the same thin binding a maintainer would add on the caller's side; the
+reference's own caller is Rust (a `FluidStepper` impl over the C ABI, see
+INTEGRATION.md). `GpuFluidStepper` and `PhysGpuBackend` mirror the reference's trait
+methods (crates/vxl-phys-core/src/interop.rs:293-316, crates/vxl-phys-gpu/src/lib.rs:20-29)
+so tests read like the reference's own.
+
+The library is built in-tree (rust-wl_b200/lib/libvxl_sph.so). There is no CPU
+fallback: if the library is missing or no sm_100 device is present, calls raise.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+import numpy as np
+
+PKG_DIR = Path(__file__).resolve().parent.parent
+LIB_PATH = PKG_DIR / "lib" / "libvxl_sph.so"
+ABI_VERSION = 1
+
+OK, NULL_POINTER, VERSION_MISMATCH, SIZE_MISMATCH, NOT_READY, PANIC_CAUGHT = range(6)
+INVALID_ARGUMENT, CUDA_ERROR, OUT_OF_MEMORY, DEVICE_FAULT_FLAG = range(6, 10)
+STATUS_NAMES = {
+    0: "Ok", 1: "NullPointer", 2: "VersionMismatch", 3: "SizeMismatch", 4: "NotReady",
+    5: "PanicCaught", 6: "InvalidArgument", 7: "CudaError", 8: "OutOfMemory", 9: "DeviceFaultFlag",
+}
+
+
+class VxlError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {msg}")
+        self.status = status
+
+
+class BlockHeader(C.Structure):
+    _fields_ = [("size", C.c_uint32), ("version", C.c_uint32)]
+
+
+class Params(C.Structure):
+    _fields_ = [
+        ("hdr", BlockHeader),
+        ("rest_density", C.c_float),
+        ("smoothing_radius", C.c_float),
+        ("xsph_viscosity", C.c_float),
+        ("tensile_instability_suppression", C.c_uint32),
+        ("sound_speed", C.c_float),
+        ("gamma_tait", C.c_float),
+        ("substeps", C.c_uint32),
+        ("boundary_layers", C.c_uint32),
+        ("gravity", C.c_float * 3),
+        ("max_speed_frac", C.c_float),
+        ("artificial_viscosity", C.c_float),
+        ("particle_mass", C.c_float),
+        ("max_bins", C.c_uint32),
+    ]
+
+
+class Desc(C.Structure):
+    _fields_ = [
+        ("hdr", BlockHeader),
+        ("params", Params),
+        ("n_fluid", C.c_uint64),
+        ("n_boundary", C.c_uint64),
+        ("pos_xyz", C.POINTER(C.c_float)),
+        ("vel_xyz", C.POINTER(C.c_float)),
+        ("pmass", C.POINTER(C.c_float)),
+        ("device", C.c_int32),
+    ]
+
+
+class Span(C.Structure):
+    _fields_ = [("body", C.c_uint32), ("origin", C.c_float * 3), ("start", C.c_uint32), ("end", C.c_uint32)]
+
+
+class Reaction(C.Structure):
+    _fields_ = [("body", C.c_uint32), ("force", C.c_float * 3), ("torque", C.c_float * 3)]
+
+
+class GridInfo(C.Structure):
+    _fields_ = [
+        ("hdr", BlockHeader),
+        ("min", C.c_float * 3),
+        ("inv", C.c_float),
+        ("bin", C.c_float),
+        ("dims", C.c_uint32 * 3),
+        ("total", C.c_uint64),
+    ]
+
+
+class Stats(C.Structure):
+    _fields_ = [
+        ("hdr", BlockHeader),
+        ("n_fluid", C.c_uint64),
+        ("n_boundary", C.c_uint64),
+        ("cells", C.c_uint64),
+        ("launches_last_tick", C.c_uint64),
+        ("device_bytes", C.c_uint64),
+        ("last_tick_ms", C.c_float),
+    ]
+
+
+def header(struct_type) -> BlockHeader:
+    return BlockHeader(C.sizeof(struct_type), ABI_VERSION)
+
+
+# Every symbol include/vxl_sph.h declares, with its ctypes signature.
+_FP = C.POINTER(C.c_float)
+_U32P = C.POINTER(C.c_uint32)
+_H = C.c_void_p
+SIGNATURES = {
+    "vxl_sph_abi_version": (C.c_uint32, []),
+    "vxl_sph_last_error": (C.c_char_p, []),
+    "vxl_sph_backend_name": (C.c_char_p, []),
+    "vxl_sph_backend_available": (C.c_int, []),
+    "vxl_sph_lattice_mass": (C.c_int, [C.POINTER(Params), C.c_float, _FP]),
+    "vxl_sph_boundary_lattice": (C.c_int, [C.c_uint32, _FP, C.c_float, C.c_float, C.c_float, C.c_uint32, _FP,
+                                           C.c_uint64, C.POINTER(C.c_uint64), _FP]),
+    "vxl_sph_create": (C.c_int, [C.POINTER(Desc), C.POINTER(_H)]),
+    "vxl_sph_destroy": (C.c_int, [_H]),
+    "vxl_sph_upload_boundary": (C.c_int, [_H, C.c_uint64, _FP, _FP, C.c_uint64]),
+    "vxl_sph_step_tick": (C.c_int, [_H, C.c_float, C.POINTER(Span), C.c_uint32, C.POINTER(Reaction)]),
+    "vxl_sph_step_tick_async": (C.c_int, [_H, C.c_float, C.POINTER(Span), C.c_uint32]),
+    "vxl_sph_sync": (C.c_int, [_H, C.POINTER(Reaction), C.c_uint32]),
+    "vxl_sph_substep": (C.c_int, [_H, C.c_float]),
+    "vxl_sph_bounds": (C.c_int, [_H, _FP, _FP]),
+    "vxl_sph_read_state": (C.c_int, [_H, _FP, _FP]),
+    "vxl_sph_write_state": (C.c_int, [_H, _FP, _FP]),
+    "vxl_sph_set_record": (C.c_int, [_H, C.c_int]),
+    "vxl_sph_read_fields": (C.c_int, [_H, _FP, _FP, _FP, _FP, _FP]),
+    "vxl_sph_export_grid": (C.c_int, [_H, _U32P, _U32P, C.c_uint64, _U32P, C.POINTER(GridInfo)]),
+    "vxl_sph_get_stats": (C.c_int, [_H, C.POINTER(Stats)]),
+    "vxl_sph_set_stream": (C.c_int, [_H, C.c_void_p]),
+    "vxl_sph_set_profile": (C.c_int, [_H, C.c_int]),
+    "vxl_sph_profile_read": (C.c_int, [_H, C.c_uint32, C.POINTER(C.c_char_p), C.POINTER(C.c_double),
+                                       C.POINTER(C.c_uint64)]),
+}
+
+_lib = None
+
+
+def load(path: str | os.PathLike | None = None) -> C.CDLL:
+    """Load the in-tree library (raises if it is missing: there is no fallback)."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = Path(path) if path else LIB_PATH
+    if not p.exists():
+        raise FileNotFoundError(f"{p} not built (run rust-wl_b200/build.py)")
+    lib = C.CDLL(str(p))
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    if lib.vxl_sph_abi_version() != ABI_VERSION:
+        raise VxlError(VERSION_MISMATCH, "library ABI version differs from the binding")
+    if path is None:
+        _lib = lib
+    return lib
+
+
+def _check(status: int) -> None:
+    if status != OK:
+        msg = load().vxl_sph_last_error()
+        raise VxlError(status, msg.decode() if msg else "")
+
+
+def _fptr(a: np.ndarray | None):
+    if a is None:
+        return None
+    assert a.dtype == np.float32 and a.flags.c_contiguous
+    return a.ctypes.data_as(_FP)
+
+
+def _u32ptr(a: np.ndarray | None):
+    if a is None:
+        return None
+    assert a.dtype == np.uint32 and a.flags.c_contiguous
+    return a.ctypes.data_as(_U32P)
+
+
+def make_params(*, rest_density=1000.0, smoothing_radius=0.1, xsph_viscosity=0.1, tensile_instability_suppression=True,
+                sound_speed=10.0, gamma_tait=7.0, substeps=4, boundary_layers=2, gravity=(0.0, -9.81, 0.0),
+                max_speed_frac=0.4, artificial_viscosity=1.0, particle_mass=0.0, max_bins=0) -> Params:
+    """Params with the reference's FluidConfig defaults (crates/vxl-phys-fluid/src/config.rs:47-68)."""
+    p = Params()
+    p.hdr = header(Params)
+    p.rest_density = rest_density
+    p.smoothing_radius = smoothing_radius
+    p.xsph_viscosity = xsph_viscosity
+    p.tensile_instability_suppression = 1 if tensile_instability_suppression else 0
+    p.sound_speed = sound_speed
+    p.gamma_tait = gamma_tait
+    p.substeps = substeps
+    p.boundary_layers = boundary_layers
+    for a in range(3):
+        p.gravity[a] = gravity[a]
+    p.max_speed_frac = max_speed_frac
+    p.artificial_viscosity = artificial_viscosity
+    p.particle_mass = particle_mass
+    p.max_bins = max_bins
+    return p
+
+
+def lattice_mass(params: Params, spacing: float) -> float:
+    out = C.c_float()
+    _check(load().vxl_sph_lattice_mass(C.byref(params), spacing, C.byref(out)))
+    return out.value
+
+
+def boundary_lattice(shape: int, half=(0.0, 0.0, 0.0), radius: float = 0.0, spacing: float = 0.05, h: float = 0.1,
+                     layers: int = 2) -> tuple[np.ndarray, float]:
+    """Body-space Akinci lattice (N, 3) float32 and per-particle volume."""
+    lib = load()
+    hv = np.asarray(half, dtype=np.float32)
+    n = C.c_uint64()
+    vol = C.c_float()
+    _check(lib.vxl_sph_boundary_lattice(shape, _fptr(hv), radius, spacing, h, layers, None, 0, C.byref(n), None))
+    pts = np.zeros((n.value, 3), dtype=np.float32)
+    _check(lib.vxl_sph_boundary_lattice(shape, _fptr(hv), radius, spacing, h, layers, _fptr(pts), n.value,
+                                        C.byref(n), C.byref(vol)))
+    return pts, vol.value
+
+
+def spans_array(spans) -> tuple:
+    arr = (Span * max(len(spans), 1))()
+    for q, (body, origin, start, end) in enumerate(spans):
+        arr[q].body = body
+        for a in range(3):
+            arr[q].origin[a] = origin[a]
+        arr[q].start = start
+        arr[q].end = end
+    return arr, len(spans)
+
+
+class Scene:
+    """A resident scene on one GPU (handle of the C ABI)."""
+
+    def __init__(self, params: Params, pos: np.ndarray, vel: np.ndarray, pmass: np.ndarray, n_fluid: int,
+                 device: int = 0):
+        lib = load()
+        pos = np.ascontiguousarray(pos, dtype=np.float32).reshape(-1, 3)
+        vel = np.ascontiguousarray(vel, dtype=np.float32).reshape(-1, 3)
+        pmass = np.ascontiguousarray(pmass, dtype=np.float32).reshape(-1)
+        n = pos.shape[0]
+        if params.particle_mass == 0.0 and n_fluid > 0:
+            params.particle_mass = float(pmass[0])
+        d = Desc()
+        d.hdr = header(Desc)
+        d.params = params
+        d.n_fluid = n_fluid
+        d.n_boundary = n - n_fluid
+        d.pos_xyz = _fptr(pos)
+        d.vel_xyz = _fptr(vel)
+        d.pmass = _fptr(pmass)
+        d.device = device
+        h = C.c_void_p()
+        _check(lib.vxl_sph_create(C.byref(d), C.byref(h)))
+        self._h = h
+        self.lib = lib
+        self.n_fluid = n_fluid
+        self.n_total = n
+        self.n_boundary = n - n_fluid
+        self.params = params
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            _check(self.lib.vxl_sph_destroy(self._h))
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def step_tick(self, dt_tick: float, spans=()) -> list[tuple[int, np.ndarray, np.ndarray]]:
+        arr, ns = spans_array(spans)
+        out = (Reaction * max(ns, 1))()
+        _check(self.lib.vxl_sph_step_tick(self._h, dt_tick, arr, ns, out))
+        return [(out[q].body, np.array(out[q].force[:], np.float32), np.array(out[q].torque[:], np.float32))
+                for q in range(ns)]
+
+    def step_tick_async(self, dt_tick: float, spans=()) -> None:
+        arr, ns = spans_array(spans)
+        self._async_spans = ns
+        _check(self.lib.vxl_sph_step_tick_async(self._h, dt_tick, arr, ns))
+
+    def sync(self):
+        ns = getattr(self, "_async_spans", 0)
+        out = (Reaction * max(ns, 1))()
+        _check(self.lib.vxl_sph_sync(self._h, out, ns))
+        return [(out[q].body, np.array(out[q].force[:], np.float32), np.array(out[q].torque[:], np.float32))
+                for q in range(ns)]
+
+    def substep(self, dt: float) -> None:
+        _check(self.lib.vxl_sph_substep(self._h, dt))
+
+    def upload_boundary(self, pos: np.ndarray, vel: np.ndarray) -> None:
+        pos = np.ascontiguousarray(pos, dtype=np.float32).reshape(-1, 3)
+        vel = np.ascontiguousarray(vel, dtype=np.float32).reshape(-1, 3)
+        _check(self.lib.vxl_sph_upload_boundary(self._h, self.n_fluid, _fptr(pos), _fptr(vel), pos.shape[0]))
+
+    def read_state(self, out=None) -> tuple[np.ndarray, np.ndarray]:
+        """Positions and velocities in reference order; `out=(pos, vel)` reuses caller
+        buffers (e.g. pinned host memory)."""
+        if out is None:
+            p = np.empty((self.n_total, 3), np.float32)
+            v = np.empty((self.n_total, 3), np.float32)
+        else:
+            p, v = out
+        _check(self.lib.vxl_sph_read_state(self._h, _fptr(p), _fptr(v)))
+        return p, v
+
+    def write_state(self, pos: np.ndarray | None, vel: np.ndarray | None) -> None:
+        pp = None if pos is None else np.ascontiguousarray(pos, dtype=np.float32).reshape(-1, 3)
+        vv = None if vel is None else np.ascontiguousarray(vel, dtype=np.float32).reshape(-1, 3)
+        _check(self.lib.vxl_sph_write_state(self._h, _fptr(pp), _fptr(vv)))
+
+    def set_record(self, on: bool) -> None:
+        _check(self.lib.vxl_sph_set_record(self._h, 1 if on else 0))
+
+    def read_fields(self, acc: bool = True):
+        n = self.n_total
+        dens = np.empty(n, np.float32)
+        press = np.empty(n, np.float32)
+        a = np.empty((n, 3), np.float32) if acc else None
+        x = np.empty((n, 3), np.float32) if acc else None
+        bf = np.empty((max(self.n_boundary, 0), 3), np.float32)
+        _check(self.lib.vxl_sph_read_fields(self._h, _fptr(dens), _fptr(press), _fptr(a), _fptr(x),
+                                            _fptr(bf) if self.n_boundary else None))
+        return dens, press, a, x, bf
+
+    def export_grid(self):
+        info = GridInfo()
+        info.hdr = header(GridInfo)
+        _check(self.lib.vxl_sph_export_grid(self._h, None, None, 0, None, C.byref(info)))
+        total = info.total
+        items = np.empty(self.n_total, np.uint32)
+        start = np.empty(total + 1, np.uint32)
+        bins = np.empty(self.n_total, np.uint32)
+        _check(self.lib.vxl_sph_export_grid(self._h, _u32ptr(items), _u32ptr(start), total + 1, _u32ptr(bins),
+                                            C.byref(info)))
+        return items, start, bins, info
+
+    def bounds(self):
+        lo = np.empty(3, np.float32)
+        hi = np.empty(3, np.float32)
+        _check(self.lib.vxl_sph_bounds(self._h, _fptr(lo), _fptr(hi)))
+        return lo, hi
+
+    def set_stream(self, stream_handle: int | None) -> None:
+        """Enqueue on a caller-owned cudaStream_t (e.g. torch.cuda.Stream().cuda_stream)."""
+        _check(self.lib.vxl_sph_set_stream(self._h, C.c_void_p(stream_handle or 0)))
+
+    def set_profile(self, on: bool) -> None:
+        _check(self.lib.vxl_sph_set_profile(self._h, 1 if on else 0))
+
+    def profile(self) -> dict:
+        """{kernel name: (total device ms, launches)} since profiling was switched on."""
+        out = {}
+        k = 0
+        while True:
+            name = C.c_char_p()
+            ms = C.c_double()
+            n = C.c_uint64()
+            st = self.lib.vxl_sph_profile_read(self._h, k, C.byref(name), C.byref(ms), C.byref(n))
+            if st == INVALID_ARGUMENT:
+                break
+            _check(st)
+            out[name.value.decode()] = (ms.value, n.value)
+            k += 1
+        return out
+
+    def stats(self) -> Stats:
+        s = Stats()
+        s.hdr = header(Stats)
+        _check(self.lib.vxl_sph_get_stats(self._h, C.byref(s)))
+        return s
+
+
+class PhysGpuBackend:
+    """Mirror of `PhysGpuBackend` (crates/vxl-phys-gpu/src/lib.rs:20-29)."""
+
+    def name(self) -> str:
+        return load().vxl_sph_backend_name().decode()
+
+    def available(self) -> bool:
+        return bool(load().vxl_sph_backend_available())
+
+    def submit(self, tag: str) -> bool:
+        # The reference's fluid path never calls submit (SURVEY: marker trait); the
+        # fluid entry points are the stepper's.
+        return False
+
+
+class GpuFluidStepper:
+    """Mirror of `FluidStepper` as implemented by GpuFluidStepper
+    (crates/vxl-phys-gpu/src/pipeline/stepper.rs:69-147) over the C ABI.
+
+    Built once from the full particle set; each `step` re-uploads the boundary segment
+    (length mismatches raise, stepper.rs:84-96), advances one tick on the device and
+    keeps the tick-averaged reactions.
+    """
+
+    def __init__(self, params: Params, n_fluid: int, pos, vel, pmass, device: int = 0):
+        self.scene = Scene(params, pos, vel, pmass, n_fluid, device)
+        self.n_fluid = n_fluid
+        self.nb = self.scene.n_boundary
+        self._reactions: list = []
+
+    def step(self, dt_tick: float, n_fluid: int, pos, vel, pmass, spans) -> None:
+        pos = np.asarray(pos, np.float32).reshape(-1, 3)
+        vel = np.asarray(vel, np.float32).reshape(-1, 3)
+        if n_fluid != self.n_fluid:
+            raise VxlError(SIZE_MISMATCH, f"fluid prefix {n_fluid} != {self.n_fluid}")
+        if pos.shape[0] != n_fluid + self.nb:
+            raise VxlError(SIZE_MISMATCH, f"particle count {pos.shape[0]} != {n_fluid}+{self.nb}")
+        if len(pmass) != pos.shape[0]:
+            raise VxlError(SIZE_MISMATCH, "pmass length differs from the particle count")
+        if self.nb:
+            self.scene.upload_boundary(pos[n_fluid:], vel[n_fluid:])
+        self._reactions = self.scene.step_tick(dt_tick, spans)
+
+    def reactions(self):
+        return self._reactions
+
+    def bounds(self):
+        try:
+            return self.scene.bounds()
+        except VxlError:
+            return None
+
+    def gather_walls(self, h: float, providers) -> None:
+        # Provider walls are not part of this path (the configs use Akinci walls).
+        return None

@@ -1,0 +1,206 @@
+"""Seeded synthetic WCSPH scenes (dam breaks in Akinci-walled tanks).
+
+The reference has no stored scenes; its benchmarks build lattice blocks on the fly
+(crates/vxl-phys-fluid/examples/sph_scale.rs:27-36) and tanks of static boxes
+(crates/vxl-phys-gpu/examples/gpu_tick_probe.rs:20-63). These builders make the same
+kinds of scenes at the workload sizes this library is measured on:
+
+  dam0   16,384 fluid particles (16 x 32 x 32) at s = 0.02 in a 1.0 x 0.64 x 0.64 m tank
+  dam1   1,000,000 (100^3) at s = 0.01 in a 2 x 2 x 1 m tank (fill 25% by volume)
+  dam10m 9,938,375 (215^3) at s = 0.005 in a 2.5 x 1.2 x 1.2 m tank + 64 boxes
+
+Kernel constants for all: h = 2 s, rho0 = 1000, gamma = 7, c0 = 20 m/s, alpha = 0.05,
+eps = 0.5, g = -9.81, 10 substeps per 60 Hz tick, one Akinci layer on every wall box
+(wall thickness 2 s). Positions are the reference lattice (origin + (i + 1/2) s, i outer,
+k inner; crates/vxl-phys-fluid/src/fluid_access.rs:14-26) plus uniform jitter of +-1%
+of the spacing from numpy's PCG64 with the scene seed; the particle mass is calibrated
+on the unjittered lattice (fluid_access.rs:27-42).
+
+All arithmetic that produces particle data is float32, in the reference's order, so
+the oracle fed the same arrays sees the same inputs bit for bit.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import Params, boundary_lattice, lattice_mass, make_params
+
+F = np.float32
+
+
+@dataclass
+class SceneSpec:
+    name: str
+    params: Params
+    pos: np.ndarray      # (N_t, 3) float32, fluid prefix then boundary suffix
+    vel: np.ndarray      # (N_t, 3) float32
+    pmass: np.ndarray    # (N_t,) float32
+    n_fluid: int
+    spans: list          # [(body, origin(3), start, end)]
+    spacing: float
+    ticks: int
+    meta: dict = field(default_factory=dict)
+
+    @property
+    def n_total(self) -> int:
+        return int(self.pos.shape[0])
+
+    @property
+    def n_boundary(self) -> int:
+        return self.n_total - self.n_fluid
+
+
+def fluid_block(origin, dims, spacing) -> np.ndarray:
+    """n0 x n1 x n2 lattice at origin + (i + 1/2) s, reference order (fluid_access.rs:16-26)."""
+    s = F(spacing)
+    i, j, k = np.meshgrid(np.arange(dims[0]), np.arange(dims[1]), np.arange(dims[2]), indexing="ij")
+    out = np.empty((i.size, 3), F)
+    for a, g in enumerate((i, j, k)):
+        out[:, a] = F(origin[a]) + (g.reshape(-1).astype(F) + F(0.5)) * s
+    return out
+
+
+def jitter(pos: np.ndarray, spacing: float, seed: int, frac: float = 0.01) -> np.ndarray:
+    rng = np.random.Generator(np.random.PCG64(seed))
+    amp = F(frac) * F(spacing)
+    return (pos + rng.uniform(-1.0, 1.0, size=pos.shape).astype(F) * amp).astype(F)
+
+
+def _cross(a: np.ndarray, b: np.ndarray) -> np.ndarray:
+    # crates/vxl-phys-core/src/math.rs (Vec3::cross), float32 elementwise
+    return np.stack([a[..., 1] * b[..., 2] - a[..., 2] * b[..., 1],
+                     a[..., 2] * b[..., 0] - a[..., 0] * b[..., 2],
+                     a[..., 0] * b[..., 1] - a[..., 1] * b[..., 0]], axis=-1).astype(F)
+
+
+def rotate(q, v: np.ndarray) -> np.ndarray:
+    """Quat::rotate_vec3: t = 2 (q x v); v + q x t + w t (float32)."""
+    qv = np.broadcast_to(np.asarray(q[:3], F), v.shape)
+    t = (_cross(qv, v) * F(2.0)).astype(F)
+    return ((v + _cross(qv, t)) + t * F(q[3])).astype(F)
+
+
+@dataclass
+class Body:
+    id: int
+    half: tuple
+    pos: tuple
+    rot: tuple = (0.0, 0.0, 0.0, 1.0)
+    linvel: tuple = (0.0, 0.0, 0.0)
+    angvel: tuple = (0.0, 0.0, 0.0)
+
+
+def body_particles(bodies, spacing: float, h: float, layers: int, rest_density: float, cache=None):
+    """set_boundary_particles (crates/vxl-phys-fluid/src/fluid_step.rs:13-53) on the host:
+    per-shape lattice (cached), world transform, surface velocity v + w x r, pmass = rho0 V_b,
+    body-major layout; returns (pos, vel, pmass, spans relative to the boundary start)."""
+    cache = {} if cache is None else cache
+    ps, vs, ms, spans = [], [], [], []
+    n = 0
+    for b in bodies:
+        key = tuple(np.asarray(b.half, F).tolist())
+        if key not in cache:
+            cache[key] = boundary_lattice(0, key, 0.0, spacing, h, layers)
+        lat, vol = cache[key]
+        if lat.shape[0] == 0:
+            continue
+        bp = np.asarray(b.pos, F)
+        wp = (bp + rotate(b.rot, lat)).astype(F)
+        r = (wp - bp).astype(F)
+        wv = (np.asarray(b.linvel, F) + _cross(np.broadcast_to(np.asarray(b.angvel, F), r.shape), r)).astype(F)
+        ps.append(wp)
+        vs.append(wv)
+        ms.append(np.full(wp.shape[0], F(rest_density) * F(vol), F))
+        spans.append((b.id, tuple(float(x) for x in bp), n, n + wp.shape[0]))
+        n += wp.shape[0]
+    if not ps:
+        return np.zeros((0, 3), F), np.zeros((0, 3), F), np.zeros(0, F), []
+    return np.concatenate(ps), np.concatenate(vs), np.concatenate(ms), spans
+
+
+def tank_bodies(inner, t: float, first_id: int = 0) -> list:
+    """Floor + four walls (static boxes) around the open box [0, inner]; thickness t
+    (the reference's --tank pattern, gpu_tick_probe.rs:20-63, with the tank's own size)."""
+    lx, ly, lz = (F(x) for x in inner)
+    t = F(t)
+    th = t * F(0.5)
+    return [
+        Body(first_id + 0, (lx * F(0.5) + t, th, lz * F(0.5) + t), (lx * F(0.5), -th, lz * F(0.5))),
+        Body(first_id + 1, (th, ly * F(0.5), lz * F(0.5) + t), (-th, ly * F(0.5), lz * F(0.5))),
+        Body(first_id + 2, (th, ly * F(0.5), lz * F(0.5) + t), (lx + th, ly * F(0.5), lz * F(0.5))),
+        Body(first_id + 3, (lx * F(0.5) + t, ly * F(0.5), th), (lx * F(0.5), ly * F(0.5), -th)),
+        Body(first_id + 4, (lx * F(0.5) + t, ly * F(0.5), th), (lx * F(0.5), ly * F(0.5), lz + th)),
+    ]
+
+
+def baseline_params(spacing: float, substeps: int = 10, layers: int = 1, **over) -> Params:
+    kw = dict(rest_density=1000.0, smoothing_radius=2.0 * spacing, xsph_viscosity=0.5, sound_speed=20.0,
+              gamma_tait=7.0, substeps=substeps, boundary_layers=layers, gravity=(0.0, -9.81, 0.0),
+              max_speed_frac=0.4, artificial_viscosity=0.05)
+    kw.update(over)
+    p = make_params(**kw)
+    p.particle_mass = lattice_mass(p, spacing)
+    return p
+
+
+def assemble(name, params, fluid_pos, bodies, spacing, ticks, meta=None, cache=None) -> SceneSpec:
+    nf = fluid_pos.shape[0]
+    bpos, bvel, bm, bspans = body_particles(bodies, spacing, params.smoothing_radius, params.boundary_layers,
+                                            params.rest_density, cache)
+    pos = np.concatenate([fluid_pos, bpos]).astype(F)
+    vel = np.zeros_like(pos)
+    vel[nf:] = bvel
+    pm = np.concatenate([np.full(nf, F(params.particle_mass), F), bm]).astype(F)
+    spans = [(b, o, s + nf, e + nf) for (b, o, s, e) in bspans]
+    return SceneSpec(name, params, pos, vel, pm, nf, spans, spacing, ticks, meta or {})
+
+
+def dam_break(name: str, dims, spacing: float, tank, ticks: int, seed: int, extra_bodies=(), substeps: int = 10,
+              layers: int = 1, **over) -> SceneSpec:
+    params = baseline_params(spacing, substeps=substeps, layers=layers, **over)
+    fluid = jitter(fluid_block((0.0, 0.0, 0.0), dims, spacing), spacing, seed)
+    bodies = tank_bodies(tank, 2.0 * spacing) + list(extra_bodies)
+    fill = float(np.prod(np.asarray(dims) * spacing) / np.prod(tank))
+    return assemble(name, params, fluid, bodies, spacing, ticks,
+                    {"dims": tuple(dims), "tank": tuple(tank), "fill": fill, "seed": seed})
+
+
+def floating_boxes(n: int, seed: int, lo, hi, half_lo: float, half_hi: float, first_id: int, gap: float) -> list:
+    """n boxes with per-axis half extents U(half_lo, half_hi) at non-overlapping random
+    centres inside [lo, hi] (seeded rejection sampling)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    out, boxes = [], []
+    tries = 0
+    while len(out) < n and tries < 100000:
+        tries += 1
+        half = rng.uniform(half_lo, half_hi, 3).astype(F)
+        c = np.array([rng.uniform(lo[a] + half[a], hi[a] - half[a]) for a in range(3)], F)
+        if any(np.all(np.abs(c - c2) < half + h2 + gap) for c2, h2 in boxes):
+            continue
+        boxes.append((c, half))
+        out.append(Body(first_id + len(out), tuple(float(x) for x in half), tuple(float(x) for x in c)))
+    return out
+
+
+def dam0(seed: int = 0) -> SceneSpec:
+    return dam_break("dam0", (16, 32, 32), 0.02, (1.0, 0.64, 0.64), 600, seed)
+
+
+def dam1(seed: int = 1) -> SceneSpec:
+    return dam_break("dam1", (100, 100, 100), 0.01, (2.0, 2.0, 1.0), 300, seed)
+
+
+def dam10m(seed: int = 2, boxes: int = 64) -> SceneSpec:
+    extra = floating_boxes(boxes, seed + 1000, (1.2, 0.05, 0.05), (2.45, 1.1, 1.15), 0.025, 0.075, 5, 0.02)
+    return dam_break("dam10m", (215, 215, 215), 0.005, (2.5, 1.2, 1.2), 120, seed, extra_bodies=extra)
+
+
+def small_dam(n=(8, 8, 8), spacing: float = 0.05, tank=(0.8, 0.6, 0.6), seed: int = 3, substeps: int = 4,
+              ticks: int = 10, **over) -> SceneSpec:
+    """A small tank scene for parity tests (same construction, smaller sizes)."""
+    return dam_break("small", n, spacing, tank, ticks, seed, substeps=substeps, **over)
+
+
+CONFIGS = {"dam0": dam0, "dam1": dam1, "dam10m": dam10m}

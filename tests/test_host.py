@@ -1,0 +1,173 @@
+"""Host-side checks that need no GPU: the C ABI library loads and exports every symbol
+include/vxl_sph.h declares, its struct layouts match the header, its host set-up math
+(lattice mass, Akinci lattice) equals the oracle bit for bit, the scene builders give
+the oracle's set_boundary_particles result, and argument errors come back as the
+reference's FfiError codes (crates/vxl-phys-ffi/src/lib.rs:26-33) rather than crashes.
+"""
+import ctypes as C
+import re
+import subprocess
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+ROOT = Path(__file__).resolve().parent.parent
+HEADER = ROOT / "include" / "vxl_sph.h"
+
+
+def declared_functions():
+    text = HEADER.read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(vxl_sph_[a-z_0-9]+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol(vxl):
+    lib = vxl.load()
+    names = declared_functions()
+    assert len(names) >= 20
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+    # and the binding covers every one of them
+    assert set(names) == set(vxl.SIGNATURES), set(names) ^ set(vxl.SIGNATURES)
+
+
+def test_abi_version(vxl):
+    assert vxl.load().vxl_sph_abi_version() == vxl.ABI_VERSION == 1
+
+
+def test_struct_sizes_match_header(vxl, tmp_path):
+    src = tmp_path / "sizes.c"
+    src.write_text(
+        '#include <stdio.h>\n#include "vxl_sph.h"\nint main(void){printf("%zu %zu %zu %zu %zu %zu %zu\\n",'
+        "sizeof(vxl_sph_params),sizeof(vxl_sph_desc),sizeof(vxl_sph_span),sizeof(vxl_sph_reaction),"
+        "sizeof(vxl_sph_grid_info),sizeof(vxl_sph_stats),sizeof(vxl_block_header));return 0;}\n")
+    exe = tmp_path / "sizes"
+    subprocess.run(["gcc", "-std=c99", "-I", str(ROOT / "include"), str(src), "-o", str(exe)], check=True)
+    got = [int(x) for x in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
+    want = [C.sizeof(t) for t in (vxl.Params, vxl.Desc, vxl.Span, vxl.Reaction, vxl.GridInfo, vxl.Stats,
+                                  vxl.BlockHeader)]
+    assert got == want
+
+
+@pytest.mark.parametrize("h,s", [(0.1, 0.05), (0.04, 0.02), (0.02, 0.01), (0.01, 0.005), (0.1, 0.03)])
+def test_lattice_mass_bit_identical(vxl, oracle_mod, h, s):
+    p = vxl.make_params(smoothing_radius=h)
+    c = oracle_mod.default_cfg(smoothing_radius=h)
+    m_lib = vxl.lattice_mass(p, s)
+    m_orc = float(oracle_mod.load().orc_lattice_mass(C.byref(c), s))
+    assert np.float32(m_lib).tobytes() == np.float32(m_orc).tobytes()
+
+
+@pytest.mark.parametrize("shape,half,radius,s,h,layers", [
+    (0, (0.06, 0.06, 0.06), 0.0, 0.05, 0.1, 2),
+    (0, (0.3, 0.05, 0.3), 0.0, 0.05, 0.1, 2),
+    (0, (0.02, 0.32, 0.36), 0.0, 0.02, 0.04, 1),
+    (0, (0.07, 0.11, 0.13), 0.0, 0.01, 0.02, 3),
+    (1, (0, 0, 0), 0.2, 0.05, 0.1, 2),
+    (1, (0, 0, 0), 0.13, 0.02, 0.04, 1),
+])
+def test_boundary_lattice_bit_identical(vxl, oracle_mod, shape, half, radius, s, h, layers):
+    pts_l, vol_l = vxl.boundary_lattice(shape, half, radius, s, h, layers)
+    pts_o, vol_o, _ = oracle_mod.lattice(shape, half, radius, s, h, layers)
+    assert pts_l.shape == pts_o.shape
+    assert pts_l.tobytes() == pts_o.tobytes()
+    assert np.float32(vol_l) == np.float32(vol_o)
+
+
+def test_scene_bodies_equal_oracle_set_boundary_particles(vxl, oracle_mod):
+    from vxl_sph import scenes
+    spec = scenes.small_dam()
+    c = oracle_mod.cfg_from_params(spec.params)
+    o = oracle_mod.OracleSystem(c, (0, 0, 0), (spec.n_fluid, 1, 1), spec.spacing)
+    bodies = scenes.tank_bodies(spec.meta["tank"], 2.0 * spec.spacing)
+    nb = o.set_bodies(bodies)
+    assert nb == spec.n_boundary
+    r = o.read_f32()
+    nf = spec.n_fluid
+    assert r["pos"][nf:].tobytes() == spec.pos[nf:].tobytes()
+    assert r["vel"][nf:].tobytes() == spec.vel[nf:].tobytes()
+    assert r["pmass"][nf:].tobytes() == spec.pmass[nf:].tobytes()
+    assert [(b, s, e) for b, _, s, e in o.spans()] == [(b, s, e) for b, _, s, e in spec.spans]
+    assert np.float32(o.mass) == np.float32(spec.params.particle_mass)
+
+
+def test_scene_moving_body_velocity_matches_oracle(vxl, oracle_mod):
+    from vxl_sph import scenes
+    b = scenes.Body(3, (0.05, 0.07, 0.04), (0.2, 0.3, 0.1), rot=(0.0, 0.38268343, 0.0, 0.9238795),
+                    linvel=(0.5, -0.2, 0.1), angvel=(0.3, 1.2, -0.7))
+    params = scenes.baseline_params(0.01)
+    pos, vel, pm, spans = scenes.body_particles([b], 0.01, params.smoothing_radius, 1, 1000.0)
+    c = oracle_mod.cfg_from_params(params)
+    o = oracle_mod.OracleSystem(c, (0, 0, 0), (1, 1, 1), 0.01)
+    o.set_bodies([b])
+    r = o.read_f32()
+    assert r["pos"][1:].tobytes() == pos.tobytes()
+    assert r["vel"][1:].tobytes() == vel.tobytes()
+
+
+def _desc(vxl, n=8):
+    p = vxl.make_params(particle_mass=1.0)
+    pos = np.zeros((n, 3), np.float32)
+    d = vxl.Desc()
+    d.hdr = vxl.header(vxl.Desc)
+    d.params = p
+    d.n_fluid = n
+    d.n_boundary = 0
+    d.pos_xyz = pos.ctypes.data_as(C.POINTER(C.c_float))
+    d.vel_xyz = pos.ctypes.data_as(C.POINTER(C.c_float))
+    d.pmass = None
+    return d, pos
+
+
+def test_create_argument_errors(vxl):
+    lib = vxl.load()
+    h = C.c_void_p()
+    assert lib.vxl_sph_create(None, C.byref(h)) == vxl.NULL_POINTER
+    d, keep = _desc(vxl)
+    d.hdr.version = 2
+    assert lib.vxl_sph_create(C.byref(d), C.byref(h)) == vxl.VERSION_MISMATCH
+    d, keep = _desc(vxl)
+    d.hdr.size = 8
+    assert lib.vxl_sph_create(C.byref(d), C.byref(h)) == vxl.SIZE_MISMATCH
+    d, keep = _desc(vxl)
+    d.params.particle_mass = 0.0
+    assert lib.vxl_sph_create(C.byref(d), C.byref(h)) == vxl.INVALID_ARGUMENT
+    d, keep = _desc(vxl)
+    d.params.max_bins = (1 << 21) + 1
+    assert lib.vxl_sph_create(C.byref(d), C.byref(h)) == vxl.INVALID_ARGUMENT
+    assert b"max_bins" in lib.vxl_sph_last_error()
+
+
+def test_null_handle_errors(vxl):
+    lib = vxl.load()
+    assert lib.vxl_sph_destroy(None) == vxl.NULL_POINTER
+    assert lib.vxl_sph_step_tick(None, 1 / 60, None, 0, None) == vxl.NULL_POINTER
+    assert lib.vxl_sph_read_state(None, None, None) == vxl.NULL_POINTER
+    assert lib.vxl_sph_upload_boundary(None, 0, None, None, 0) == vxl.NULL_POINTER
+
+
+def test_no_cpu_fallback_without_gpu(vxl):
+    """Without a usable sm_100 device the library refuses to run (no CPU path)."""
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    assert vxl.PhysGpuBackend().available() is False
+    assert vxl.PhysGpuBackend().name() == "b200-cuda-wcsph"
+    d, keep = _desc(vxl)
+    h = C.c_void_p()
+    st = vxl.load().vxl_sph_create(C.byref(d), C.byref(h))
+    assert st == vxl.CUDA_ERROR and not h.value
+
+
+def test_scene_sizes(vxl):
+    from vxl_sph import scenes
+    s0 = scenes.dam0()
+    assert s0.n_fluid == 16384 and s0.n_boundary > 0
+    assert s0.params.substeps == 10 and abs(s0.params.smoothing_radius - 0.04) < 1e-9
+    assert all(s0.pmass[:s0.n_fluid] == np.float32(s0.params.particle_mass))
+    # jitter is within +-1% of the spacing and seeded
+    lat = scenes.fluid_block((0, 0, 0), (16, 32, 32), 0.02)
+    dj = np.abs(s0.pos[:s0.n_fluid] - lat)
+    assert dj.max() <= 0.01 * 0.02 * 1.0001 and dj.max() > 0
+    assert scenes.dam0().pos.tobytes() == s0.pos.tobytes()
