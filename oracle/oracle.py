@@ -76,6 +76,7 @@ def load() -> C.CDLL:
         "orc_n_fluid": (C.c_uint64, [C.c_void_p]),
         "orc_mass": (C.c_double, [C.c_void_p]),
         "orc_set_threads": (None, [C.c_void_p, C.c_uint32]),
+        "orc_set_mass": (None, [C.c_void_p, C.c_double]),
         "orc_lattice_mass": (C.c_float, [C.POINTER(Cfg), C.c_float]),
         "orc_set_state": (C.c_int, [C.c_void_p, _FP, _FP, C.c_uint64]),
         "orc_set_bodies": (C.c_uint64, [C.c_void_p, C.POINTER(OBody), C.c_uint32]),
@@ -161,7 +162,10 @@ class OracleSystem:
         cfg = cfg_from_params(spec.params, threads)
         dims = (spec.n_fluid, 1, 1)
         o = cls(cfg, (0.0, 0.0, 0.0), dims, spec.spacing, fp64)
-        if abs(o.mass - spec.params.particle_mass) > 0:
+        if fp64:
+            # identical state: the twin uses the f32 system's mass value
+            o.lib.orc_set_mass(o._h, float(np.float32(spec.params.particle_mass)))
+        elif np.float32(o.mass) != np.float32(spec.params.particle_mass):
             raise AssertionError("oracle lattice mass differs from the scene's calibrated mass")
         pos = np.ascontiguousarray(spec.pos[:spec.n_fluid], np.float32)
         vel = np.ascontiguousarray(spec.vel[:spec.n_fluid], np.float32)

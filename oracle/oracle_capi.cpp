@@ -140,6 +140,16 @@ void orc_set_threads(void* p, uint32_t t) {
   with<float>((Handle*)p, [&](auto& s) { s.cfg.threads = t; });
 }
 
+// Override the fluid particle mass (and the fluid prefix's pmass), e.g. to give the FP64
+// twin exactly the f32 system's calibrated mass.
+void orc_set_mass(void* p, double m) {
+  with<float>((Handle*)p, [&](auto& s) {
+    using R = std::decay_t<decltype(s.h)>;
+    s.mass = (R)m;
+    for (size_t i = 0; i < s.n_fluid; ++i) s.pmass[i] = (R)m;
+  });
+}
+
 // Lattice mass calibration without building a system (crates/vxl-phys-fluid/src/fluid_access.rs:27-42).
 float orc_lattice_mass(const orc_cfg* cfg, float spacing) {
   return FluidSystem<float>::lattice_mass(to_cfg<float>(cfg), spacing);

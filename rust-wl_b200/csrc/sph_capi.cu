@@ -5,6 +5,7 @@
 // implemented by GpuFluidStepper (crates/vxl-phys-gpu/src/pipeline/stepper.rs:22-147).
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <new>
 #include <string>
@@ -33,6 +34,34 @@ vxl_status fail(vxl_status s, const std::string& msg) {
   } while (0)
 
 constexpr int kThreads = 256;
+
+// VXL_SPH_DEBUG=1: report, on stderr, any CUDA runtime error left pending at the entry
+// or exit of a public call (attributes a sticky error to the call that caused it).
+bool debug_on() {
+  static int on = -1;
+  if (on < 0) {
+    const char* e = std::getenv("VXL_SPH_DEBUG");
+    on = (e && e[0] == '1') ? 1 : 0;
+  }
+  return on == 1;
+}
+
+struct ApiTrace {
+  const char* fn;
+  explicit ApiTrace(const char* f) : fn(f) {
+    if (debug_on()) {
+      cudaError_t e = cudaPeekAtLastError();
+      if (e != cudaSuccess) std::fprintf(stderr, "[vxl_sph] pending at entry of %s: %s\n", fn, cudaGetErrorString(e));
+    }
+  }
+  ~ApiTrace() {
+    if (debug_on()) {
+      cudaError_t e = cudaPeekAtLastError();
+      if (e != cudaSuccess) std::fprintf(stderr, "[vxl_sph] pending at exit of %s: %s\n", fn, cudaGetErrorString(e));
+    }
+  }
+};
+#define API_TRACE() ApiTrace api_trace_(__func__)
 
 inline uint32_t blocks_for(uint64_t n, int t = kThreads) { return (uint32_t)((n + t - 1) / t); }
 
@@ -87,6 +116,7 @@ struct vxl_sph_handle {
 
   // per-kernel device timers (vxl_sph_set_profile)
   bool prof = false;
+  bool capturing = false;  // inside cudaStreamBeginCapture .. EndCapture
   bool graph_prof = false;
   bool prof_pending = false;
   std::vector<cudaEvent_t> prof_ev;
@@ -136,6 +166,13 @@ const char* const kKernelNames[KID_COUNT] = {
   "k_gridbox", "k_keys", "k_scan_partial", "k_scan_top", "k_scan_final", "k_place", "k_canon",
   "k_density", "k_force", "k_bforce", "k_reactions", "k_scale"};
 
+// Inside stream capture a plain cudaEventRecord only expresses a dependency; the
+// External flag makes the graph record the event each time it runs.
+void record_event(vxl_sph_handle* h, cudaEvent_t e) {
+  if (h->capturing) cudaEventRecordWithFlags(e, h->stream, cudaEventRecordExternal);
+  else cudaEventRecord(e, h->stream);
+}
+
 int prof_begin(vxl_sph_handle* h, int kid) {
   if (!h->prof) return -1;
   if (2 * h->prof_used + 2 > h->prof_ev.size()) {
@@ -148,12 +185,12 @@ int prof_begin(vxl_sph_handle* h, int kid) {
   }
   size_t i = h->prof_used++;
   h->prof_kid[i] = kid;
-  cudaEventRecord(h->prof_ev[2 * i], h->stream);
+  record_event(h, h->prof_ev[2 * i]);
   return (int)i;
 }
 
 void prof_end(vxl_sph_handle* h, int i) {
-  if (i >= 0) cudaEventRecord(h->prof_ev[2 * i + 1], h->stream);
+  if (i >= 0) record_event(h, h->prof_ev[2 * i + 1]);
 }
 
 // Add the elapsed times of the last enqueued tick (waits for it).
@@ -162,9 +199,13 @@ void prof_collect(vxl_sph_handle* h) {
   cudaStreamSynchronize(h->stream);
   for (size_t i = 0; i < h->prof_used; ++i) {
     float ms = 0.f;
-    if (cudaEventElapsedTime(&ms, h->prof_ev[2 * i], h->prof_ev[2 * i + 1]) == cudaSuccess) {
+    cudaError_t e = cudaEventElapsedTime(&ms, h->prof_ev[2 * i], h->prof_ev[2 * i + 1]);
+    if (e == cudaSuccess) {
       h->prof_ms[h->prof_kid[i]] += ms;
       h->prof_n[h->prof_kid[i]] += 1;
+    } else {
+      if (debug_on()) std::fprintf(stderr, "[vxl_sph] cudaEventElapsedTime(%zu): %s\n", i, cudaGetErrorString(e));
+      cudaGetLastError();  // the timer pair is dropped; do not leave the error pending
     }
   }
   h->prof_pending = false;
@@ -285,11 +326,18 @@ vxl_status stage_spans(vxl_sph_handle* h, const vxl_sph_span* spans, uint32_t ns
     CU(cudaMallocHost((void**)&h->breact_h, cap * 6 * sizeof(float)));
     h->spans_cap = cap;
   }
+  std::vector<SpanDev> next(nspans);
   for (uint32_t q = 0; q < nspans; ++q) {
     const vxl_sph_span& s = spans[q];
     if (s.start < h->nf || s.end < s.start || s.end > h->nt)
       return fail(VXL_INVALID_ARGUMENT, "span " + std::to_string(q) + " is outside the boundary segment");
-    h->spans_h[q] = SpanDev{s.body, s.origin[0], s.origin[1], s.origin[2], s.start, s.end};
+    next[q] = SpanDev{s.body, s.origin[0], s.origin[1], s.origin[2], s.start, s.end};
+  }
+  // The tick graph copies the pinned table when it runs; an earlier tick may still be
+  // queued, so wait for it before changing the table (steady state: unchanged, no wait).
+  if (std::memcmp(next.data(), h->spans_h, nspans * sizeof(SpanDev)) != 0) {
+    CU(cudaStreamSynchronize(h->stream));
+    std::memcpy(h->spans_h, next.data(), nspans * sizeof(SpanDev));
   }
   return VXL_OK;
 }
@@ -315,7 +363,9 @@ vxl_status run_tick(vxl_sph_handle* h, float dt_tick, uint32_t nspans) {
     cudaGraph_t g = nullptr;
     h->prof_used = 0;
     CU(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+    h->capturing = true;
     enqueue_tick(h, dt_tick, nspans);
+    h->capturing = false;
     CU(cudaStreamEndCapture(h->stream, &g));
     cudaError_t e = cudaGraphInstantiate(&h->graph, g, 0);
     cudaGraphDestroy(g);
@@ -395,6 +445,7 @@ int vxl_sph_backend_available(void) {
 }
 
 vxl_status vxl_sph_create(const vxl_sph_desc* desc, vxl_sph_handle** out) {
+  API_TRACE();
   try {
     if (!desc || !out) return fail(VXL_NULL_POINTER, "desc or out is NULL");
     *out = nullptr;
@@ -504,6 +555,7 @@ vxl_status vxl_sph_create(const vxl_sph_desc* desc, vxl_sph_handle** out) {
 }
 
 vxl_status vxl_sph_destroy(vxl_sph_handle* h) {
+  API_TRACE();
   if (!h) return fail(VXL_NULL_POINTER, "handle is NULL");
   DeviceGuard dg(h->device);
   cudaStreamSynchronize(h->stream);
@@ -514,6 +566,7 @@ vxl_status vxl_sph_destroy(vxl_sph_handle* h) {
 
 vxl_status vxl_sph_upload_boundary(vxl_sph_handle* h, uint64_t n_fluid, const float* pos_xyz, const float* vel_xyz,
                                    uint64_t nb) {
+  API_TRACE();
   if (!h) return fail(VXL_NULL_POINTER, "handle is NULL");
   if (n_fluid != h->nf || nb != h->nb)
     return fail(VXL_SIZE_MISMATCH, "boundary segment length differs from the scene (rebuild the scene)");
@@ -527,10 +580,13 @@ vxl_status vxl_sph_upload_boundary(vxl_sph_handle* h, uint64_t n_fluid, const fl
   k_upload_boundary<<<blocks_for(nb), kThreads, 0, h->stream>>>(h->stage, h->stage + 3 * nb, h->pos[0], h->vel[0],
                                                                  h->slot_of, h->bpos, h->ctl->bbox, h->k);
   CU(cudaGetLastError());
+  // the caller's arrays are borrowed for this call only: finish the copies before returning
+  CU(cudaStreamSynchronize(h->stream));
   return VXL_OK;
 }
 
 vxl_status vxl_sph_step_tick_async(vxl_sph_handle* h, float dt_tick, const vxl_sph_span* spans, uint32_t nspans) {
+  API_TRACE();
   try {
     if (!h) return fail(VXL_NULL_POINTER, "handle is NULL");
     if (!(dt_tick > 0.0f) || !std::isfinite(dt_tick)) return fail(VXL_INVALID_ARGUMENT, "dt_tick must be > 0");
@@ -548,6 +604,7 @@ vxl_status vxl_sph_step_tick_async(vxl_sph_handle* h, float dt_tick, const vxl_s
 }
 
 vxl_status vxl_sph_sync(vxl_sph_handle* h, vxl_sph_reaction* out_reactions, uint32_t nspans) {
+  API_TRACE();
   if (!h) return fail(VXL_NULL_POINTER, "handle is NULL");
   DeviceGuard dg(h->device);
   if (nspans > h->last_nspans) return fail(VXL_SIZE_MISMATCH, "more reactions requested than spans stepped");
@@ -556,6 +613,7 @@ vxl_status vxl_sph_sync(vxl_sph_handle* h, vxl_sph_reaction* out_reactions, uint
 
 vxl_status vxl_sph_step_tick(vxl_sph_handle* h, float dt_tick, const vxl_sph_span* spans, uint32_t nspans,
                              vxl_sph_reaction* out_reactions) {
+  API_TRACE();
   if (nspans > 0 && !out_reactions) return fail(VXL_NULL_POINTER, "out_reactions is NULL with nspans > 0");
   vxl_status s = vxl_sph_step_tick_async(h, dt_tick, spans, nspans);
   if (s != VXL_OK) return s;
@@ -563,6 +621,7 @@ vxl_status vxl_sph_step_tick(vxl_sph_handle* h, float dt_tick, const vxl_sph_spa
 }
 
 vxl_status vxl_sph_substep(vxl_sph_handle* h, float dt) {
+  API_TRACE();
   if (!h) return fail(VXL_NULL_POINTER, "handle is NULL");
   if (!(dt > 0.0f)) return fail(VXL_INVALID_ARGUMENT, "dt must be > 0");
   DeviceGuard dg(h->device);
@@ -578,6 +637,7 @@ vxl_status vxl_sph_substep(vxl_sph_handle* h, float dt) {
 }
 
 vxl_status vxl_sph_bounds(vxl_sph_handle* h, float lo[3], float hi[3]) {
+  API_TRACE();
   if (!h || !lo || !hi) return fail(VXL_NULL_POINTER, "NULL argument");
   DeviceGuard dg(h->device);
   uint32_t box[6];
@@ -592,6 +652,7 @@ vxl_status vxl_sph_bounds(vxl_sph_handle* h, float lo[3], float hi[3]) {
 }
 
 vxl_status vxl_sph_read_state(vxl_sph_handle* h, float* pos_xyz, float* vel_xyz) {
+  API_TRACE();
   if (!h) return fail(VXL_NULL_POINTER, "handle is NULL");
   DeviceGuard dg(h->device);
   if (h->nt == 0) return VXL_OK;
@@ -606,6 +667,7 @@ vxl_status vxl_sph_read_state(vxl_sph_handle* h, float* pos_xyz, float* vel_xyz)
 }
 
 vxl_status vxl_sph_write_state(vxl_sph_handle* h, const float* pos_xyz, const float* vel_xyz) {
+  API_TRACE();
   if (!h) return fail(VXL_NULL_POINTER, "handle is NULL");
   DeviceGuard dg(h->device);
   if (h->nt == 0) return VXL_OK;
@@ -620,10 +682,12 @@ vxl_status vxl_sph_write_state(vxl_sph_handle* h, const float* pos_xyz, const fl
     if (s != VXL_OK) return s;
   }
   CU(cudaGetLastError());
+  CU(cudaStreamSynchronize(h->stream));  // the caller's arrays are borrowed for this call only
   return VXL_OK;
 }
 
 vxl_status vxl_sph_set_record(vxl_sph_handle* h, int on) {
+  API_TRACE();
   if (!h) return fail(VXL_NULL_POINTER, "handle is NULL");
   h->record = on != 0;
   return VXL_OK;
@@ -631,6 +695,7 @@ vxl_status vxl_sph_set_record(vxl_sph_handle* h, int on) {
 
 vxl_status vxl_sph_read_fields(vxl_sph_handle* h, float* dens, float* press, float* acc_xyz, float* xsph_xyz,
                                float* bforce_xyz) {
+  API_TRACE();
   if (!h) return fail(VXL_NULL_POINTER, "handle is NULL");
   DeviceGuard dg(h->device);
   uint64_t nt = h->nt;
@@ -661,6 +726,7 @@ vxl_status vxl_sph_read_fields(vxl_sph_handle* h, float* dens, float* press, flo
 
 vxl_status vxl_sph_export_grid(vxl_sph_handle* h, uint32_t* items, uint32_t* start, uint64_t start_cap,
                                uint32_t* bins, vxl_sph_grid_info* info) {
+  API_TRACE();
   if (!h) return fail(VXL_NULL_POINTER, "handle is NULL");
   DeviceGuard dg(h->device);
   if (!h->ran_substep) return fail(VXL_NOT_READY, "no substep has run yet");
@@ -691,6 +757,7 @@ vxl_status vxl_sph_export_grid(vxl_sph_handle* h, uint32_t* items, uint32_t* sta
 }
 
 vxl_status vxl_sph_set_stream(vxl_sph_handle* h, void* cuda_stream) {
+  API_TRACE();
   if (!h) return fail(VXL_NULL_POINTER, "handle is NULL");
   DeviceGuard dg(h->device);
   prof_collect(h);
@@ -700,10 +767,19 @@ vxl_status vxl_sph_set_stream(vxl_sph_handle* h, void* cuda_stream) {
 }
 
 vxl_status vxl_sph_set_profile(vxl_sph_handle* h, int on) {
+  API_TRACE();
   if (!h) return fail(VXL_NULL_POINTER, "handle is NULL");
   DeviceGuard dg(h->device);
   prof_collect(h);
   h->prof = on != 0;
+  // events for every launch of a tick, created here (never during graph capture)
+  size_t need = 2 * ((size_t)h->substeps * 12 + 8);
+  while (h->prof && h->prof_ev.size() < need) {
+    cudaEvent_t e;
+    CU(cudaEventCreate(&e));
+    h->prof_ev.push_back(e);
+  }
+  h->prof_kid.resize(h->prof_ev.size() / 2);
   for (int k = 0; k < KID_COUNT; ++k) {
     h->prof_ms[k] = 0.0;
     h->prof_n[k] = 0;
@@ -713,6 +789,7 @@ vxl_status vxl_sph_set_profile(vxl_sph_handle* h, int on) {
 
 vxl_status vxl_sph_profile_read(vxl_sph_handle* h, uint32_t k, const char** name, double* total_ms,
                                 uint64_t* launches) {
+  API_TRACE();
   if (!h) return fail(VXL_NULL_POINTER, "handle is NULL");
   if (k >= (uint32_t)KID_COUNT) return fail(VXL_INVALID_ARGUMENT, "kernel index past the table");
   DeviceGuard dg(h->device);
@@ -724,6 +801,7 @@ vxl_status vxl_sph_profile_read(vxl_sph_handle* h, uint32_t k, const char** name
 }
 
 vxl_status vxl_sph_get_stats(vxl_sph_handle* h, vxl_sph_stats* out) {
+  API_TRACE();
   if (!h || !out) return fail(VXL_NULL_POINTER, "NULL argument");
   if (!check_header(out->hdr, sizeof(vxl_sph_stats))) return fail(VXL_SIZE_MISMATCH, "stats header");
   DeviceGuard dg(h->device);
