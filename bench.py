@@ -322,6 +322,20 @@ def run_ours(args) -> None:
         dist.destroy_process_group()
 
 
+def run_ncu_case(args) -> None:
+    """Smallest run of the workload for a profiler: build, `--warmup` ticks, exit."""
+    import vxl_sph
+    vxl_sph.load()
+    spec = build_scene(args.workload)
+    scene = vxl_sph.Scene(spec.params, spec.pos, spec.vel, spec.pmass, spec.n_fluid)
+    dt_tick = float(np.float32(1.0) / np.float32(60.0))
+    for _ in range(max(args.warmup, 1)):
+        scene.step_tick(dt_tick, spec.spans)
+    scene.close()
+    print(json.dumps({"ncu_case": spec.name, "ticks": max(args.warmup, 1), "n_fluid": spec.n_fluid,
+                      "n_boundary": spec.n_boundary}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -330,8 +344,11 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", default="dam1", choices=["dam0", "dam1", "dam10m"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ncu-case", action="store_true", help="build + warm-up ticks only (for ncu captures)")
     args = ap.parse_args()
-    if args.impl == "reference":
+    if args.ncu_case:
+        run_ncu_case(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_ours(args)

@@ -3,6 +3,7 @@
 //
 // Reference seam: FluidStepper (crates/vxl-phys-core/src/interop.rs:293-316) as
 // implemented by GpuFluidStepper (crates/vxl-phys-gpu/src/pipeline/stepper.rs:22-147).
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -92,6 +93,9 @@ struct vxl_sph_handle {
   float4* xsph = nullptr;
   float4* bforce = nullptr;
   float4* bpos = nullptr;
+  uint32_t* nbr = nullptr;    // neighbour list, nbr[k * nt + s], k < nbr_cap
+  uint32_t* nbr_n = nullptr;  // neighbour count per slot
+  uint32_t nbr_cap = 64;
   Ctl* ctl = nullptr;
   float* stage = nullptr;  // 8 * nt floats: device staging for host uploads/exports
   SpanDev* spans_d = nullptr;
@@ -99,6 +103,14 @@ struct vxl_sph_handle {
   uint32_t spans_cap = 0;
   float* breact_d = nullptr;
   float* breact_h = nullptr;  // pinned
+  SpanChunk* chunks_d = nullptr;
+  SpanChunk* chunks_h = nullptr;  // pinned
+  uint32_t* chunk_first_d = nullptr;
+  uint32_t* chunk_first_h = nullptr;  // pinned
+  float* react_partial = nullptr;
+  uint32_t chunks_cap = 0;
+  uint32_t nchunks = 0;
+  uint32_t graph_nchunks = 0;
   Ctl* ctl_h = nullptr;       // pinned
   bool record = false;
   bool ran_substep = false;
@@ -145,11 +157,14 @@ void free_all(vxl_sph_handle* h) {
   if (h->graph) cudaGraphExecDestroy(h->graph);
   void* ptrs[] = {h->pos[0], h->pos[1], h->vel[0], h->vel[1], h->orig, h->slot_of, h->cellrank, h->items,
                   h->counts, h->start, h->partial, h->rc, h->press, h->acc, h->xsph, h->bforce, h->bpos,
-                  h->ctl, h->stage, h->spans_d, h->breact_d};
+                  h->ctl, h->stage, h->spans_d, h->breact_d, h->nbr, h->nbr_n, h->chunks_d,
+                  h->chunk_first_d, h->react_partial};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (h->spans_h) cudaFreeHost(h->spans_h);
   if (h->breact_h) cudaFreeHost(h->breact_h);
+  if (h->chunks_h) cudaFreeHost(h->chunks_h);
+  if (h->chunk_first_h) cudaFreeHost(h->chunk_first_h);
   if (h->ctl_h) cudaFreeHost(h->ctl_h);
   if (h->ev0) cudaEventDestroy(h->ev0);
   if (h->ev1) cudaEventDestroy(h->ev1);
@@ -160,11 +175,11 @@ void free_all(vxl_sph_handle* h) {
 // Kernel names of the per-kernel timer table (index = id).
 enum KernelId : int {
   KID_GRIDBOX, KID_KEYS, KID_SCAN_PARTIAL, KID_SCAN_TOP, KID_SCAN_FINAL, KID_PLACE, KID_CANON,
-  KID_DENSITY, KID_FORCE, KID_BFORCE, KID_REACTIONS, KID_SCALE, KID_COUNT
+  KID_DENSITY, KID_FORCE, KID_BFORCE, KID_REACT_CHUNKS, KID_REACT_SPANS, KID_SCALE, KID_COUNT
 };
 const char* const kKernelNames[KID_COUNT] = {
   "k_gridbox", "k_keys", "k_scan_partial", "k_scan_top", "k_scan_final", "k_place", "k_canon",
-  "k_density", "k_force", "k_bforce", "k_reactions", "k_scale"};
+  "k_density", "k_force", "k_bforce", "k_react_chunks", "k_react_spans", "k_scale"};
 
 // Inside stream capture a plain cudaEventRecord only expresses a dependency; the
 // External flag makes the graph record the event each time it runs.
@@ -271,17 +286,22 @@ void enqueue_substep(vxl_sph_handle* h, float dt, uint32_t nspans) {
   LAUNCH(KID_PLACE, k_place<<<nblk, kThreads, 0, st>>>(h->cellrank, h->start, h->orig, h->items, nt));
   LAUNCH(KID_CANON, k_canon<<<148 * 8, 256, 0, st>>>(h->items, h->start, h->ctl, h->pos[0], h->vel[0], h->pos[1],
                                                      h->vel[1], h->orig, h->slot_of));
-  LAUNCH(KID_DENSITY, k_density<<<nblk, kThreads, 0, st>>>(h->pos[1], h->start, h->ctl, h->rc, h->press, h->k));
-  LAUNCH(KID_FORCE, k_force<<<nblk, kThreads, 0, st>>>(h->pos[1], h->vel[1], h->rc, h->start, h->ctl, h->pos[0],
-                                                       h->vel[0], h->record ? h->acc : nullptr,
-                                                       h->record ? h->xsph : nullptr, h->k, sc));
+  LAUNCH(KID_DENSITY, k_density<<<nblk, kThreads, 0, st>>>(h->pos[1], h->start, h->ctl, h->rc, h->press, h->nbr,
+                                                           h->nbr_n, h->nbr_cap, h->k));
+  LAUNCH(KID_FORCE, k_force<<<nblk, kThreads, 0, st>>>(h->pos[1], h->vel[1], h->rc, h->start, h->nbr, h->nbr_n,
+                                                       h->nbr_cap, h->ctl, h->pos[0], h->vel[0],
+                                                       h->record ? h->acc : nullptr, h->record ? h->xsph : nullptr,
+                                                       h->k, sc));
   if (h->nb > 0 && (nspans > 0 || h->record)) {
     LAUNCH(KID_BFORCE, k_bforce<<<blocks_for(nt, 128), 128, 0, st>>>(h->pos[1], h->vel[1], h->rc, h->start, h->orig,
-                                                                     h->ctl, h->bforce, h->k));
+                                                                     h->nbr, h->nbr_n, h->nbr_cap, h->ctl,
+                                                                     h->bforce, h->k));
   }
-  if (nspans > 0) {
-    LAUNCH(KID_REACTIONS,
-           k_reactions<<<nspans, 512, 0, st>>>(h->bforce, h->bpos, h->spans_d, h->breact_d, (uint32_t)h->nf));
+  if (nspans > 0 && h->nchunks > 0) {
+    LAUNCH(KID_REACT_CHUNKS, k_react_chunks<<<h->nchunks, kReactThreads, 0, st>>>(
+                                 h->bforce, h->bpos, h->spans_d, h->chunks_d, h->react_partial, (uint32_t)h->nf));
+    LAUNCH(KID_REACT_SPANS, k_react_spans<<<blocks_for(nspans, 64), 64, 0, st>>>(h->react_partial, h->chunk_first_d,
+                                                                                 h->breact_d, nspans));
   }
 }
 
@@ -292,6 +312,9 @@ void enqueue_tick(vxl_sph_handle* h, float dt_tick, uint32_t nspans) {
   float dt = dt_tick / (float)sub;  // fluid_step.rs:77
   if (nspans > 0) {
     cudaMemcpyAsync(h->spans_d, h->spans_h, nspans * sizeof(SpanDev), cudaMemcpyHostToDevice, st);
+    if (h->nchunks > 0)
+      cudaMemcpyAsync(h->chunks_d, h->chunks_h, h->nchunks * sizeof(SpanChunk), cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(h->chunk_first_d, h->chunk_first_h, (nspans + 1) * sizeof(uint32_t), cudaMemcpyHostToDevice, st);
     cudaMemsetAsync(h->breact_d, 0, nspans * 6 * sizeof(float), st);
   }
   for (uint32_t s = 0; s < sub; ++s) enqueue_substep(h, dt, nspans);
@@ -308,43 +331,66 @@ void enqueue_tick(vxl_sph_handle* h, float dt_tick, uint32_t nspans) {
 vxl_status stage_spans(vxl_sph_handle* h, const vxl_sph_span* spans, uint32_t nspans) {
   if (nspans == 0) return VXL_OK;
   if (!spans) return fail(VXL_NULL_POINTER, "spans is NULL with nspans > 0");
-  if (nspans > h->spans_cap) {
+  std::vector<SpanDev> next(nspans);
+  std::vector<SpanChunk> chunks;
+  std::vector<uint32_t> first(nspans + 1, 0);
+  for (uint32_t q = 0; q < nspans; ++q) {
+    const vxl_sph_span& sp = spans[q];
+    if (sp.start < h->nf || sp.end < sp.start || sp.end > h->nt)
+      return fail(VXL_INVALID_ARGUMENT, "span " + std::to_string(q) + " is outside the boundary segment");
+    next[q] = SpanDev{sp.body, sp.origin[0], sp.origin[1], sp.origin[2], sp.start, sp.end};
+    first[q] = (uint32_t)chunks.size();
+    for (uint32_t b = sp.start; b < sp.end; b += kReactChunk)
+      chunks.push_back(SpanChunk{q, b, std::min(sp.end, b + kReactChunk), 0u});
+  }
+  first[nspans] = (uint32_t)chunks.size();
+  uint32_t nch = (uint32_t)chunks.size();
+  if (nspans > h->spans_cap || nch > h->chunks_cap) {
+    CU(cudaStreamSynchronize(h->stream));
     if (h->graph) {
       cudaGraphExecDestroy(h->graph);
       h->graph = nullptr;
     }
-    if (h->spans_d) cudaFree(h->spans_d);
-    if (h->spans_h) cudaFreeHost(h->spans_h);
-    if (h->breact_d) cudaFree(h->breact_d);
-    if (h->breact_h) cudaFreeHost(h->breact_h);
+    void* dptr[] = {h->spans_d, h->breact_d, h->chunks_d, h->chunk_first_d, h->react_partial};
+    for (void* q : dptr)
+      if (q) cudaFree(q);
+    void* hptr[] = {h->spans_h, h->breact_h, h->chunks_h, h->chunk_first_h};
+    for (void* q : hptr)
+      if (q) cudaFreeHost(q);
     h->spans_d = nullptr; h->spans_h = nullptr; h->breact_d = nullptr; h->breact_h = nullptr;
-    uint32_t cap = nspans < 64 ? 64 : nspans;
-    vxl_status s;
-    if ((s = dalloc(h, &h->spans_d, cap)) != VXL_OK) return s;
-    if ((s = dalloc(h, &h->breact_d, (size_t)cap * 6)) != VXL_OK) return s;
+    h->chunks_d = nullptr; h->chunks_h = nullptr; h->chunk_first_d = nullptr; h->chunk_first_h = nullptr;
+    h->react_partial = nullptr;
+    uint32_t cap = std::max<uint32_t>(nspans, 64);
+    uint32_t ccap = std::max<uint32_t>(nch, cap + (uint32_t)(h->nb / kReactChunk) + 1);
+    vxl_status st;
+    if ((st = dalloc(h, &h->spans_d, cap)) != VXL_OK) return st;
+    if ((st = dalloc(h, &h->breact_d, (size_t)cap * 6)) != VXL_OK) return st;
+    if ((st = dalloc(h, &h->chunks_d, ccap)) != VXL_OK) return st;
+    if ((st = dalloc(h, &h->chunk_first_d, (size_t)cap + 1)) != VXL_OK) return st;
+    if ((st = dalloc(h, &h->react_partial, (size_t)ccap * 6)) != VXL_OK) return st;
     CU(cudaMallocHost((void**)&h->spans_h, cap * sizeof(SpanDev)));
     CU(cudaMallocHost((void**)&h->breact_h, cap * 6 * sizeof(float)));
+    CU(cudaMallocHost((void**)&h->chunks_h, ccap * sizeof(SpanChunk)));
+    CU(cudaMallocHost((void**)&h->chunk_first_h, (cap + 1) * sizeof(uint32_t)));
+    std::memset(h->spans_h, 0xff, cap * sizeof(SpanDev));
     h->spans_cap = cap;
+    h->chunks_cap = ccap;
   }
-  std::vector<SpanDev> next(nspans);
-  for (uint32_t q = 0; q < nspans; ++q) {
-    const vxl_sph_span& s = spans[q];
-    if (s.start < h->nf || s.end < s.start || s.end > h->nt)
-      return fail(VXL_INVALID_ARGUMENT, "span " + std::to_string(q) + " is outside the boundary segment");
-    next[q] = SpanDev{s.body, s.origin[0], s.origin[1], s.origin[2], s.start, s.end};
-  }
-  // The tick graph copies the pinned table when it runs; an earlier tick may still be
-  // queued, so wait for it before changing the table (steady state: unchanged, no wait).
-  if (std::memcmp(next.data(), h->spans_h, nspans * sizeof(SpanDev)) != 0) {
+  // The tick graph copies the pinned tables when it runs; an earlier tick may still be
+  // queued, so wait for it before changing them (steady state: unchanged, no wait).
+  if (std::memcmp(next.data(), h->spans_h, nspans * sizeof(SpanDev)) != 0 || nch != h->nchunks) {
     CU(cudaStreamSynchronize(h->stream));
     std::memcpy(h->spans_h, next.data(), nspans * sizeof(SpanDev));
+    if (nch) std::memcpy(h->chunks_h, chunks.data(), nch * sizeof(SpanChunk));
+    std::memcpy(h->chunk_first_h, first.data(), (nspans + 1) * sizeof(uint32_t));
+    h->nchunks = nch;
   }
   return VXL_OK;
 }
 
 vxl_status run_tick(vxl_sph_handle* h, float dt_tick, uint32_t nspans) {
   bool need_capture = !h->graph || h->graph_dt != dt_tick || h->graph_nspans != nspans ||
-                      h->graph_record != h->record || h->graph_prof != h->prof;
+                      h->graph_record != h->record || h->graph_prof != h->prof || h->graph_nchunks != h->nchunks;
   prof_collect(h);
   h->launches_counter = 0;
   if (!h->use_graph) {
@@ -374,6 +420,7 @@ vxl_status run_tick(vxl_sph_handle* h, float dt_tick, uint32_t nspans) {
     h->graph_nspans = nspans;
     h->graph_record = h->record;
     h->graph_prof = h->prof;
+    h->graph_nchunks = h->nchunks;
     h->launches_last_tick = h->launches_counter;
   }
   CU(cudaGraphLaunch(h->graph, h->stream));
@@ -506,6 +553,8 @@ vxl_status vxl_sph_create(const vxl_sph_desc* desc, vxl_sph_handle** out) {
     A(dalloc(h, &h->press, nta));
     A(dalloc(h, &h->acc, nta));
     A(dalloc(h, &h->xsph, nta));
+    A(dalloc(h, &h->nbr, (size_t)h->nbr_cap * nta));
+    A(dalloc(h, &h->nbr_n, nta));
     A(dalloc(h, &h->bforce, nb ? nb : 1));
     A(dalloc(h, &h->bpos, nb ? nb : 1));
     A(dalloc(h, &h->ctl, 1));

@@ -280,8 +280,58 @@ __global__ void k_place(const uint2* __restrict__ cellrank, const uint32_t* __re
 
 // Per cell: order the placed entries by reference index (the reference's index-ascending
 // table, grid.rs:56-62) and gather position/velocity into the sorted buffer.
-// One warp per cell (grid-stride over cells). Rank of an entry = number of entries in
-// the cell with a smaller reference index (indices are unique).
+// A warp scans 32 consecutive cells at a time and handles each non-empty one
+// cooperatively. Rank of an entry = number of entries in the cell with a smaller
+// reference index (indices are unique).
+__device__ __forceinline__ void canon_cell(uint32_t b, uint32_t n, int lane, uint32_t* skeys, Ctl* ctl,
+                                           const uint2* __restrict__ items, const float4* __restrict__ pos_in,
+                                           const float4* __restrict__ vel_in, float4* __restrict__ pos_out,
+                                           float4* __restrict__ vel_out, uint32_t* __restrict__ orig,
+                                           uint32_t* __restrict__ slot_of) {
+  if (n <= 32) {
+    uint2 it = make_uint2(0xffffffffu, 0u);
+    if ((uint32_t)lane < n) it = items[b + lane];
+    uint32_t rank = 0;
+    for (uint32_t j = 0; j < n; ++j) {
+      uint32_t kj = __shfl_sync(0xffffffffu, it.x, j);
+      rank += (kj < it.x) ? 1u : 0u;
+    }
+    if ((uint32_t)lane < n) {
+      uint32_t dst = b + rank;
+      pos_out[dst] = pos_in[it.y];
+      vel_out[dst] = vel_in[it.y];
+      orig[dst] = it.x;
+      slot_of[it.x] = dst;
+    }
+  } else if (n <= (uint32_t)kCanonSmem) {
+    for (uint32_t e = lane; e < n; e += 32) skeys[e] = items[b + e].x;
+    __syncwarp();
+    for (uint32_t e = lane; e < n; e += 32) {
+      uint2 it = items[b + e];
+      uint32_t rank = 0;
+      for (uint32_t j = 0; j < n; ++j) rank += (skeys[j] < it.x) ? 1u : 0u;
+      uint32_t dst = b + rank;
+      pos_out[dst] = pos_in[it.y];
+      vel_out[dst] = vel_in[it.y];
+      orig[dst] = it.x;
+      slot_of[it.x] = dst;
+    }
+    __syncwarp();
+  } else {
+    if (lane == 0) atomicOr(&ctl->err, kErrCanonLarge);
+    for (uint32_t e = lane; e < n; e += 32) {
+      uint2 it = items[b + e];
+      uint32_t rank = 0;
+      for (uint32_t j = 0; j < n; ++j) rank += (items[b + j].x < it.x) ? 1u : 0u;
+      uint32_t dst = b + rank;
+      pos_out[dst] = pos_in[it.y];
+      vel_out[dst] = vel_in[it.y];
+      orig[dst] = it.x;
+      slot_of[it.x] = dst;
+    }
+  }
+}
+
 __global__ void k_canon(const uint2* __restrict__ items, const uint32_t* __restrict__ start, Ctl* ctl,
                         const float4* __restrict__ pos_in, const float4* __restrict__ vel_in,
                         float4* __restrict__ pos_out, float4* __restrict__ vel_out, uint32_t* __restrict__ orig,
@@ -291,51 +341,20 @@ __global__ void k_canon(const uint2* __restrict__ items, const uint32_t* __restr
   const int lane = threadIdx.x & 31;
   const int wib = threadIdx.x >> 5;
   const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
-  for (uint32_t c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; c < total; c += warps) {
-    uint32_t b = start[c];
-    uint32_t n = start[c + 1] - b;
-    if (n == 0) continue;
-    if (n <= 32) {
-      uint2 it = make_uint2(0xffffffffu, 0u);
-      if ((uint32_t)lane < n) it = items[b + lane];
-      uint32_t rank = 0;
-      for (uint32_t j = 0; j < n; ++j) {
-        uint32_t kj = __shfl_sync(0xffffffffu, it.x, j);
-        rank += (kj < it.x) ? 1u : 0u;
-      }
-      if ((uint32_t)lane < n) {
-        uint32_t dst = b + rank;
-        pos_out[dst] = pos_in[it.y];
-        vel_out[dst] = vel_in[it.y];
-        orig[dst] = it.x;
-        slot_of[it.x] = dst;
-      }
-    } else if (n <= (uint32_t)kCanonSmem) {
-      for (uint32_t e = lane; e < n; e += 32) skeys[wib][e] = items[b + e].x;
-      __syncwarp();
-      for (uint32_t e = lane; e < n; e += 32) {
-        uint2 it = items[b + e];
-        uint32_t rank = 0;
-        for (uint32_t j = 0; j < n; ++j) rank += (skeys[wib][j] < it.x) ? 1u : 0u;
-        uint32_t dst = b + rank;
-        pos_out[dst] = pos_in[it.y];
-        vel_out[dst] = vel_in[it.y];
-        orig[dst] = it.x;
-        slot_of[it.x] = dst;
-      }
-      __syncwarp();
-    } else {
-      if (lane == 0) atomicOr(&ctl->err, kErrCanonLarge);
-      for (uint32_t e = lane; e < n; e += 32) {
-        uint2 it = items[b + e];
-        uint32_t rank = 0;
-        for (uint32_t j = 0; j < n; ++j) rank += (items[b + j].x < it.x) ? 1u : 0u;
-        uint32_t dst = b + rank;
-        pos_out[dst] = pos_in[it.y];
-        vel_out[dst] = vel_in[it.y];
-        orig[dst] = it.x;
-        slot_of[it.x] = dst;
-      }
+  for (uint32_t base = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32u; base < total; base += warps * 32u) {
+    uint32_t c = base + lane;
+    uint32_t b = 0, n = 0;
+    if (c < total) {
+      b = start[c];
+      n = start[c + 1] - b;
+    }
+    uint32_t mask = __ballot_sync(0xffffffffu, n > 0);
+    while (mask) {
+      int l = __ffs(mask) - 1;
+      mask &= mask - 1;
+      uint32_t cb = __shfl_sync(0xffffffffu, b, l);
+      uint32_t cn = __shfl_sync(0xffffffffu, n, l);
+      canon_cell(cb, cn, lane, skeys[wib], ctl, items, pos_in, vel_in, pos_out, vel_out, orig, slot_of);
     }
   }
 }
@@ -367,18 +386,24 @@ __device__ __forceinline__ void walk27(const GridBox& g, const uint32_t* __restr
 // (crates/vxl-phys-fluid/src/fluid_density.rs:24-51); boundary: rho = pmass_i w0 +
 // sum_fluid pmass_j W (fluid_density.rs:59-69). Writes (rho, p / rho^2) for the force
 // pass (the reference recomputes press/(rho*rho) per pair: same value).
+// Also records, in walk order, the slots of the neighbours that contributed (all of
+// them for fluid, fluid ones for boundary particles): nbr[k * n_total + s], k < cap,
+// and the full count in nbr_n[s] (a count above cap sends the consumers back to the walk).
 __global__ void __launch_bounds__(256) k_density(const float4* __restrict__ pos, const uint32_t* __restrict__ start,
                                                  const Ctl* __restrict__ ctl, float2* __restrict__ rc,
-                                                 float* __restrict__ press_out, SphConst k) {
+                                                 float* __restrict__ press_out, uint32_t* __restrict__ nbr,
+                                                 uint32_t* __restrict__ nbr_n, uint32_t cap, SphConst k) {
   uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= k.n_total) return;
   const GridBox g = ctl->grid;
+  const uint32_t nt = k.n_total;
   float4 pi = pos[s];
   bool fluid_i = pi.w > 0.0f;
   uint32_t cx, cy, cz;
   bin_of(g, pi.x, pi.y, pi.z, cx, cy, cz);
   float sum = fluid_i ? k.w0 : 0.0f;
   float sum_b = 0.0f;
+  uint32_t cnt = 0;
   const float h2 = k.h2, k6 = k.k6;
   walk27(g, start, cx, cy, cz, [&](uint32_t j) {
     if (j == s) return;
@@ -388,14 +413,22 @@ __global__ void __launch_bounds__(256) k_density(const float4* __restrict__ pos,
     if (r2 <= h2) {
       float t = h2 - r2;
       float w = k6 * t * t * t;
+      bool rec = true;
       if (fluid_i) {
         if (pj.w > 0.0f) sum += w;
         else sum_b += (-pj.w) * w;
       } else if (pj.w > 0.0f) {
         sum += pj.w * w;
+      } else {
+        rec = false;
+      }
+      if (rec) {
+        if (cnt < cap) nbr[(size_t)cnt * nt + s] = j;
+        ++cnt;
       }
     }
   });
+  nbr_n[s] = cnt;
   float rho = fluid_i ? (k.mass * sum + sum_b) : ((-pi.w) * k.w0 + sum);
   float p = tait(k, rho);
   rc[s] = make_float2(rho, p / (rho * rho));
@@ -405,19 +438,21 @@ __global__ void __launch_bounds__(256) k_density(const float4* __restrict__ pos,
 // Force (gravity + spiky pressure + Monaghan viscosity + XSPH, fluid_force.rs:165-214)
 // fused with integration (semi-implicit Euler + CFL clamp, fluid_step.rs:112-123) for
 // fluid slots; boundary slots are copied unchanged (kinematic within the tick).
+// Neighbours come from the density pass's list (same walk order, so the same sums);
+// a particle whose list overflowed walks the 27 cells again.
 // Reads the sorted buffer (pos, vel) and writes the integrated state to (pos_out, vel_out)
 // in the same slot order; accumulates the fluid AABB for the next substep's grid box.
 __global__ void __launch_bounds__(256) k_force(const float4* __restrict__ pos, const float4* __restrict__ vel,
                                                const float2* __restrict__ rc, const uint32_t* __restrict__ start,
-                                               Ctl* ctl, float4* __restrict__ pos_out, float4* __restrict__ vel_out,
-                                               float4* __restrict__ acc_out, float4* __restrict__ xsph_out,
-                                               SphConst k, StepConst st) {
+                                               const uint32_t* __restrict__ nbr, const uint32_t* __restrict__ nbr_n,
+                                               uint32_t cap, Ctl* ctl, float4* __restrict__ pos_out,
+                                               float4* __restrict__ vel_out, float4* __restrict__ acc_out,
+                                               float4* __restrict__ xsph_out, SphConst k, StepConst st) {
   uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
   bool valid = s < k.n_total;
   float nx = 0, ny = 0, nz = 0;
   bool fluid_i = false;
   if (valid) {
-    const GridBox g = ctl->grid;
     float4 pi = pos[s];
     float4 vi = vel[s];
     fluid_i = pi.w > 0.0f;
@@ -430,14 +465,7 @@ __global__ void __launch_bounds__(256) k_force(const float4* __restrict__ pos, c
       const float h = k.h, h2 = k.h2, ks = k.ks, k6 = k.k6, alpha_c = k.alpha_c, h001 = k.h001;
       float ax = k.gx, ay = k.gy, az = k.gz;
       float xx = 0.0f, xy = 0.0f, xz = 0.0f;
-      uint32_t cx, cy, cz;
-      bin_of(g, pi.x, pi.y, pi.z, cx, cy, cz);
-      walk27(g, start, cx, cy, cz, [&](uint32_t j) {
-        if (j == s) return;
-        float4 pj = pos[j];
-        float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
-        float r2 = dx * dx + dy * dy + dz * dz;
-        if (!(r2 <= h2)) return;
+      auto pair = [&](uint32_t j, float4 pj, float dx, float dy, float dz, float r2) {
         float2 rcj = rc[j];
         float4 vj = vel[j];
         const float rho_j = rcj.x, cj2 = rcj.y;
@@ -466,7 +494,29 @@ __global__ void __launch_bounds__(256) k_force(const float4* __restrict__ pos, c
         xx = xx + (vj.x - vi.x) * f;
         xy = xy + (vj.y - vi.y) * f;
         xz = xz + (vj.z - vi.z) * f;
-      });
+      };
+      const uint32_t cnt = nbr_n[s];
+      if (cnt <= cap) {
+        const uint32_t nt = k.n_total;
+        for (uint32_t q = 0; q < cnt; ++q) {
+          uint32_t j = nbr[(size_t)q * nt + s];
+          float4 pj = pos[j];
+          float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
+          float r2 = dx * dx + dy * dy + dz * dz;
+          pair(j, pj, dx, dy, dz, r2);
+        }
+      } else {
+        const GridBox g = ctl->grid;
+        uint32_t cx, cy, cz;
+        bin_of(g, pi.x, pi.y, pi.z, cx, cy, cz);
+        walk27(g, start, cx, cy, cz, [&](uint32_t j) {
+          if (j == s) return;
+          float4 pj = pos[j];
+          float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
+          float r2 = dx * dx + dy * dy + dz * dz;
+          if (r2 <= h2) pair(j, pj, dx, dy, dz, r2);
+        });
+      }
       if (acc_out) {
         acc_out[s] = make_float4(ax, ay, az, 0.0f);
         xsph_out[s] = make_float4(xx, xy, xz, 0.0f);
@@ -514,12 +564,14 @@ __device__ __forceinline__ float bforce_pair(const SphConst& k, float r2, float 
 
 // Reaction on each boundary particle j: the reference accumulates bforce[j] -= F_ij over
 // fluid i in ascending reference index (the outer loop of force_pass_serial). Here the
-// boundary particle gathers its fluid neighbours, orders them by reference index and
+// boundary particle takes its fluid neighbours (recorded by the density pass, or found by
+// walking the 27 cells when that list overflowed), orders them by reference index and
 // sums in that order, so the result is the same sum. Output in boundary order
 // (bforce[k], k = reference index - n_fluid).
 __global__ void __launch_bounds__(128) k_bforce(const float4* __restrict__ pos, const float4* __restrict__ vel,
                                                 const float2* __restrict__ rc, const uint32_t* __restrict__ start,
-                                                const uint32_t* __restrict__ orig, Ctl* ctl,
+                                                const uint32_t* __restrict__ orig, const uint32_t* __restrict__ nbr,
+                                                const uint32_t* __restrict__ nbr_n, uint32_t cap, Ctl* ctl,
                                                 float4* __restrict__ bforce, SphConst k) {
   uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= k.n_total) return;
@@ -536,12 +588,7 @@ __global__ void __launch_bounds__(128) k_bforce(const float4* __restrict__ pos, 
   uint32_t slot[kBGatherCap];
   int n = 0;
   bool overflow = false;
-  walk27(g, start, cx, cy, cz, [&](uint32_t i) {
-    float4 p = pos[i];
-    if (!(p.w > 0.0f)) return;
-    float dx = p.x - pj.x, dy = p.y - pj.y, dz = p.z - pj.z;
-    float r2 = dx * dx + dy * dy + dz * dz;
-    if (!(r2 <= h2)) return;
+  auto insert = [&](uint32_t i) {
     if (n < kBGatherCap) {
       uint32_t o = orig[i];
       int q = n++;
@@ -555,7 +602,20 @@ __global__ void __launch_bounds__(128) k_bforce(const float4* __restrict__ pos, 
     } else {
       overflow = true;
     }
-  });
+  };
+  const uint32_t cnt = nbr_n[s];
+  if (cnt <= cap) {
+    for (uint32_t q = 0; q < cnt; ++q) insert(nbr[(size_t)q * k.n_total + s]);
+  } else {
+    walk27(g, start, cx, cy, cz, [&](uint32_t i) {
+      float4 p = pos[i];
+      if (!(p.w > 0.0f)) return;
+      float dx = p.x - pj.x, dy = p.y - pj.y, dz = p.z - pj.z;
+      float r2 = dx * dx + dy * dy + dz * dz;
+      if (!(r2 <= h2)) return;
+      insert(i);
+    });
+  }
   float bx = 0.0f, by = 0.0f, bz = 0.0f;
   auto apply = [&](uint32_t i) {
     float4 p = pos[i];
@@ -571,7 +631,7 @@ __global__ void __launch_bounds__(128) k_bforce(const float4* __restrict__ pos, 
     for (int q = 0; q < n; ++q) apply(slot[q]);
   } else {
     // Slow path: visit fluid neighbours in ascending reference index by repeated
-    // minimum search (O(neighbours x candidates)); reported through the info flag.
+    // minimum search (O(neighbours x candidates)); counted in ctl->slow_gathers.
     atomicAdd(&ctl->slow_gathers, 1u);
     uint32_t last = 0;
     bool first = true;
@@ -599,20 +659,32 @@ __global__ void __launch_bounds__(128) k_bforce(const float4* __restrict__ pos, 
 }
 
 // Per-span force and torque about the body origin (fluid_boundary.rs:10-28), added to
-// the tick accumulator. One block per span, fixed-shape reduction: thread t sums
-// k = t, t + blockDim, ... in order, then a fixed tree; deterministic run to run.
+// the tick accumulator. Fixed-shape two-level reduction, deterministic run to run:
+// level 1, one block per chunk of <= kReactChunk consecutive particles of a span
+// (thread t sums t, t + blockDim, ... in order, then a fixed tree); level 2, one thread
+// per span adds its chunk partials in chunk order.
 struct SpanDev {
   uint32_t body;
   float ox, oy, oz;
   uint32_t start, end;
 };
 
-__global__ void __launch_bounds__(512) k_reactions(const float4* __restrict__ bforce, const float4* __restrict__ bpos,
-                                                   const SpanDev* __restrict__ spans, float* __restrict__ breact,
-                                                   uint32_t n_fluid) {
-  const SpanDev sp = spans[blockIdx.x];
+struct SpanChunk {
+  uint32_t span, begin, end, pad;
+};
+
+constexpr uint32_t kReactChunk = 4096;
+constexpr int kReactThreads = 256;
+
+__global__ void __launch_bounds__(kReactThreads) k_react_chunks(const float4* __restrict__ bforce,
+                                                                const float4* __restrict__ bpos,
+                                                                const SpanDev* __restrict__ spans,
+                                                                const SpanChunk* __restrict__ chunks,
+                                                                float* __restrict__ partial, uint32_t n_fluid) {
+  const SpanChunk ch = chunks[blockIdx.x];
+  const SpanDev sp = spans[ch.span];
   float f[6] = {0, 0, 0, 0, 0, 0};
-  for (uint32_t kk = sp.start + threadIdx.x; kk < sp.end; kk += blockDim.x) {
+  for (uint32_t kk = ch.begin + threadIdx.x; kk < ch.end; kk += kReactThreads) {
     float4 fk = bforce[kk - n_fluid];
     float4 p = bpos[kk - n_fluid];
     float rx = p.x - sp.ox, ry = p.y - sp.oy, rz = p.z - sp.oz;
@@ -623,16 +695,26 @@ __global__ void __launch_bounds__(512) k_reactions(const float4* __restrict__ bf
     f[4] = f[4] + (rz * fk.x - rx * fk.z);
     f[5] = f[5] + (rx * fk.y - ry * fk.x);
   }
-  __shared__ float sh[6][512];
+  __shared__ float sh[6][kReactThreads];
   for (int a = 0; a < 6; ++a) sh[a][threadIdx.x] = f[a];
   __syncthreads();
-  for (uint32_t w = blockDim.x / 2; w > 0; w >>= 1) {
+  for (uint32_t w = kReactThreads / 2; w > 0; w >>= 1) {
     if (threadIdx.x < w)
       for (int a = 0; a < 6; ++a) sh[a][threadIdx.x] = sh[a][threadIdx.x] + sh[a][threadIdx.x + w];
     __syncthreads();
   }
-  if (threadIdx.x == 0)
-    for (int a = 0; a < 6; ++a) breact[6 * blockIdx.x + a] = breact[6 * blockIdx.x + a] + sh[a][0];
+  if (threadIdx.x < 6) partial[6 * blockIdx.x + threadIdx.x] = sh[threadIdx.x][0];
+}
+
+// chunk_first[q] .. chunk_first[q + 1]: the chunks of span q (in order).
+__global__ void k_react_spans(const float* __restrict__ partial, const uint32_t* __restrict__ chunk_first,
+                              float* __restrict__ breact, uint32_t nspans) {
+  uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= nspans) return;
+  float f[6] = {0, 0, 0, 0, 0, 0};
+  for (uint32_t c = chunk_first[q]; c < chunk_first[q + 1]; ++c)
+    for (int a = 0; a < 6; ++a) f[a] = f[a] + partial[6 * c + a];
+  for (int a = 0; a < 6; ++a) breact[6 * q + a] = breact[6 * q + a] + f[a];
 }
 
 // Tick average (fluid_step.rs:84-88): e *= 1 / substeps.
