@@ -359,22 +359,39 @@ __global__ void k_canon(const uint2* __restrict__ items, const uint32_t* __restr
   }
 }
 
-// Walk the 27 cells of (cx, cy, cz) in the reference order (dz outer, dy, dx inner;
-// crates/vxl-phys-fluid/src/grid.rs:123-153), calling f(j) for every slot j in them.
+// Walk the 27 cells around position p (cell (cx, cy, cz)) in the reference order
+// (dz outer, dy, dx inner; crates/vxl-phys-fluid/src/grid.rs:123-153), calling f(j) for
+// every slot j in them — except cells whose nominal box lies farther than h from p.
+// Such a cell holds no particle with r2 <= h2, so skipping it changes neither the set nor
+// the order of accepted neighbours. The test is conservative: per-axis gaps to the
+// neighbouring cell faces are clamped at 0 and compared with (h + bin/1024)^2, a margin
+// far above the f32 rounding of cell faces and bin assignment.
 template <class F>
-__device__ __forceinline__ void walk27(const GridBox& g, const uint32_t* __restrict__ start, uint32_t cx,
-                                       uint32_t cy, uint32_t cz, F&& f) {
+__device__ __forceinline__ void walk27(const GridBox& g, const uint32_t* __restrict__ start, float px, float py,
+                                       float pz, uint32_t cx, uint32_t cy, uint32_t cz, float h, F&& f) {
+  const float lx = g.minx + (float)cx * g.bin, ly = g.miny + (float)cy * g.bin, lz = g.minz + (float)cz * g.bin;
+  const float gxl = fmaxf(px - lx, 0.0f), gxr = fmaxf(lx + g.bin - px, 0.0f);
+  const float gyl = fmaxf(py - ly, 0.0f), gyr = fmaxf(ly + g.bin - py, 0.0f);
+  const float gzl = fmaxf(pz - lz, 0.0f), gzr = fmaxf(lz + g.bin - pz, 0.0f);
+  const float reach = h + g.bin * (1.0f / 1024.0f);
+  const float reach2 = reach * reach;
   for (int dz = -1; dz <= 1; ++dz) {
-    int z = (int)cz + dz;
+    const int z = (int)cz + dz;
     if (z < 0 || z >= (int)g.nz) continue;
+    const float gz = dz < 0 ? gzl : (dz > 0 ? gzr : 0.0f);
+    const float dz2 = gz * gz;
     for (int dy = -1; dy <= 1; ++dy) {
-      int y = (int)cy + dy;
+      const int y = (int)cy + dy;
       if (y < 0 || y >= (int)g.ny) continue;
+      const float gy = dy < 0 ? gyl : (dy > 0 ? gyr : 0.0f);
+      const float dyz2 = dz2 + gy * gy;
       for (int dx = -1; dx <= 1; ++dx) {
-        int x = (int)cx + dx;
+        const int x = (int)cx + dx;
         if (x < 0 || x >= (int)g.nx) continue;
-        uint32_t idx = ((uint32_t)x * g.ny + (uint32_t)y) * g.nz + (uint32_t)z;
-        uint32_t j1 = start[idx + 1];
+        const float gx = dx < 0 ? gxl : (dx > 0 ? gxr : 0.0f);
+        if (dyz2 + gx * gx > reach2) continue;
+        const uint32_t idx = ((uint32_t)x * g.ny + (uint32_t)y) * g.nz + (uint32_t)z;
+        const uint32_t j1 = start[idx + 1];
         for (uint32_t j = start[idx]; j < j1; ++j) f(j);
       }
     }
@@ -389,7 +406,7 @@ __device__ __forceinline__ void walk27(const GridBox& g, const uint32_t* __restr
 // Also records, in walk order, the slots of the neighbours that contributed (all of
 // them for fluid, fluid ones for boundary particles): nbr[k * n_total + s], k < cap,
 // and the full count in nbr_n[s] (a count above cap sends the consumers back to the walk).
-__global__ void __launch_bounds__(256) k_density(const float4* __restrict__ pos, const uint32_t* __restrict__ start,
+__global__ void __launch_bounds__(256, 6) k_density(const float4* __restrict__ pos, const uint32_t* __restrict__ start,
                                                  const Ctl* __restrict__ ctl, float2* __restrict__ rc,
                                                  float* __restrict__ press_out, uint32_t* __restrict__ nbr,
                                                  uint32_t* __restrict__ nbr_n, uint32_t cap, SphConst k) {
@@ -405,7 +422,7 @@ __global__ void __launch_bounds__(256) k_density(const float4* __restrict__ pos,
   float sum_b = 0.0f;
   uint32_t cnt = 0;
   const float h2 = k.h2, k6 = k.k6;
-  walk27(g, start, cx, cy, cz, [&](uint32_t j) {
+  walk27(g, start, pi.x, pi.y, pi.z, cx, cy, cz, k.h, [&](uint32_t j) {
     if (j == s) return;
     float4 pj = pos[j];
     float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
@@ -509,7 +526,7 @@ __global__ void __launch_bounds__(256) k_force(const float4* __restrict__ pos, c
         const GridBox g = ctl->grid;
         uint32_t cx, cy, cz;
         bin_of(g, pi.x, pi.y, pi.z, cx, cy, cz);
-        walk27(g, start, cx, cy, cz, [&](uint32_t j) {
+        walk27(g, start, pi.x, pi.y, pi.z, cx, cy, cz, k.h, [&](uint32_t j) {
           if (j == s) return;
           float4 pj = pos[j];
           float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
@@ -607,7 +624,7 @@ __global__ void __launch_bounds__(128) k_bforce(const float4* __restrict__ pos, 
   if (cnt <= cap) {
     for (uint32_t q = 0; q < cnt; ++q) insert(nbr[(size_t)q * k.n_total + s]);
   } else {
-    walk27(g, start, cx, cy, cz, [&](uint32_t i) {
+    walk27(g, start, pj.x, pj.y, pj.z, cx, cy, cz, k.h, [&](uint32_t i) {
       float4 p = pos[i];
       if (!(p.w > 0.0f)) return;
       float dx = p.x - pj.x, dy = p.y - pj.y, dz = p.z - pj.z;
@@ -637,7 +654,7 @@ __global__ void __launch_bounds__(128) k_bforce(const float4* __restrict__ pos, 
     bool first = true;
     for (;;) {
       uint32_t best = 0xffffffffu, best_slot = 0;
-      walk27(g, start, cx, cy, cz, [&](uint32_t i) {
+      walk27(g, start, pj.x, pj.y, pj.z, cx, cy, cz, k.h, [&](uint32_t i) {
         float4 p = pos[i];
         if (!(p.w > 0.0f)) return;
         uint32_t o = orig[i];
