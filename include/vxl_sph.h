@@ -227,6 +227,31 @@ vxl_status vxl_sph_set_profile(vxl_sph_handle* h, int on);
 vxl_status vxl_sph_profile_read(vxl_sph_handle* h, uint32_t k, const char** name, double* total_ms,
                                 uint64_t* launches);
 
+/* Neighbour-table build that allocates nothing. No counterpart in the reference: it is
+ * for callers that cannot allocate device memory while they run — an engine that
+ * reserves one fixed arena for all GPU work at start-up and forbids further cudaMalloc,
+ * or a per-frame plugin that must not call cudaMalloc/cudaFree because both can
+ * synchronise the device and stall its frame loop.
+ *
+ * Builds, on the current device, the same table a substep builds (cell keys by the
+ * reference's grid rule, particles grouped by cell in ascending index): d_pos_xyz is
+ * 3*n floats of device memory; d_items receives n particle indices; d_start receives
+ * total+1 slot offsets and must hold max_bins+1 entries; *info (host memory) receives
+ * the grid. Work runs on cuda_stream (a cudaStream_t, or NULL) and the call returns
+ * after it has finished.
+ *
+ * Limits: n <= 524,288 particles and max_bins <= 524,288 cells (0 means 524,288);
+ * larger sizes return VXL_INVALID_ARGUMENT. Working memory is one fixed array of about
+ * 8.4 MB inside the library, held by every GPU that loads it until the process exits;
+ * the call makes no cudaMalloc, cudaFree or other allocating call. The first call on a
+ * device looks the array's address up (cudaGetSymbolAddress): make that first call
+ * before any stream capture on that device. Every call reuses the same array (the
+ * counts it needs zeroed are cleared at the start of each call), so calls that overlap
+ * on the GPU — from two streams or two host threads — race and must not be made. */
+vxl_status vxl_sph_build_grid_static(const float* d_pos_xyz, uint32_t n, float h, uint32_t max_bins,
+                                     uint32_t* d_items, uint32_t* d_start, uint64_t start_cap,
+                                     vxl_sph_grid_info* info, void* cuda_stream);
+
 #ifdef __cplusplus
 }
 #endif

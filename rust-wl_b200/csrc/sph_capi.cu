@@ -68,6 +68,8 @@ inline uint32_t blocks_for(uint64_t n, int t = kThreads) { return (uint32_t)((n 
 
 }  // namespace
 
+void vxl_set_last_error(const char* msg) { g_last_error = msg ? msg : ""; }
+
 struct vxl_sph_handle {
   int device = 0;
   cudaStream_t stream = nullptr;      // stream all work is enqueued on

@@ -25,3 +25,6 @@ inline float vxl_o2f_host(uint32_t o) {
   std::memcpy(&f, &u, 4);
   return f;
 }
+
+// Sets the thread-local message returned by vxl_sph_last_error() (defined in sph_capi.cu).
+void vxl_set_last_error(const char* msg);

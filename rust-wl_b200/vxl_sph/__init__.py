@@ -136,6 +136,8 @@ SIGNATURES = {
     "vxl_sph_set_profile": (C.c_int, [_H, C.c_int]),
     "vxl_sph_profile_read": (C.c_int, [_H, C.c_uint32, C.POINTER(C.c_char_p), C.POINTER(C.c_double),
                                        C.POINTER(C.c_uint64)]),
+    "vxl_sph_build_grid_static": (C.c_int, [C.c_void_p, C.c_uint32, C.c_float, C.c_uint32, C.c_void_p, C.c_void_p,
+                                            C.c_uint64, C.POINTER(GridInfo), C.c_void_p]),
 }
 
 _lib = None

@@ -18,7 +18,7 @@ CSRC = PKG / "csrc"
 LIB_DIR = PKG / "lib"
 LIB = LIB_DIR / "libvxl_sph.so"
 
-SOURCES = ["sph_capi.cu", "lattice.cpp"]
+SOURCES = ["sph_capi.cu", "lattice.cpp", "sph_static_grid.cu"]
 HEADERS = ["sph_device.cuh", "sph_kernels.cuh", "vxl_sph_internal.h"]
 
 NVCC_FLAGS = [
