@@ -57,6 +57,19 @@ def substep_bytes(nf: int, nb: int, cells: int) -> float:
     return 116.0 * (nf + nb) + 72.0 * nf + 40.0 * nb + 8.0 * cells
 
 
+def ncu_traffic(kernel: str, workload: str):
+    """DRAM bytes per launch of `kernel` on `workload` from the committed ncu summary."""
+    p = ROOT / "profiles" / "roofline_traffic.txt"
+    try:
+        for line in p.read_text().splitlines():
+            f = line.split()
+            if len(f) >= 3 and not line.startswith("#") and f[0] == kernel and f[1] == workload:
+                return float(f[2])
+    except OSError:
+        pass
+    return None
+
+
 def hbm_peak() -> tuple[float, str]:
     p = ROOT / "MEASURED_PEAKS.json"
     try:
@@ -256,7 +269,8 @@ def run_ours(args) -> None:
     avg_ms = dom_ms / max(dom_n, 1)
     achieved = (bytes_launch / (avg_ms / 1e3) / 1e9) if bytes_launch else None
     roofline = {"kernel": dom_name, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": (achieved / peak) if achieved else None, "traffic": None,
+                "frac": (achieved / peak) if achieved else None,
+                "traffic": ncu_traffic(dom_name, spec.name),
                 "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
                 else "fallback 6650 GB/s",
                 "avg_launch_ms": avg_ms, "launches": dom_n, "share": dom_ms / prof_total if prof_total else None,
