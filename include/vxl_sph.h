@@ -227,6 +227,101 @@ vxl_status vxl_sph_set_profile(vxl_sph_handle* h, int on);
 vxl_status vxl_sph_profile_read(vxl_sph_handle* h, uint32_t k, const char** name, double* total_ms,
                                 uint64_t* launches);
 
+/* ------------------------------------------------------------------ batched form
+ * One handle can hold many independent scenes: they are packed
+ * into one particle pool and stepped together, one launch per kernel per substep for
+ * all scenes, with each scene's own constants and grid (a segmented sort on
+ * scene-offset cell keys) and the particle passes run as persistent kernels over a
+ * (scene, tile) work list. No counterpart in the reference (its GPU tier steps one
+ * Packet); each scene's results equal a plain handle's for the same inputs. */
+
+/* Create a handle holding n scenes (descs[i] as for vxl_sph_create; all on `device`;
+ * all must share `substeps` to be stepped by vxl_sph_step_tick). cell_capacity bounds
+ * the sum of the scenes' cells per substep (0 = the sum of their max_bins, capped at
+ * 2^28); a substep that would exceed it is skipped and reported as
+ * VXL_DEVICE_FAULT_FLAG. */
+vxl_status vxl_sph_create_batch(const vxl_sph_desc* descs, uint32_t n, int32_t device, uint64_t cell_capacity,
+                                vxl_sph_handle** out);
+uint32_t vxl_sph_scene_count(vxl_sph_handle* h);
+
+/* Per-scene variants of the plain calls (scene-local particle indices). */
+vxl_status vxl_sph_read_state_scene(vxl_sph_handle* h, uint32_t scene, float* pos_xyz, float* vel_xyz);
+vxl_status vxl_sph_write_state_scene(vxl_sph_handle* h, uint32_t scene, const float* pos_xyz, const float* vel_xyz);
+vxl_status vxl_sph_upload_boundary_scene(vxl_sph_handle* h, uint32_t scene, const float* pos_xyz,
+                                         const float* vel_xyz, uint64_t nb);
+vxl_status vxl_sph_set_spans_scene(vxl_sph_handle* h, uint32_t scene, const vxl_sph_span* spans, uint32_t nspans);
+vxl_status vxl_sph_export_grid_scene(vxl_sph_handle* h, uint32_t scene, uint32_t* items, uint32_t* start,
+                                     uint64_t start_cap, uint32_t* bins, vxl_sph_grid_info* info);
+vxl_status vxl_sph_read_fields_scene(vxl_sph_handle* h, uint32_t scene, float* dens, float* press,
+                                     float* acc_xyz, float* xsph_xyz, float* bforce_xyz);
+/* Reactions of every span of every scene from the last tick, in scene order then span
+ * order; *n receives the count (call with cap = 0 to size). */
+vxl_status vxl_sph_reactions_all(vxl_sph_handle* h, vxl_sph_reaction* out, uint32_t cap, uint32_t* n);
+
+/* Launch shape of the particle passes: threads per block (128 or 256), slots per work
+ * item of the persistent passes (multiple of 128) and persistent blocks per SM (as a
+ * multiple of the occupancy limit). */
+typedef struct vxl_sph_tuning {
+  vxl_block_header hdr;
+  uint32_t block;
+  uint32_t tile;
+  uint32_t waves;
+  float ms_per_substep; /* filled by vxl_sph_autotune: device time of the chosen shape */
+} vxl_sph_tuning;
+vxl_status vxl_sph_set_tuning(vxl_sph_handle* h, const vxl_sph_tuning* t);
+vxl_status vxl_sph_get_tuning(vxl_sph_handle* h, vxl_sph_tuning* t);
+/* Autotuner: times every candidate shape on the handle's own scenes (`trials` substeps
+ * each, from a snapshot of the state that is restored afterwards) and keeps the fastest.
+ * Results are identical for every shape; only the time differs. */
+vxl_status vxl_sph_autotune(vxl_sph_handle* h, float dt_tick, uint32_t trials, vxl_sph_tuning* best);
+
+/* ------------------------------------------------------------------ served form
+ * A request loop: scene-step requests are submitted at any time,
+ * admitted while their device footprint fits an HBM budget, stepped together with
+ * every other admitted scene, and retired when their tick count is reached; the set of
+ * scenes is repacked at substep boundaries (admission and retirement happen between
+ * substeps, so a request admitted while others run starts on the next substep). No
+ * counterpart in the reference. Scene state stays on the device from admission to
+ * retirement; a retired scene's final state is kept on the host for vxl_sph_serve_read. */
+typedef struct vxl_sph_server vxl_sph_server;
+
+typedef struct vxl_sph_request_status {
+  vxl_block_header hdr;
+  uint32_t state;        /* 0 queued, 1 running, 2 done, 3 rejected */
+  uint32_t ticks_done;
+  uint32_t ticks_total;
+  uint32_t pad;
+  double submit_s;       /* host clock (seconds since the server was created) */
+  double admit_s;
+  double done_s;
+  double tick_p50_ms;    /* wall time per tick of this request while it ran */
+  double tick_p99_ms;
+} vxl_sph_request_status;
+
+typedef struct vxl_sph_serve_report {
+  vxl_block_header hdr;
+  uint32_t active;       /* scenes stepped by this call */
+  uint32_t queued;
+  uint32_t admitted;     /* admitted before this substep */
+  uint32_t retired;      /* retired before this substep */
+  uint64_t particles;    /* fluid particles advanced by this substep */
+  uint64_t device_bytes_in_use;
+} vxl_sph_serve_report;
+
+/* budget_bytes: device memory the scenes may use (particle slots and cells);
+ * max_scenes: scene table size. */
+vxl_status vxl_sph_serve_create(int32_t device, uint64_t budget_bytes, uint32_t max_scenes, vxl_sph_server** out);
+vxl_status vxl_sph_serve_destroy(vxl_sph_server* s);
+/* Queue one request: a scene (copied) to be stepped `ticks` ticks of desc->params.substeps
+ * substeps each. Rejected (state 3, VXL_OUT_OF_MEMORY) if it can never fit the budget. */
+vxl_status vxl_sph_serve_submit(vxl_sph_server* s, const vxl_sph_desc* desc, uint32_t ticks, uint64_t* out_id);
+/* Retire finished scenes, admit queued ones that fit, then advance every admitted scene by
+ * one substep of its own dt = dt_tick / substeps. Synchronous. */
+vxl_status vxl_sph_serve_step(vxl_sph_server* s, float dt_tick, vxl_sph_serve_report* report);
+vxl_status vxl_sph_serve_poll(vxl_sph_server* s, uint64_t id, vxl_sph_request_status* out);
+/* Positions/velocities of a running or finished request (scene-local order). */
+vxl_status vxl_sph_serve_read(vxl_sph_server* s, uint64_t id, float* pos_xyz, float* vel_xyz);
+
 /* Neighbour-table build that allocates nothing. No counterpart in the reference: it is
  * for callers that cannot allocate device memory while they run — an engine that
  * reserves one fixed arena for all GPU work at start-up and forbids further cudaMalloc,

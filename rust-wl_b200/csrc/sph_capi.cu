@@ -1,459 +1,46 @@
-// C ABI of the plain (single-scene) WCSPH step: resident device state, the substep
-// launch sequence, CUDA-graph replay of whole ticks, and the export paths.
+// C ABI of the WCSPH step (include/vxl_sph.h): the plain drop-in handle and its batched
+// multi-scene form. A handle is an Engine (sph_engine.h); the plain form is an engine
+// holding one scene.
 //
 // Reference seam: FluidStepper (crates/vxl-phys-core/src/interop.rs:293-316) as
 // implemented by GpuFluidStepper (crates/vxl-phys-gpu/src/pipeline/stepper.rs:22-147).
 #include <algorithm>
 #include <cmath>
-#include <cstdio>
-#include <cstdlib>
 #include <cstring>
 #include <new>
 #include <string>
 #include <vector>
 
-#include "sph_kernels.cuh"
+#include "sph_engine.h"
 #include "vxl_sph.h"
 #include "vxl_sph_internal.h"
 
-using namespace vxl;
-
-namespace {
-
-thread_local std::string g_last_error;
-
-vxl_status fail(vxl_status s, const std::string& msg) {
-  g_last_error = msg;
-  return s;
-}
-
-#define CU(call)                                                                              \
-  do {                                                                                        \
-    cudaError_t e_ = (call);                                                                  \
-    if (e_ != cudaSuccess)                                                                    \
-      return fail(VXL_CUDA_ERROR, std::string(#call) + ": " + cudaGetErrorString(e_));       \
-  } while (0)
-
-constexpr int kThreads = 256;
-
-// VXL_SPH_DEBUG=1: report, on stderr, any CUDA runtime error left pending at the entry
-// or exit of a public call (attributes a sticky error to the call that caused it).
-bool debug_on() {
-  static int on = -1;
-  if (on < 0) {
-    const char* e = std::getenv("VXL_SPH_DEBUG");
-    on = (e && e[0] == '1') ? 1 : 0;
-  }
-  return on == 1;
-}
-
-struct ApiTrace {
-  const char* fn;
-  explicit ApiTrace(const char* f) : fn(f) {
-    if (debug_on()) {
-      cudaError_t e = cudaPeekAtLastError();
-      if (e != cudaSuccess) std::fprintf(stderr, "[vxl_sph] pending at entry of %s: %s\n", fn, cudaGetErrorString(e));
-    }
-  }
-  ~ApiTrace() {
-    if (debug_on()) {
-      cudaError_t e = cudaPeekAtLastError();
-      if (e != cudaSuccess) std::fprintf(stderr, "[vxl_sph] pending at exit of %s: %s\n", fn, cudaGetErrorString(e));
-    }
-  }
-};
-#define API_TRACE() ApiTrace api_trace_(__func__)
-
-inline uint32_t blocks_for(uint64_t n, int t = kThreads) { return (uint32_t)((n + t - 1) / t); }
-
-}  // namespace
-
-void vxl_set_last_error(const char* msg) { g_last_error = msg ? msg : ""; }
+using vxl::Engine;
+using vxl::set_error;
 
 struct vxl_sph_handle {
-  int device = 0;
-  cudaStream_t stream = nullptr;      // stream all work is enqueued on
-  cudaStream_t own_stream = nullptr;  // the handle's own stream (destroyed with it)
-  vxl_sph_params params{};
-  SphConst k{};
-  uint64_t nf = 0, nb = 0, nt = 0;
-  uint32_t max_bins = 0;
-  uint32_t substeps = 1;
-
-  float4* pos[2] = {nullptr, nullptr};
-  float4* vel[2] = {nullptr, nullptr};
-  uint32_t* orig = nullptr;
-  uint32_t* slot_of = nullptr;
-  uint2* cellrank = nullptr;
-  uint2* items = nullptr;
-  uint32_t* counts = nullptr;
-  uint32_t* start = nullptr;
-  uint32_t* partial = nullptr;
-  float2* rc = nullptr;
-  float* press = nullptr;
-  float4* acc = nullptr;
-  float4* xsph = nullptr;
-  float4* bforce = nullptr;
-  float4* bpos = nullptr;
-  uint32_t* nbr = nullptr;    // neighbour list, nbr[k * nt + s], k < nbr_cap
-  uint32_t* nbr_n = nullptr;  // neighbour count per slot
-  uint32_t nbr_cap = 64;
-  Ctl* ctl = nullptr;
-  float* stage = nullptr;  // 8 * nt floats: device staging for host uploads/exports
-  SpanDev* spans_d = nullptr;
-  SpanDev* spans_h = nullptr;  // pinned
-  uint32_t spans_cap = 0;
-  float* breact_d = nullptr;
-  float* breact_h = nullptr;  // pinned
-  SpanChunk* chunks_d = nullptr;
-  SpanChunk* chunks_h = nullptr;  // pinned
-  uint32_t* chunk_first_d = nullptr;
-  uint32_t* chunk_first_h = nullptr;  // pinned
-  float* react_partial = nullptr;
-  uint32_t chunks_cap = 0;
-  uint32_t nchunks = 0;
-  uint32_t graph_nchunks = 0;
-  Ctl* ctl_h = nullptr;       // pinned
-  bool record = false;
-  bool ran_substep = false;
-
-  cudaGraphExec_t graph = nullptr;
-  float graph_dt = 0.f;
-  uint32_t graph_nspans = 0;
-  bool graph_record = false;
-  bool use_graph = true;
-  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-  uint64_t launches_last_tick = 0;
-  uint64_t launches_counter = 0;
-  uint64_t device_bytes = 0;
-  uint32_t last_nspans = 0;
-
-  // per-kernel device timers (vxl_sph_set_profile)
-  bool prof = false;
-  bool capturing = false;  // inside cudaStreamBeginCapture .. EndCapture
-  bool graph_prof = false;
-  bool prof_pending = false;
-  std::vector<cudaEvent_t> prof_ev;
-  std::vector<int> prof_kid;
-  size_t prof_used = 0;
-  double prof_ms[16] = {};
-  uint64_t prof_n[16] = {};
+  Engine* e = nullptr;
+  std::vector<vxl_sph_reaction> last;  // reactions of the last synced tick
+  uint32_t last_nspans = 0;            // spans of scene 0 in the last enqueued tick
 };
 
 namespace {
-
-template <class T>
-vxl_status dalloc(vxl_sph_handle* h, T** p, size_t count) {
-  size_t bytes = count * sizeof(T);
-  if (bytes == 0) bytes = sizeof(T);
-  cudaError_t e = cudaMalloc((void**)p, bytes);
-  if (e != cudaSuccess) {
-    *p = nullptr;
-    return fail(VXL_OUT_OF_MEMORY, std::string("cudaMalloc: ") + cudaGetErrorString(e));
-  }
-  h->device_bytes += bytes;
-  return VXL_OK;
-}
-
-void free_all(vxl_sph_handle* h) {
-  if (h->graph) cudaGraphExecDestroy(h->graph);
-  void* ptrs[] = {h->pos[0], h->pos[1], h->vel[0], h->vel[1], h->orig, h->slot_of, h->cellrank, h->items,
-                  h->counts, h->start, h->partial, h->rc, h->press, h->acc, h->xsph, h->bforce, h->bpos,
-                  h->ctl, h->stage, h->spans_d, h->breact_d, h->nbr, h->nbr_n, h->chunks_d,
-                  h->chunk_first_d, h->react_partial};
-  for (void* p : ptrs)
-    if (p) cudaFree(p);
-  if (h->spans_h) cudaFreeHost(h->spans_h);
-  if (h->breact_h) cudaFreeHost(h->breact_h);
-  if (h->chunks_h) cudaFreeHost(h->chunks_h);
-  if (h->chunk_first_h) cudaFreeHost(h->chunk_first_h);
-  if (h->ctl_h) cudaFreeHost(h->ctl_h);
-  if (h->ev0) cudaEventDestroy(h->ev0);
-  if (h->ev1) cudaEventDestroy(h->ev1);
-  for (cudaEvent_t e : h->prof_ev) cudaEventDestroy(e);
-  if (h->own_stream) cudaStreamDestroy(h->own_stream);
-}
-
-// Kernel names of the per-kernel timer table (index = id).
-enum KernelId : int {
-  KID_GRIDBOX, KID_KEYS, KID_SCAN_PARTIAL, KID_SCAN_TOP, KID_SCAN_FINAL, KID_PLACE, KID_CANON,
-  KID_DENSITY, KID_FORCE, KID_BFORCE, KID_REACT_CHUNKS, KID_REACT_SPANS, KID_SCALE, KID_COUNT
-};
-const char* const kKernelNames[KID_COUNT] = {
-  "k_gridbox", "k_keys", "k_scan_partial", "k_scan_top", "k_scan_final", "k_place", "k_canon",
-  "k_density", "k_force", "k_bforce", "k_react_chunks", "k_react_spans", "k_scale"};
-
-// Inside stream capture a plain cudaEventRecord only expresses a dependency; the
-// External flag makes the graph record the event each time it runs.
-void record_event(vxl_sph_handle* h, cudaEvent_t e) {
-  if (h->capturing) cudaEventRecordWithFlags(e, h->stream, cudaEventRecordExternal);
-  else cudaEventRecord(e, h->stream);
-}
-
-int prof_begin(vxl_sph_handle* h, int kid) {
-  if (!h->prof) return -1;
-  if (2 * h->prof_used + 2 > h->prof_ev.size()) {
-    for (int q = 0; q < 64; ++q) {
-      cudaEvent_t e;
-      cudaEventCreate(&e);
-      h->prof_ev.push_back(e);
-    }
-    h->prof_kid.resize(h->prof_ev.size() / 2);
-  }
-  size_t i = h->prof_used++;
-  h->prof_kid[i] = kid;
-  record_event(h, h->prof_ev[2 * i]);
-  return (int)i;
-}
-
-void prof_end(vxl_sph_handle* h, int i) {
-  if (i >= 0) record_event(h, h->prof_ev[2 * i + 1]);
-}
-
-// Add the elapsed times of the last enqueued tick (waits for it).
-void prof_collect(vxl_sph_handle* h) {
-  if (!h->prof_pending) return;
-  cudaStreamSynchronize(h->stream);
-  for (size_t i = 0; i < h->prof_used; ++i) {
-    float ms = 0.f;
-    cudaError_t e = cudaEventElapsedTime(&ms, h->prof_ev[2 * i], h->prof_ev[2 * i + 1]);
-    if (e == cudaSuccess) {
-      h->prof_ms[h->prof_kid[i]] += ms;
-      h->prof_n[h->prof_kid[i]] += 1;
-    } else {
-      if (debug_on()) std::fprintf(stderr, "[vxl_sph] cudaEventElapsedTime(%zu): %s\n", i, cudaGetErrorString(e));
-      cudaGetLastError();  // the timer pair is dropped; do not leave the error pending
-    }
-  }
-  h->prof_pending = false;
-}
-
-#define LAUNCH(kid, ...)                 \
-  do {                                   \
-    int pe_ = prof_begin(h, kid);        \
-    __VA_ARGS__;                         \
-    prof_end(h, pe_);                    \
-    h->launches_counter += 1;            \
-  } while (0)
 
 bool check_header(const vxl_block_header& hd, uint32_t size) {
   return hd.size == size && hd.version == VXL_SPH_ABI_VERSION;
 }
 
-// crates/vxl-phys-fluid/src/fluid_access.rs:8-13: h, h2, k6, ks, w0, B in f32 with the
-// reference's operation order (host code is built with -ffp-contract=off).
-SphConst make_const(const vxl_sph_params& p, uint64_t nf, uint64_t nt, uint32_t max_bins) {
-  SphConst k{};
-  float h = std::fmax(p.smoothing_radius, 1e-5f);
-  float h2 = h * h;
-  const float pi = 3.14159265358979323846f;
-  k.h = h;
-  k.h2 = h2;
-  k.k6 = 315.0f / (64.0f * pi * vxl_powi(h, 9));
-  k.ks = 45.0f / (pi * vxl_powi(h, 6));
-  k.w0 = k.k6 * h2 * h2 * h2;
-  k.b_tait = p.sound_speed * p.sound_speed * p.rest_density / p.gamma_tait;
-  k.mass = p.particle_mass;
-  k.rho0 = p.rest_density;
-  k.gamma = p.gamma_tait;
-  k.eps = p.xsph_viscosity;
-  k.alpha_c = p.artificial_viscosity * p.sound_speed;
-  k.h001 = 0.01f * h2;
-  k.gx = p.gravity[0];
-  k.gy = p.gravity[1];
-  k.gz = p.gravity[2];
-  k.clamp_p = p.tensile_instability_suppression ? 1u : 0u;
-  k.gamma7 = std::fabs(p.gamma_tait - 7.0f) < 1e-6f ? 1u : 0u;
-  k.n_fluid = (uint32_t)nf;
-  k.n_total = (uint32_t)nt;
-  k.max_bins = max_bins;
-  return k;
-}
-
-// Launch one substep (crates/vxl-phys-fluid/src/fluid_step.rs:91-127) on h->stream.
-void enqueue_substep(vxl_sph_handle* h, float dt, uint32_t nspans) {
-  cudaStream_t st = h->stream;
-  const uint32_t nt = (uint32_t)h->nt;
-  const uint32_t nblk = blocks_for(nt);
-  const uint32_t tiles = (h->max_bins + kScanTile - 1) / kScanTile;
-  StepConst sc;
-  sc.dt = dt;
-  sc.vmax = h->params.max_speed_frac * h->k.h / dt;
-  sc.vmax2 = sc.vmax * sc.vmax;
-  LAUNCH(KID_GRIDBOX, k_gridbox<<<1, 32, 0, st>>>(h->ctl, h->k.h, h->max_bins));
-  LAUNCH(KID_KEYS, k_keys<<<nblk, kThreads, 0, st>>>(h->pos[0], h->ctl, h->counts, h->cellrank, nt));
-  LAUNCH(KID_SCAN_PARTIAL, k_scan_partial<<<tiles, kScanThreads, 0, st>>>(h->counts, h->ctl, h->partial));
-  LAUNCH(KID_SCAN_TOP, k_scan_top<<<1, 1024, 0, st>>>(h->partial, h->ctl, h->start));
-  LAUNCH(KID_SCAN_FINAL, k_scan_final<<<tiles, kScanThreads, 0, st>>>(h->counts, h->ctl, h->partial, h->start));
-  LAUNCH(KID_PLACE, k_place<<<nblk, kThreads, 0, st>>>(h->cellrank, h->start, h->orig, h->items, nt));
-  LAUNCH(KID_CANON, k_canon<<<148 * 8, 256, 0, st>>>(h->items, h->start, h->ctl, h->pos[0], h->vel[0], h->pos[1],
-                                                     h->vel[1], h->orig, h->slot_of));
-  LAUNCH(KID_DENSITY, k_density<<<nblk, kThreads, 0, st>>>(h->pos[1], h->start, h->ctl, h->rc, h->press, h->nbr,
-                                                           h->nbr_n, h->nbr_cap, h->k));
-  LAUNCH(KID_FORCE, k_force<<<nblk, kThreads, 0, st>>>(h->pos[1], h->vel[1], h->rc, h->start, h->nbr, h->nbr_n,
-                                                       h->nbr_cap, h->ctl, h->pos[0], h->vel[0],
-                                                       h->record ? h->acc : nullptr, h->record ? h->xsph : nullptr,
-                                                       h->k, sc));
-  if (h->nb > 0 && (nspans > 0 || h->record)) {
-    LAUNCH(KID_BFORCE, k_bforce<<<blocks_for(nt, 128), 128, 0, st>>>(h->pos[1], h->vel[1], h->rc, h->start, h->orig,
-                                                                     h->nbr, h->nbr_n, h->nbr_cap, h->ctl,
-                                                                     h->bforce, h->k));
-  }
-  if (nspans > 0 && h->nchunks > 0) {
-    LAUNCH(KID_REACT_CHUNKS, k_react_chunks<<<h->nchunks, kReactThreads, 0, st>>>(
-                                 h->bforce, h->bpos, h->spans_d, h->chunks_d, h->react_partial, (uint32_t)h->nf));
-    LAUNCH(KID_REACT_SPANS, k_react_spans<<<blocks_for(nspans, 64), 64, 0, st>>>(h->react_partial, h->chunk_first_d,
-                                                                                 h->breact_d, nspans));
-  }
-}
-
-// Everything of one tick after the span table is in its pinned staging buffer.
-void enqueue_tick(vxl_sph_handle* h, float dt_tick, uint32_t nspans) {
-  cudaStream_t st = h->stream;
-  uint32_t sub = h->substeps;
-  float dt = dt_tick / (float)sub;  // fluid_step.rs:77
-  if (nspans > 0) {
-    cudaMemcpyAsync(h->spans_d, h->spans_h, nspans * sizeof(SpanDev), cudaMemcpyHostToDevice, st);
-    if (h->nchunks > 0)
-      cudaMemcpyAsync(h->chunks_d, h->chunks_h, h->nchunks * sizeof(SpanChunk), cudaMemcpyHostToDevice, st);
-    cudaMemcpyAsync(h->chunk_first_d, h->chunk_first_h, (nspans + 1) * sizeof(uint32_t), cudaMemcpyHostToDevice, st);
-    cudaMemsetAsync(h->breact_d, 0, nspans * 6 * sizeof(float), st);
-  }
-  for (uint32_t s = 0; s < sub; ++s) enqueue_substep(h, dt, nspans);
-  if (nspans > 0) {
-    if (sub > 1) {
-      float inv = 1.0f / (float)sub;  // fluid_step.rs:85
-      LAUNCH(KID_SCALE, k_scale<<<blocks_for(nspans * 6), kThreads, 0, st>>>(h->breact_d, nspans * 6, inv));
-    }
-    cudaMemcpyAsync(h->breact_h, h->breact_d, nspans * 6 * sizeof(float), cudaMemcpyDeviceToHost, st);
-  }
-  cudaMemcpyAsync(h->ctl_h, h->ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, st);
-}
-
-vxl_status stage_spans(vxl_sph_handle* h, const vxl_sph_span* spans, uint32_t nspans) {
-  if (nspans == 0) return VXL_OK;
-  if (!spans) return fail(VXL_NULL_POINTER, "spans is NULL with nspans > 0");
-  std::vector<SpanDev> next(nspans);
-  std::vector<SpanChunk> chunks;
-  std::vector<uint32_t> first(nspans + 1, 0);
-  for (uint32_t q = 0; q < nspans; ++q) {
-    const vxl_sph_span& sp = spans[q];
-    if (sp.start < h->nf || sp.end < sp.start || sp.end > h->nt)
-      return fail(VXL_INVALID_ARGUMENT, "span " + std::to_string(q) + " is outside the boundary segment");
-    next[q] = SpanDev{sp.body, sp.origin[0], sp.origin[1], sp.origin[2], sp.start, sp.end};
-    first[q] = (uint32_t)chunks.size();
-    for (uint32_t b = sp.start; b < sp.end; b += kReactChunk)
-      chunks.push_back(SpanChunk{q, b, std::min(sp.end, b + kReactChunk), 0u});
-  }
-  first[nspans] = (uint32_t)chunks.size();
-  uint32_t nch = (uint32_t)chunks.size();
-  if (nspans > h->spans_cap || nch > h->chunks_cap) {
-    CU(cudaStreamSynchronize(h->stream));
-    if (h->graph) {
-      cudaGraphExecDestroy(h->graph);
-      h->graph = nullptr;
-    }
-    void* dptr[] = {h->spans_d, h->breact_d, h->chunks_d, h->chunk_first_d, h->react_partial};
-    for (void* q : dptr)
-      if (q) cudaFree(q);
-    void* hptr[] = {h->spans_h, h->breact_h, h->chunks_h, h->chunk_first_h};
-    for (void* q : hptr)
-      if (q) cudaFreeHost(q);
-    h->spans_d = nullptr; h->spans_h = nullptr; h->breact_d = nullptr; h->breact_h = nullptr;
-    h->chunks_d = nullptr; h->chunks_h = nullptr; h->chunk_first_d = nullptr; h->chunk_first_h = nullptr;
-    h->react_partial = nullptr;
-    uint32_t cap = std::max<uint32_t>(nspans, 64);
-    uint32_t ccap = std::max<uint32_t>(nch, cap + (uint32_t)(h->nb / kReactChunk) + 1);
-    vxl_status st;
-    if ((st = dalloc(h, &h->spans_d, cap)) != VXL_OK) return st;
-    if ((st = dalloc(h, &h->breact_d, (size_t)cap * 6)) != VXL_OK) return st;
-    if ((st = dalloc(h, &h->chunks_d, ccap)) != VXL_OK) return st;
-    if ((st = dalloc(h, &h->chunk_first_d, (size_t)cap + 1)) != VXL_OK) return st;
-    if ((st = dalloc(h, &h->react_partial, (size_t)ccap * 6)) != VXL_OK) return st;
-    CU(cudaMallocHost((void**)&h->spans_h, cap * sizeof(SpanDev)));
-    CU(cudaMallocHost((void**)&h->breact_h, cap * 6 * sizeof(float)));
-    CU(cudaMallocHost((void**)&h->chunks_h, ccap * sizeof(SpanChunk)));
-    CU(cudaMallocHost((void**)&h->chunk_first_h, (cap + 1) * sizeof(uint32_t)));
-    std::memset(h->spans_h, 0xff, cap * sizeof(SpanDev));
-    h->spans_cap = cap;
-    h->chunks_cap = ccap;
-  }
-  // The tick graph copies the pinned tables when it runs; an earlier tick may still be
-  // queued, so wait for it before changing them (steady state: unchanged, no wait).
-  if (std::memcmp(next.data(), h->spans_h, nspans * sizeof(SpanDev)) != 0 || nch != h->nchunks) {
-    CU(cudaStreamSynchronize(h->stream));
-    std::memcpy(h->spans_h, next.data(), nspans * sizeof(SpanDev));
-    if (nch) std::memcpy(h->chunks_h, chunks.data(), nch * sizeof(SpanChunk));
-    std::memcpy(h->chunk_first_h, first.data(), (nspans + 1) * sizeof(uint32_t));
-    h->nchunks = nch;
-  }
-  return VXL_OK;
-}
-
-vxl_status run_tick(vxl_sph_handle* h, float dt_tick, uint32_t nspans) {
-  bool need_capture = !h->graph || h->graph_dt != dt_tick || h->graph_nspans != nspans ||
-                      h->graph_record != h->record || h->graph_prof != h->prof || h->graph_nchunks != h->nchunks;
-  prof_collect(h);
-  h->launches_counter = 0;
-  if (!h->use_graph) {
-    h->prof_used = 0;
-    enqueue_tick(h, dt_tick, nspans);
-    h->prof_pending = h->prof;
-    h->launches_last_tick = h->launches_counter;
-    CU(cudaGetLastError());
-    return VXL_OK;
-  }
-  if (need_capture) {
-    if (h->graph) {
-      cudaGraphExecDestroy(h->graph);
-      h->graph = nullptr;
-    }
-    cudaGraph_t g = nullptr;
-    h->prof_used = 0;
-    CU(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
-    h->capturing = true;
-    enqueue_tick(h, dt_tick, nspans);
-    h->capturing = false;
-    CU(cudaStreamEndCapture(h->stream, &g));
-    cudaError_t e = cudaGraphInstantiate(&h->graph, g, 0);
-    cudaGraphDestroy(g);
-    if (e != cudaSuccess) return fail(VXL_CUDA_ERROR, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
-    h->graph_dt = dt_tick;
-    h->graph_nspans = nspans;
-    h->graph_record = h->record;
-    h->graph_prof = h->prof;
-    h->graph_nchunks = h->nchunks;
-    h->launches_last_tick = h->launches_counter;
-  }
-  CU(cudaGraphLaunch(h->graph, h->stream));
-  h->prof_pending = h->prof;
-  return VXL_OK;
-}
-
-vxl_status finish_sync(vxl_sph_handle* h, vxl_sph_reaction* out, uint32_t nspans) {
-  CU(cudaStreamSynchronize(h->stream));
-  prof_collect(h);
-  if (h->ctl_h->err & kErrGridLoop) return fail(VXL_DEVICE_FAULT_FLAG, "grid box doubling loop did not settle");
-  if (out && nspans > 0) {
-    for (uint32_t q = 0; q < nspans; ++q) {
-      out[q].body = h->spans_h[q].body;
-      for (int a = 0; a < 3; ++a) {
-        out[q].force[a] = h->breact_h[6 * q + a];
-        out[q].torque[a] = h->breact_h[6 * q + 3 + a];
-      }
-    }
-  }
-  return VXL_OK;
-}
-
-vxl_status recompute_bboxes(vxl_sph_handle* h) {
-  static const uint32_t init[6] = {0xffffffffu, 0xffffffffu, 0xffffffffu, 0u, 0u, 0u};
-  CU(cudaMemcpyAsync(h->ctl->fbox, init, sizeof(init), cudaMemcpyHostToDevice, h->stream));
-  CU(cudaMemcpyAsync(h->ctl->bbox, init, sizeof(init), cudaMemcpyHostToDevice, h->stream));
-  uint32_t nblk = blocks_for(h->nt);
-  k_bbox<<<nblk, kThreads, 0, h->stream>>>(h->pos[0], (uint32_t)h->nt, 1, h->ctl->fbox);
-  k_bbox<<<nblk, kThreads, 0, h->stream>>>(h->pos[0], (uint32_t)h->nt, 0, h->ctl->bbox);
-  CU(cudaGetLastError());
+vxl_status check_desc(const vxl_sph_desc* d) {
+  if (!d) return set_error(VXL_NULL_POINTER, "desc is NULL");
+  if (d->hdr.version != VXL_SPH_ABI_VERSION || d->params.hdr.version != VXL_SPH_ABI_VERSION)
+    return set_error(VXL_VERSION_MISMATCH, "ABI version mismatch");
+  if (!check_header(d->hdr, sizeof(vxl_sph_desc)) || !check_header(d->params.hdr, sizeof(vxl_sph_params)))
+    return set_error(VXL_SIZE_MISMATCH, "struct size mismatch");
+  if (d->n_fluid + d->n_boundary >= (1ull << 31)) return set_error(VXL_INVALID_ARGUMENT, "more than 2^31 particles");
+  const uint32_t mb = d->params.max_bins ? d->params.max_bins : (1u << 21);
+  if (mb > (1u << 21)) return set_error(VXL_INVALID_ARGUMENT, "max_bins above 2^21");
+  if (!(d->params.particle_mass > 0.0f) || !(d->params.rest_density > 0.0f) || !(d->params.gamma_tait > 0.0f))
+    return set_error(VXL_INVALID_ARGUMENT, "particle_mass, rest_density and gamma_tait must be positive");
   return VXL_OK;
 }
 
@@ -470,13 +57,51 @@ struct DeviceGuard {
   }
 };
 
+#define HANDLE_OR_FAIL(h)                                                     \
+  if (!(h) || !(h)->e) return set_error(VXL_NULL_POINTER, "handle is NULL"); \
+  DeviceGuard dg_((h)->e->device())
+
+vxl_status make_engine(const vxl_sph_desc* descs, uint32_t n, int32_t device, uint64_t cell_capacity,
+                       vxl_sph_handle** out) {
+  if (!out) return set_error(VXL_NULL_POINTER, "out is NULL");
+  *out = nullptr;
+  if (!descs || n == 0) return set_error(VXL_NULL_POINTER, "no scene descriptions");
+  uint64_t slots = 0, cells = 0;
+  for (uint32_t i = 0; i < n; ++i) {
+    vxl_status s = check_desc(descs + i);
+    if (s != VXL_OK) return s;
+    slots += descs[i].n_fluid + descs[i].n_boundary;
+    cells += (uint64_t)(descs[i].params.max_bins ? descs[i].params.max_bins : (1u << 21));
+  }
+  if (cell_capacity == 0) cell_capacity = std::min<uint64_t>(cells, 1ull << 28);
+  Engine* e = nullptr;
+  vxl_status s = Engine::create(device, slots, cell_capacity, n, &e);
+  if (s != VXL_OK) return s;
+  for (uint32_t i = 0; i < n; ++i) {
+    const vxl_sph_desc& d = descs[i];
+    s = e->add_scene(d.params, d.n_fluid, d.n_boundary, d.pos_xyz, d.vel_xyz, d.pmass, i, nullptr);
+    if (s != VXL_OK) {
+      delete e;
+      return s;
+    }
+  }
+  auto* h = new (std::nothrow) vxl_sph_handle();
+  if (!h) {
+    delete e;
+    return set_error(VXL_OUT_OF_MEMORY, "host allocation failed");
+  }
+  h->e = e;
+  *out = h;
+  return VXL_OK;
+}
+
 }  // namespace
 
 extern "C" {
 
 uint32_t vxl_sph_abi_version(void) { return VXL_SPH_ABI_VERSION; }
 
-const char* vxl_sph_last_error(void) { return g_last_error.c_str(); }
+const char* vxl_sph_last_error(void) { return vxl_get_last_error(); }
 
 const char* vxl_sph_backend_name(void) { return "b200-cuda-wcsph"; }
 
@@ -494,377 +119,234 @@ int vxl_sph_backend_available(void) {
 }
 
 vxl_status vxl_sph_create(const vxl_sph_desc* desc, vxl_sph_handle** out) {
-  API_TRACE();
   try {
-    if (!desc || !out) return fail(VXL_NULL_POINTER, "desc or out is NULL");
-    *out = nullptr;
-    if (desc->hdr.version != VXL_SPH_ABI_VERSION || desc->params.hdr.version != VXL_SPH_ABI_VERSION)
-      return fail(VXL_VERSION_MISMATCH, "ABI version mismatch");
-    if (!check_header(desc->hdr, sizeof(vxl_sph_desc)) || !check_header(desc->params.hdr, sizeof(vxl_sph_params)))
-      return fail(VXL_SIZE_MISMATCH, "struct size mismatch");
-    uint64_t nf = desc->n_fluid, nb = desc->n_boundary, nt = nf + nb;
-    if (nt > 0 && (!desc->pos_xyz || !desc->vel_xyz)) return fail(VXL_NULL_POINTER, "pos/vel is NULL");
-    if (nb > 0 && !desc->pmass) return fail(VXL_NULL_POINTER, "pmass is NULL with boundary particles");
-    if (nt >= (1ull << 31)) return fail(VXL_INVALID_ARGUMENT, "more than 2^31 particles");
-    const vxl_sph_params& p = desc->params;
-    uint32_t max_bins = p.max_bins ? p.max_bins : (1u << 21);
-    if (max_bins > (1u << 21)) return fail(VXL_INVALID_ARGUMENT, "max_bins above 2^21");
-    if (!(p.particle_mass > 0.0f) || !(p.rest_density > 0.0f) || !(p.gamma_tait > 0.0f))
-      return fail(VXL_INVALID_ARGUMENT, "particle_mass, rest_density and gamma_tait must be positive");
-    if (desc->pmass)
-      for (uint64_t i = 0; i < nf; ++i)
-        if (desc->pmass[i] != p.particle_mass)
-          return fail(VXL_INVALID_ARGUMENT, "fluid pmass must equal params.particle_mass");
-    for (uint64_t i = nf; i < nt; ++i)
-      if (!(desc->pmass[i] > 0.0f)) return fail(VXL_INVALID_ARGUMENT, "boundary pmass must be positive");
-
-    auto* h = new (std::nothrow) vxl_sph_handle();
-    if (!h) return fail(VXL_OUT_OF_MEMORY, "host allocation failed");
-    h->device = desc->device;
-    DeviceGuard dg(h->device);
-    cudaError_t e = cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking);
-    h->stream = h->own_stream;
-    if (e != cudaSuccess) {
-      delete h;
-      return fail(VXL_CUDA_ERROR, std::string("cudaStreamCreate: ") + cudaGetErrorString(e));
-    }
-    h->params = p;
-    h->nf = nf;
-    h->nb = nb;
-    h->nt = nt;
-    h->max_bins = max_bins;
-    h->substeps = p.substeps ? p.substeps : 1;
-    h->k = make_const(p, nf, nt, max_bins);
-    vxl_status s = VXL_OK;
-    auto A = [&](vxl_status r) {
-      if (s == VXL_OK) s = r;
-    };
-    uint64_t nta = nt ? nt : 1;
-    A(dalloc(h, &h->pos[0], nta));
-    A(dalloc(h, &h->pos[1], nta));
-    A(dalloc(h, &h->vel[0], nta));
-    A(dalloc(h, &h->vel[1], nta));
-    A(dalloc(h, &h->orig, nta));
-    A(dalloc(h, &h->slot_of, nta));
-    A(dalloc(h, &h->cellrank, nta));
-    A(dalloc(h, &h->items, nta));
-    A(dalloc(h, &h->counts, (size_t)max_bins + 1));
-    A(dalloc(h, &h->start, (size_t)max_bins + 1));
-    A(dalloc(h, &h->partial, 1024));
-    A(dalloc(h, &h->rc, nta));
-    A(dalloc(h, &h->press, nta));
-    A(dalloc(h, &h->acc, nta));
-    A(dalloc(h, &h->xsph, nta));
-    A(dalloc(h, &h->nbr, (size_t)h->nbr_cap * nta));
-    A(dalloc(h, &h->nbr_n, nta));
-    A(dalloc(h, &h->bforce, nb ? nb : 1));
-    A(dalloc(h, &h->bpos, nb ? nb : 1));
-    A(dalloc(h, &h->ctl, 1));
-    A(dalloc(h, &h->stage, 8 * nta));
-    if (s == VXL_OK) {
-      if (cudaMallocHost((void**)&h->ctl_h, sizeof(Ctl)) != cudaSuccess) s = fail(VXL_OUT_OF_MEMORY, "pinned alloc");
-      else std::memset(h->ctl_h, 0, sizeof(Ctl));
-    }
-    if (s == VXL_OK) {
-      cudaEventCreate(&h->ev0);
-      cudaEventCreate(&h->ev1);
-      cudaMemsetAsync(h->counts, 0, ((size_t)max_bins + 1) * 4, h->stream);
-      cudaMemsetAsync(h->start, 0, ((size_t)max_bins + 1) * 4, h->stream);
-      cudaMemsetAsync(h->ctl, 0, sizeof(Ctl), h->stream);
-      cudaMemsetAsync(h->acc, 0, nta * sizeof(float4), h->stream);
-      cudaMemsetAsync(h->xsph, 0, nta * sizeof(float4), h->stream);
-      cudaMemsetAsync(h->bforce, 0, (nb ? nb : 1) * sizeof(float4), h->stream);
-      cudaMemsetAsync(h->rc, 0, nta * sizeof(float2), h->stream);
-      cudaMemsetAsync(h->press, 0, nta * sizeof(float), h->stream);
-      if (nt > 0) {
-        cudaMemcpyAsync(h->stage, desc->pos_xyz, nt * 12, cudaMemcpyHostToDevice, h->stream);
-        cudaMemcpyAsync(h->stage + 3 * nt, desc->vel_xyz, nt * 12, cudaMemcpyHostToDevice, h->stream);
-        float* pm_d = nullptr;
-        if (nb > 0) {
-          cudaMalloc((void**)&pm_d, nt * 4);
-          cudaMemcpyAsync(pm_d, desc->pmass, nt * 4, cudaMemcpyHostToDevice, h->stream);
-        }
-        k_init_state<<<blocks_for(nt), kThreads, 0, h->stream>>>(h->stage, h->stage + 3 * nt, pm_d, h->pos[0],
-                                                                  h->vel[0], h->orig, h->slot_of, h->bpos, h->k);
-        s = recompute_bboxes(h);
-        cudaStreamSynchronize(h->stream);
-        if (pm_d) cudaFree(pm_d);
-      }
-      cudaError_t e2 = cudaStreamSynchronize(h->stream);
-      if (s == VXL_OK && e2 != cudaSuccess) s = fail(VXL_CUDA_ERROR, cudaGetErrorString(e2));
-    }
-    if (s != VXL_OK) {
-      free_all(h);
-      delete h;
-      return s;
-    }
-    *out = h;
-    return VXL_OK;
+    if (!desc || !out) return set_error(VXL_NULL_POINTER, "desc or out is NULL");
+    vxl_status s = check_desc(desc);
+    if (s != VXL_OK) return s;
+    const uint64_t mb = desc->params.max_bins ? desc->params.max_bins : (1u << 21);
+    return make_engine(desc, 1, desc->device, mb, out);
   } catch (...) {
-    return fail(VXL_PANIC_CAUGHT, "exception in vxl_sph_create");
+    return set_error(VXL_PANIC_CAUGHT, "exception in vxl_sph_create");
+  }
+}
+
+vxl_status vxl_sph_create_batch(const vxl_sph_desc* descs, uint32_t n, int32_t device, uint64_t cell_capacity,
+                                vxl_sph_handle** out) {
+  try {
+    return make_engine(descs, n, device, cell_capacity, out);
+  } catch (...) {
+    return set_error(VXL_PANIC_CAUGHT, "exception in vxl_sph_create_batch");
   }
 }
 
 vxl_status vxl_sph_destroy(vxl_sph_handle* h) {
-  API_TRACE();
-  if (!h) return fail(VXL_NULL_POINTER, "handle is NULL");
-  DeviceGuard dg(h->device);
-  cudaStreamSynchronize(h->stream);
-  free_all(h);
+  if (!h) return set_error(VXL_NULL_POINTER, "handle is NULL");
+  delete h->e;
   delete h;
   return VXL_OK;
 }
 
+uint32_t vxl_sph_scene_count(vxl_sph_handle* h) { return (h && h->e) ? (uint32_t)h->e->scenes().size() : 0u; }
+
 vxl_status vxl_sph_upload_boundary(vxl_sph_handle* h, uint64_t n_fluid, const float* pos_xyz, const float* vel_xyz,
                                    uint64_t nb) {
-  API_TRACE();
-  if (!h) return fail(VXL_NULL_POINTER, "handle is NULL");
-  if (n_fluid != h->nf || nb != h->nb)
-    return fail(VXL_SIZE_MISMATCH, "boundary segment length differs from the scene (rebuild the scene)");
-  if (nb == 0) return VXL_OK;
-  if (!pos_xyz || !vel_xyz) return fail(VXL_NULL_POINTER, "pos/vel is NULL");
-  DeviceGuard dg(h->device);
-  static const uint32_t init[6] = {0xffffffffu, 0xffffffffu, 0xffffffffu, 0u, 0u, 0u};
-  CU(cudaMemcpyAsync(h->stage, pos_xyz, nb * 12, cudaMemcpyHostToDevice, h->stream));
-  CU(cudaMemcpyAsync(h->stage + 3 * nb, vel_xyz, nb * 12, cudaMemcpyHostToDevice, h->stream));
-  CU(cudaMemcpyAsync(h->ctl->bbox, init, sizeof(init), cudaMemcpyHostToDevice, h->stream));
-  k_upload_boundary<<<blocks_for(nb), kThreads, 0, h->stream>>>(h->stage, h->stage + 3 * nb, h->pos[0], h->vel[0],
-                                                                 h->slot_of, h->bpos, h->ctl->bbox, h->k);
-  CU(cudaGetLastError());
-  // the caller's arrays are borrowed for this call only: finish the copies before returning
-  CU(cudaStreamSynchronize(h->stream));
-  return VXL_OK;
+  HANDLE_OR_FAIL(h);
+  if (h->e->scenes().empty()) return set_error(VXL_NOT_READY, "no scene");
+  if (n_fluid != h->e->scenes()[0].nf)
+    return set_error(VXL_SIZE_MISMATCH, "fluid prefix differs from the scene (rebuild the scene)");
+  return h->e->upload_boundary(0, pos_xyz, vel_xyz, nb);
+}
+
+vxl_status vxl_sph_upload_boundary_scene(vxl_sph_handle* h, uint32_t scene, const float* pos_xyz,
+                                         const float* vel_xyz, uint64_t nb) {
+  HANDLE_OR_FAIL(h);
+  return h->e->upload_boundary(scene, pos_xyz, vel_xyz, nb);
+}
+
+vxl_status vxl_sph_set_spans_scene(vxl_sph_handle* h, uint32_t scene, const vxl_sph_span* spans, uint32_t nspans) {
+  HANDLE_OR_FAIL(h);
+  return h->e->set_spans(scene, spans, nspans);
 }
 
 vxl_status vxl_sph_step_tick_async(vxl_sph_handle* h, float dt_tick, const vxl_sph_span* spans, uint32_t nspans) {
-  API_TRACE();
   try {
-    if (!h) return fail(VXL_NULL_POINTER, "handle is NULL");
-    if (!(dt_tick > 0.0f) || !std::isfinite(dt_tick)) return fail(VXL_INVALID_ARGUMENT, "dt_tick must be > 0");
-    DeviceGuard dg(h->device);
-    if (h->nf == 0) return VXL_OK;  // fluid_step.rs:93-95: boundary particles are not driven alone
-    vxl_status s = stage_spans(h, spans, nspans);
-    if (s != VXL_OK) return s;
+    HANDLE_OR_FAIL(h);
+    if (h->e->scenes().size() == 1) {
+      vxl_status s = h->e->set_spans(0, spans, nspans);
+      if (s != VXL_OK) return s;
+    } else if (nspans > 0) {
+      return set_error(VXL_INVALID_ARGUMENT, "batched handles take spans through vxl_sph_set_spans_scene");
+    }
     h->last_nspans = nspans;
-    s = run_tick(h, dt_tick, nspans);
-    h->ran_substep = true;
-    return s;
+    return h->e->step_tick_async(dt_tick);
   } catch (...) {
-    return fail(VXL_PANIC_CAUGHT, "exception in vxl_sph_step_tick_async");
+    return set_error(VXL_PANIC_CAUGHT, "exception in vxl_sph_step_tick_async");
   }
 }
 
 vxl_status vxl_sph_sync(vxl_sph_handle* h, vxl_sph_reaction* out_reactions, uint32_t nspans) {
-  API_TRACE();
-  if (!h) return fail(VXL_NULL_POINTER, "handle is NULL");
-  DeviceGuard dg(h->device);
-  if (nspans > h->last_nspans) return fail(VXL_SIZE_MISMATCH, "more reactions requested than spans stepped");
-  return finish_sync(h, out_reactions, nspans);
+  HANDLE_OR_FAIL(h);
+  if (nspans > 0 && !out_reactions) return set_error(VXL_NULL_POINTER, "out_reactions is NULL with nspans > 0");
+  vxl_status s = h->e->sync(&h->last);
+  if (s != VXL_OK) return s;
+  if (nspans > h->last.size()) return set_error(VXL_SIZE_MISMATCH, "more reactions requested than spans stepped");
+  for (uint32_t q = 0; q < nspans; ++q) out_reactions[q] = h->last[q];
+  return VXL_OK;
 }
 
 vxl_status vxl_sph_step_tick(vxl_sph_handle* h, float dt_tick, const vxl_sph_span* spans, uint32_t nspans,
                              vxl_sph_reaction* out_reactions) {
-  API_TRACE();
-  if (nspans > 0 && !out_reactions) return fail(VXL_NULL_POINTER, "out_reactions is NULL with nspans > 0");
+  if (nspans > 0 && !out_reactions) return set_error(VXL_NULL_POINTER, "out_reactions is NULL with nspans > 0");
   vxl_status s = vxl_sph_step_tick_async(h, dt_tick, spans, nspans);
   if (s != VXL_OK) return s;
   return vxl_sph_sync(h, out_reactions, nspans);
 }
 
+vxl_status vxl_sph_reactions_all(vxl_sph_handle* h, vxl_sph_reaction* out, uint32_t cap, uint32_t* n) {
+  HANDLE_OR_FAIL(h);
+  if (!n) return set_error(VXL_NULL_POINTER, "n is NULL");
+  *n = (uint32_t)h->last.size();
+  if (out)
+    for (uint32_t q = 0; q < cap && q < h->last.size(); ++q) out[q] = h->last[q];
+  return VXL_OK;
+}
+
 vxl_status vxl_sph_substep(vxl_sph_handle* h, float dt) {
-  API_TRACE();
-  if (!h) return fail(VXL_NULL_POINTER, "handle is NULL");
-  if (!(dt > 0.0f)) return fail(VXL_INVALID_ARGUMENT, "dt must be > 0");
-  DeviceGuard dg(h->device);
-  if (h->nf == 0) return VXL_OK;
-  prof_collect(h);
-  h->prof_used = 0;
-  enqueue_substep(h, dt, 0);
-  h->prof_pending = h->prof;
-  CU(cudaMemcpyAsync(h->ctl_h, h->ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, h->stream));
-  CU(cudaGetLastError());
-  h->ran_substep = true;
-  return finish_sync(h, nullptr, 0);
+  HANDLE_OR_FAIL(h);
+  if (!(dt > 0.0f)) return set_error(VXL_INVALID_ARGUMENT, "dt must be > 0");
+  return h->e->substep(std::vector<float>(h->e->scenes().size(), dt));
 }
 
 vxl_status vxl_sph_bounds(vxl_sph_handle* h, float lo[3], float hi[3]) {
-  API_TRACE();
-  if (!h || !lo || !hi) return fail(VXL_NULL_POINTER, "NULL argument");
-  DeviceGuard dg(h->device);
-  uint32_t box[6];
-  CU(cudaMemcpyAsync(box, h->ctl->fbox, sizeof(box), cudaMemcpyDeviceToHost, h->stream));
-  CU(cudaStreamSynchronize(h->stream));
-  for (int a = 0; a < 3; ++a) {
-    lo[a] = vxl_o2f_host(box[a]);
-    hi[a] = vxl_o2f_host(box[3 + a]);
-  }
-  if (!(std::isfinite(lo[0]) && std::isfinite(hi[0]))) return fail(VXL_NOT_READY, "no fluid bounds");
-  return VXL_OK;
+  HANDLE_OR_FAIL(h);
+  if (!lo || !hi) return set_error(VXL_NULL_POINTER, "NULL argument");
+  return h->e->bounds(0, lo, hi);
 }
 
 vxl_status vxl_sph_read_state(vxl_sph_handle* h, float* pos_xyz, float* vel_xyz) {
-  API_TRACE();
-  if (!h) return fail(VXL_NULL_POINTER, "handle is NULL");
-  DeviceGuard dg(h->device);
-  if (h->nt == 0) return VXL_OK;
-  float* dp = h->stage;
-  float* dv = h->stage + 3 * h->nt;
-  k_read_state<<<blocks_for(h->nt), kThreads, 0, h->stream>>>(h->pos[0], h->vel[0], h->orig, pos_xyz ? dp : nullptr,
-                                                               vel_xyz ? dv : nullptr, (uint32_t)h->nt);
-  if (pos_xyz) CU(cudaMemcpyAsync(pos_xyz, dp, h->nt * 12, cudaMemcpyDeviceToHost, h->stream));
-  if (vel_xyz) CU(cudaMemcpyAsync(vel_xyz, dv, h->nt * 12, cudaMemcpyDeviceToHost, h->stream));
-  CU(cudaStreamSynchronize(h->stream));
-  return VXL_OK;
+  HANDLE_OR_FAIL(h);
+  if (h->e->scenes().empty()) return VXL_OK;
+  return h->e->read_state(0, pos_xyz, vel_xyz);
+}
+
+vxl_status vxl_sph_read_state_scene(vxl_sph_handle* h, uint32_t scene, float* pos_xyz, float* vel_xyz) {
+  HANDLE_OR_FAIL(h);
+  return h->e->read_state(scene, pos_xyz, vel_xyz);
 }
 
 vxl_status vxl_sph_write_state(vxl_sph_handle* h, const float* pos_xyz, const float* vel_xyz) {
-  API_TRACE();
-  if (!h) return fail(VXL_NULL_POINTER, "handle is NULL");
-  DeviceGuard dg(h->device);
-  if (h->nt == 0) return VXL_OK;
-  float* dp = h->stage;
-  float* dv = h->stage + 3 * h->nt;
-  if (pos_xyz) CU(cudaMemcpyAsync(dp, pos_xyz, h->nt * 12, cudaMemcpyHostToDevice, h->stream));
-  if (vel_xyz) CU(cudaMemcpyAsync(dv, vel_xyz, h->nt * 12, cudaMemcpyHostToDevice, h->stream));
-  k_write_state<<<blocks_for(h->nt), kThreads, 0, h->stream>>>(pos_xyz ? dp : nullptr, vel_xyz ? dv : nullptr,
-                                                                h->pos[0], h->vel[0], h->orig, h->bpos, h->k);
-  if (pos_xyz) {
-    vxl_status s = recompute_bboxes(h);
-    if (s != VXL_OK) return s;
-  }
-  CU(cudaGetLastError());
-  CU(cudaStreamSynchronize(h->stream));  // the caller's arrays are borrowed for this call only
-  return VXL_OK;
+  HANDLE_OR_FAIL(h);
+  if (h->e->scenes().empty()) return VXL_OK;
+  return h->e->write_state(0, pos_xyz, vel_xyz);
+}
+
+vxl_status vxl_sph_write_state_scene(vxl_sph_handle* h, uint32_t scene, const float* pos_xyz, const float* vel_xyz) {
+  HANDLE_OR_FAIL(h);
+  return h->e->write_state(scene, pos_xyz, vel_xyz);
 }
 
 vxl_status vxl_sph_set_record(vxl_sph_handle* h, int on) {
-  API_TRACE();
-  if (!h) return fail(VXL_NULL_POINTER, "handle is NULL");
-  h->record = on != 0;
+  HANDLE_OR_FAIL(h);
+  h->e->set_record(on != 0);
   return VXL_OK;
 }
 
 vxl_status vxl_sph_read_fields(vxl_sph_handle* h, float* dens, float* press, float* acc_xyz, float* xsph_xyz,
                                float* bforce_xyz) {
-  API_TRACE();
-  if (!h) return fail(VXL_NULL_POINTER, "handle is NULL");
-  DeviceGuard dg(h->device);
-  uint64_t nt = h->nt;
-  if (nt == 0) return VXL_OK;
-  if ((acc_xyz || xsph_xyz) && !h->record) return fail(VXL_NOT_READY, "acc/xsph are recorded only with set_record(1)");
-  float* d_d = h->stage;
-  float* d_p = h->stage + nt;
-  float* d_a = h->stage + 2 * nt;
-  float* d_x = h->stage + 5 * nt;
-  k_read_fields<<<blocks_for(nt), kThreads, 0, h->stream>>>(h->rc, h->press, h->acc, h->xsph, h->orig,
-                                                             dens ? d_d : nullptr, press ? d_p : nullptr,
-                                                             acc_xyz ? d_a : nullptr, xsph_xyz ? d_x : nullptr,
-                                                             (uint32_t)nt);
-  if (dens) CU(cudaMemcpyAsync(dens, d_d, nt * 4, cudaMemcpyDeviceToHost, h->stream));
-  if (press) CU(cudaMemcpyAsync(press, d_p, nt * 4, cudaMemcpyDeviceToHost, h->stream));
-  if (acc_xyz) CU(cudaMemcpyAsync(acc_xyz, d_a, nt * 12, cudaMemcpyDeviceToHost, h->stream));
-  if (xsph_xyz) CU(cudaMemcpyAsync(xsph_xyz, d_x, nt * 12, cudaMemcpyDeviceToHost, h->stream));
-  if (bforce_xyz && h->nb > 0) {
-    std::vector<float> tmp(h->nb * 4);
-    CU(cudaMemcpyAsync(tmp.data(), h->bforce, h->nb * 16, cudaMemcpyDeviceToHost, h->stream));
-    CU(cudaStreamSynchronize(h->stream));
-    for (uint64_t q = 0; q < h->nb; ++q)
-      for (int a = 0; a < 3; ++a) bforce_xyz[3 * q + a] = tmp[4 * q + a];
-  }
-  CU(cudaStreamSynchronize(h->stream));
-  return VXL_OK;
+  HANDLE_OR_FAIL(h);
+  return h->e->read_fields(0, dens, press, acc_xyz, xsph_xyz, bforce_xyz);
+}
+
+vxl_status vxl_sph_read_fields_scene(vxl_sph_handle* h, uint32_t scene, float* dens, float* press, float* acc_xyz,
+                                     float* xsph_xyz, float* bforce_xyz) {
+  HANDLE_OR_FAIL(h);
+  return h->e->read_fields(scene, dens, press, acc_xyz, xsph_xyz, bforce_xyz);
 }
 
 vxl_status vxl_sph_export_grid(vxl_sph_handle* h, uint32_t* items, uint32_t* start, uint64_t start_cap,
                                uint32_t* bins, vxl_sph_grid_info* info) {
-  API_TRACE();
-  if (!h) return fail(VXL_NULL_POINTER, "handle is NULL");
-  DeviceGuard dg(h->device);
-  if (!h->ran_substep) return fail(VXL_NOT_READY, "no substep has run yet");
-  Ctl c;
-  CU(cudaMemcpyAsync(&c, h->ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, h->stream));
-  CU(cudaStreamSynchronize(h->stream));
-  uint64_t total = c.grid.total;
-  if (info) {
-    if (!check_header(info->hdr, sizeof(vxl_sph_grid_info))) return fail(VXL_SIZE_MISMATCH, "grid_info header");
-    info->min[0] = c.grid.minx; info->min[1] = c.grid.miny; info->min[2] = c.grid.minz;
-    info->inv = c.grid.inv;
-    info->bin = c.grid.bin;
-    info->dims[0] = c.grid.nx; info->dims[1] = c.grid.ny; info->dims[2] = c.grid.nz;
-    info->total = total;
+  HANDLE_OR_FAIL(h);
+  if (info && !check_header(info->hdr, sizeof(vxl_sph_grid_info)))
+    return set_error(VXL_SIZE_MISMATCH, "grid_info header");
+  return h->e->export_grid(0, items, start, start_cap, bins, info);
+}
+
+vxl_status vxl_sph_export_grid_scene(vxl_sph_handle* h, uint32_t scene, uint32_t* items, uint32_t* start,
+                                     uint64_t start_cap, uint32_t* bins, vxl_sph_grid_info* info) {
+  HANDLE_OR_FAIL(h);
+  if (info && !check_header(info->hdr, sizeof(vxl_sph_grid_info)))
+    return set_error(VXL_SIZE_MISMATCH, "grid_info header");
+  return h->e->export_grid(scene, items, start, start_cap, bins, info);
+}
+
+vxl_status vxl_sph_get_stats(vxl_sph_handle* h, vxl_sph_stats* out) {
+  HANDLE_OR_FAIL(h);
+  if (!out) return set_error(VXL_NULL_POINTER, "NULL argument");
+  if (!check_header(out->hdr, sizeof(vxl_sph_stats))) return set_error(VXL_SIZE_MISMATCH, "stats header");
+  uint64_t nf = 0, nb = 0;
+  for (auto& s : h->e->scenes()) {
+    nf += s.nf;
+    nb += s.nb;
   }
-  if (start) {
-    if (start_cap < total + 1) return fail(VXL_SIZE_MISMATCH, "start buffer smaller than cells + 1");
-    CU(cudaMemcpyAsync(start, h->start, (total + 1) * 4, cudaMemcpyDeviceToHost, h->stream));
-  }
-  if (items) CU(cudaMemcpyAsync(items, h->orig, h->nt * 4, cudaMemcpyDeviceToHost, h->stream));
-  if (bins) {
-    uint32_t* d_bins = (uint32_t*)h->stage;
-    k_export_bins<<<blocks_for(total), kThreads, 0, h->stream>>>(h->start, h->orig, h->ctl, d_bins);
-    CU(cudaMemcpyAsync(bins, d_bins, h->nt * 4, cudaMemcpyDeviceToHost, h->stream));
-  }
-  CU(cudaStreamSynchronize(h->stream));
+  out->n_fluid = nf;
+  out->n_boundary = nb;
+  out->cells = h->e->cells_last();
+  out->launches_last_tick = h->e->launches_last_tick();
+  out->device_bytes = h->e->device_bytes();
+  out->last_tick_ms = 0.0f;
   return VXL_OK;
 }
 
 vxl_status vxl_sph_set_stream(vxl_sph_handle* h, void* cuda_stream) {
-  API_TRACE();
-  if (!h) return fail(VXL_NULL_POINTER, "handle is NULL");
-  DeviceGuard dg(h->device);
-  prof_collect(h);
-  CU(cudaStreamSynchronize(h->stream));
-  h->stream = cuda_stream ? (cudaStream_t)cuda_stream : h->own_stream;
+  HANDLE_OR_FAIL(h);
+  h->e->set_stream((cudaStream_t)cuda_stream);
   return VXL_OK;
 }
 
 vxl_status vxl_sph_set_profile(vxl_sph_handle* h, int on) {
-  API_TRACE();
-  if (!h) return fail(VXL_NULL_POINTER, "handle is NULL");
-  DeviceGuard dg(h->device);
-  prof_collect(h);
-  h->prof = on != 0;
-  // events for every launch of a tick, created here (never during graph capture)
-  size_t need = 2 * ((size_t)h->substeps * 12 + 8);
-  while (h->prof && h->prof_ev.size() < need) {
-    cudaEvent_t e;
-    CU(cudaEventCreate(&e));
-    h->prof_ev.push_back(e);
-  }
-  h->prof_kid.resize(h->prof_ev.size() / 2);
-  for (int k = 0; k < KID_COUNT; ++k) {
-    h->prof_ms[k] = 0.0;
-    h->prof_n[k] = 0;
-  }
-  return VXL_OK;
+  HANDLE_OR_FAIL(h);
+  return h->e->set_profile(on != 0);
 }
 
 vxl_status vxl_sph_profile_read(vxl_sph_handle* h, uint32_t k, const char** name, double* total_ms,
                                 uint64_t* launches) {
-  API_TRACE();
-  if (!h) return fail(VXL_NULL_POINTER, "handle is NULL");
-  if (k >= (uint32_t)KID_COUNT) return fail(VXL_INVALID_ARGUMENT, "kernel index past the table");
-  DeviceGuard dg(h->device);
-  prof_collect(h);
-  if (name) *name = kKernelNames[k];
-  if (total_ms) *total_ms = h->prof_ms[k];
-  if (launches) *launches = h->prof_n[k];
+  HANDLE_OR_FAIL(h);
+  return h->e->profile_read(k, name, total_ms, launches);
+}
+
+vxl_status vxl_sph_set_tuning(vxl_sph_handle* h, const vxl_sph_tuning* t) {
+  HANDLE_OR_FAIL(h);
+  if (!t) return set_error(VXL_NULL_POINTER, "tuning is NULL");
+  if (!check_header(t->hdr, sizeof(vxl_sph_tuning))) return set_error(VXL_SIZE_MISMATCH, "tuning header");
+  if ((t->block != 128 && t->block != 256) || t->tile < 128 || t->tile % 128 != 0 || t->waves < 1 || t->waves > 4)
+    return set_error(VXL_INVALID_ARGUMENT, "block must be 128/256, tile a multiple of 128, waves 1..4");
+  h->e->set_tuning(vxl::Tuning{t->block, t->tile, t->waves});
   return VXL_OK;
 }
 
-vxl_status vxl_sph_get_stats(vxl_sph_handle* h, vxl_sph_stats* out) {
-  API_TRACE();
-  if (!h || !out) return fail(VXL_NULL_POINTER, "NULL argument");
-  if (!check_header(out->hdr, sizeof(vxl_sph_stats))) return fail(VXL_SIZE_MISMATCH, "stats header");
-  DeviceGuard dg(h->device);
-  Ctl c;
-  CU(cudaMemcpyAsync(&c, h->ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, h->stream));
-  CU(cudaStreamSynchronize(h->stream));
-  out->n_fluid = h->nf;
-  out->n_boundary = h->nb;
-  out->cells = c.grid.total;
-  out->launches_last_tick = h->launches_last_tick;
-  out->device_bytes = h->device_bytes;
-  out->last_tick_ms = 0.0f;
+vxl_status vxl_sph_get_tuning(vxl_sph_handle* h, vxl_sph_tuning* t) {
+  HANDLE_OR_FAIL(h);
+  if (!t) return set_error(VXL_NULL_POINTER, "tuning is NULL");
+  if (!check_header(t->hdr, sizeof(vxl_sph_tuning))) return set_error(VXL_SIZE_MISMATCH, "tuning header");
+  t->block = h->e->tuning().block;
+  t->tile = h->e->tuning().tile;
+  t->waves = h->e->tuning().waves;
+  return VXL_OK;
+}
+
+vxl_status vxl_sph_autotune(vxl_sph_handle* h, float dt_tick, uint32_t trials, vxl_sph_tuning* best) {
+  HANDLE_OR_FAIL(h);
+  if (best && !check_header(best->hdr, sizeof(vxl_sph_tuning))) return set_error(VXL_SIZE_MISMATCH, "tuning header");
+  vxl::Tuning t;
+  float ms = 0.f;
+  vxl_status s = h->e->autotune(dt_tick, trials ? trials : 3, &t, &ms);
+  if (s != VXL_OK) return s;
+  if (best) {
+    best->block = t.block;
+    best->tile = t.tile;
+    best->waves = t.waves;
+    best->ms_per_substep = ms;
+  }
   return VXL_OK;
 }
 

@@ -1,0 +1,987 @@
+// Host orchestration of the multi-scene WCSPH engine: allocation, scene admission and
+// repacking, the tile work list, substep/tick launch sequences (captured as CUDA graphs),
+// per-kernel device timers, and the per-scene export paths.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "sph_engine.cuh"
+#include "sph_engine.h"
+#include "vxl_sph_internal.h"
+
+namespace vxl {
+
+namespace {
+
+thread_local std::string g_last_error;
+
+#define CU(call)                                                                                 \
+  do {                                                                                           \
+    cudaError_t e_ = (call);                                                                     \
+    if (e_ != cudaSuccess) return set_error(VXL_CUDA_ERROR, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+constexpr int kThreads = 256;
+inline uint32_t blocks_for(uint64_t n, int t = kThreads) { return (uint32_t)((n + t - 1) / t); }
+
+enum KernelId : int {
+  KID_GRIDBOX, KID_CELLOFF, KID_KEYS, KID_SCAN_PARTIAL, KID_SCAN_TOP, KID_SCAN_FINAL, KID_PLACE, KID_CANON,
+  KID_DENSITY, KID_FORCE, KID_BFORCE, KID_REACT_CHUNKS, KID_REACT_SPANS, KID_SCALE, KID_COUNT
+};
+const char* const kKernelNames[KID_COUNT] = {
+    "k_gridbox", "k_celloff", "k_keys", "k_scan_partial", "k_scan_top", "k_scan_final", "k_place", "k_canon",
+    "k_density", "k_force", "k_bforce", "k_react_chunks", "k_react_spans", "k_scale"};
+
+constexpr size_t kSceneHostBytes = offsetof(SceneDev, g);
+
+// crates/vxl-phys-fluid/src/fluid_access.rs:8-13: h, h2, k6, ks, w0, B in f32 with the
+// reference's operation order (host code is built with -ffp-contract=off).
+SphConst make_const(const vxl_sph_params& p, uint64_t nf, uint64_t nt, uint32_t max_bins) {
+  SphConst k{};
+  const float h = std::fmax(p.smoothing_radius, 1e-5f);
+  const float h2 = h * h;
+  const float pi = 3.14159265358979323846f;
+  k.h = h;
+  k.h2 = h2;
+  k.k6 = 315.0f / (64.0f * pi * vxl_powi(h, 9));
+  k.ks = 45.0f / (pi * vxl_powi(h, 6));
+  k.w0 = k.k6 * h2 * h2 * h2;
+  k.b_tait = p.sound_speed * p.sound_speed * p.rest_density / p.gamma_tait;
+  k.mass = p.particle_mass;
+  k.rho0 = p.rest_density;
+  k.gamma = p.gamma_tait;
+  k.eps = p.xsph_viscosity;
+  k.alpha_c = p.artificial_viscosity * p.sound_speed;
+  k.h001 = 0.01f * h2;
+  k.gx = p.gravity[0];
+  k.gy = p.gravity[1];
+  k.gz = p.gravity[2];
+  k.clamp_p = p.tensile_instability_suppression ? 1u : 0u;
+  k.gamma7 = std::fabs(p.gamma_tait - 7.0f) < 1e-6f ? 1u : 0u;
+  k.n_fluid = (uint32_t)nf;
+  k.n_total = (uint32_t)nt;
+  k.max_bins = max_bins;
+  return k;
+}
+
+}  // namespace
+
+vxl_status set_error(vxl_status s, const std::string& msg) {
+  g_last_error = msg;
+  return s;
+}
+
+}  // namespace vxl
+
+// Shared by every translation unit of the library (declared in vxl_sph_internal.h).
+void vxl_set_last_error(const char* msg) { vxl::set_error(VXL_OK, msg ? msg : ""); }
+const char* vxl_get_last_error() { return vxl::g_last_error.c_str(); }
+
+namespace vxl {
+
+uint64_t Engine::bytes_per_slot(uint32_t nbr_cap) {
+  // pos, vel (x2), orig, slot_of, cellrank, items, rc, press, acc, xsph, bforce, bpos,
+  // neighbour list + count, staging
+  return 4 * 16 + 4 + 4 + 8 + 8 + 8 + 4 + 16 + 16 + 16 + 16 + (uint64_t)nbr_cap * 4 + 4 + 32;
+}
+
+uint64_t Engine::bytes_per_cell() { return 8; }
+
+template <class T>
+vxl_status Engine::dalloc(T** p, size_t count) {
+  size_t bytes = count * sizeof(T);
+  if (bytes == 0) bytes = sizeof(T);
+  cudaError_t e = cudaMalloc((void**)p, bytes);
+  if (e != cudaSuccess) {
+    *p = nullptr;
+    cudaGetLastError();
+    return set_error(VXL_OUT_OF_MEMORY, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+  }
+  device_bytes_ += bytes;
+  return VXL_OK;
+}
+
+vxl_status Engine::create(int device, uint64_t slot_cap, uint64_t cell_cap, uint32_t scene_cap, Engine** out) {
+  *out = nullptr;
+  if (slot_cap == 0) slot_cap = 1;
+  if (slot_cap >= (1ull << 31)) return set_error(VXL_INVALID_ARGUMENT, "more than 2^31 particle slots");
+  if (cell_cap == 0 || cell_cap >= (1ull << 31)) return set_error(VXL_INVALID_ARGUMENT, "cell capacity out of range");
+  auto* e = new (std::nothrow) Engine();
+  if (!e) return set_error(VXL_OUT_OF_MEMORY, "host allocation failed");
+  e->device_ = device;
+  e->slot_cap_ = slot_cap;
+  e->cell_cap_ = cell_cap;
+  e->scene_cap_ = scene_cap ? scene_cap : 1;
+  e->tiles_h_ = new std::vector<TileDev>();
+  cudaError_t ce = cudaSetDevice(device);
+  if (ce == cudaSuccess) ce = cudaStreamCreateWithFlags(&e->own_stream_, cudaStreamNonBlocking);
+  if (ce != cudaSuccess) {
+    cudaGetLastError();
+    delete e;  // the destructor releases tiles_h_
+    return set_error(VXL_CUDA_ERROR, std::string("no usable CUDA device: ") + cudaGetErrorString(ce));
+  }
+  e->stream_ = e->own_stream_;
+  vxl_status s = e->alloc_all();
+  if (s != VXL_OK) {
+    delete e;
+    return s;
+  }
+  e->set_tuning(Tuning{});
+  *out = e;
+  return VXL_OK;
+}
+
+vxl_status Engine::alloc_all() {
+  vxl_status s = VXL_OK;
+  auto A = [&](vxl_status r) {
+    if (s == VXL_OK) s = r;
+  };
+  const size_t n = slot_cap_;
+  A(dalloc((float4**)&pos_[0], n));
+  A(dalloc((float4**)&pos_[1], n));
+  A(dalloc((float4**)&vel_[0], n));
+  A(dalloc((float4**)&vel_[1], n));
+  A(dalloc(&orig_, n));
+  A(dalloc(&slot_of_, n));
+  A(dalloc((uint2**)&cellrank_, n));
+  A(dalloc((uint2**)&items_, n));
+  A(dalloc((float2**)&rc_, n));
+  A(dalloc(&press_, n));
+  A(dalloc((float4**)&acc_, n));
+  A(dalloc((float4**)&xsph_, n));
+  A(dalloc((float4**)&bforce_, n));
+  A(dalloc((float4**)&bpos_, n));
+  A(dalloc(&nbr_, (size_t)nbr_cap_ * n));
+  A(dalloc(&nbr_n_, n));
+  A(dalloc(&stage_, 8 * n));
+  A(dalloc(&counts_, cell_cap_ + 1));
+  A(dalloc(&start_, cell_cap_ + 1));
+  A(dalloc(&partial_, cell_cap_ / kScanTile + 2));
+  A(dalloc(&sc_d_, scene_cap_));
+  tiles_cap_ = (uint32_t)(n / 64 + scene_cap_ + 1);
+  A(dalloc(&tiles_d_, tiles_cap_));
+  A(dalloc(&ctl_d_, 1));
+  if (s != VXL_OK) return s;
+  CU(cudaMallocHost((void**)&sc_h_, scene_cap_ * sizeof(SceneDev)));
+  CU(cudaMallocHost((void**)&ctl_h_, sizeof(EngineCtl)));
+  std::memset(sc_h_, 0, scene_cap_ * sizeof(SceneDev));
+  std::memset(ctl_h_, 0, sizeof(EngineCtl));
+  CU(cudaMemsetAsync(counts_, 0, (cell_cap_ + 1) * 4, stream_));
+  CU(cudaMemsetAsync(start_, 0, (cell_cap_ + 1) * 4, stream_));
+  CU(cudaMemsetAsync(ctl_d_, 0, sizeof(EngineCtl), stream_));
+  CU(cudaMemsetAsync(sc_d_, 0, scene_cap_ * sizeof(SceneDev), stream_));
+  CU(cudaMemsetAsync(acc_, 0, n * 16, stream_));
+  CU(cudaMemsetAsync(xsph_, 0, n * 16, stream_));
+  CU(cudaMemsetAsync(bforce_, 0, n * 16, stream_));
+  CU(cudaMemsetAsync(rc_, 0, n * 8, stream_));
+  CU(cudaMemsetAsync(press_, 0, n * 4, stream_));
+  CU(cudaStreamSynchronize(stream_));
+  return VXL_OK;
+}
+
+void Engine::free_all() {
+  if (graph_) cudaGraphExecDestroy(graph_);
+  graph_ = nullptr;
+  void* d[] = {pos_[0], pos_[1], vel_[0], vel_[1], orig_, slot_of_, cellrank_, items_, rc_, press_, acc_, xsph_,
+               bforce_, bpos_, nbr_, nbr_n_, stage_, counts_, start_, partial_, sc_d_, tiles_d_, ctl_d_, spans_d_,
+               chunks_d_, chunk_first_d_, react_partial_, breact_d_};
+  for (void* p : d)
+    if (p) cudaFree(p);
+  void* hp[] = {sc_h_, ctl_h_, spans_h_, chunks_h_, chunk_first_h_, breact_h_};
+  for (void* p : hp)
+    if (p) cudaFreeHost(p);
+  for (cudaEvent_t e : prof_ev_) cudaEventDestroy(e);
+  prof_ev_.clear();
+  if (own_stream_) cudaStreamDestroy(own_stream_);
+  own_stream_ = nullptr;
+}
+
+Engine::~Engine() {
+  cudaSetDevice(device_);
+  if (stream_) cudaStreamSynchronize(stream_);
+  free_all();
+  delete tiles_h_;
+}
+
+void Engine::set_stream(cudaStream_t s) {
+  prof_collect();
+  cudaStreamSynchronize(stream_);
+  stream_ = s ? s : own_stream_;
+}
+
+void Engine::set_tuning(const Tuning& t) {
+  tuning_ = t;
+  if (tuning_.block != 128 && tuning_.block != 256) tuning_.block = 256;
+  if (tuning_.tile < 128) tuning_.tile = 128;
+  tuning_.tile = (tuning_.tile / 128) * 128;
+  if (tuning_.waves < 1) tuning_.waves = 1;
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device_);
+  int occ_d = 1, occ_f = 1, occ_b = 1;
+  if (tuning_.block == 128) {
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_d, k_e_density<128>, 128, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_f, k_e_force<128>, 128, 0);
+  } else {
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_d, k_e_density<256>, 256, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_f, k_e_force<256>, 256, 0);
+  }
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_b, k_e_bforce, 128, 0);
+  cudaGetLastError();
+  grid_density_ = sms * std::max(1, occ_d) * (int)tuning_.waves;
+  grid_force_ = sms * std::max(1, occ_f) * (int)tuning_.waves;
+  grid_bforce_ = sms * std::max(1, occ_b);
+  if (graph_) {
+    cudaGraphExecDestroy(graph_);
+    graph_ = nullptr;
+  }
+  rebuild_tiles();
+}
+
+vxl_status Engine::rebuild_tiles() {
+  tiles_h_->clear();
+  for (uint32_t q = 0; q < scenes_.size(); ++q) {
+    const SceneInfo& si = scenes_[q];
+    const uint32_t n = si.nf + si.nb;
+    for (uint32_t f = 0; f < n; f += tuning_.tile)
+      tiles_h_->push_back(TileDev{q, si.base + f, std::min(tuning_.tile, n - f), 0u});
+  }
+  ntiles_ = (uint32_t)tiles_h_->size();
+  if (ntiles_ > tiles_cap_) return set_error(VXL_INVALID_ARGUMENT, "tile list above capacity");
+  if (ntiles_) {
+    CU(cudaMemcpyAsync(tiles_d_, tiles_h_->data(), ntiles_ * sizeof(TileDev), cudaMemcpyHostToDevice, stream_));
+    CU(cudaStreamSynchronize(stream_));
+  }
+  ++membership_epoch_;
+  return VXL_OK;
+}
+
+// Push the host-written part of every scene record (constants, dt, slot range).
+vxl_status Engine::push_scene_records(const std::vector<float>& dt) {
+  for (uint32_t q = 0; q < scenes_.size(); ++q) {
+    SceneDev& r = sc_h_[q];
+    const SceneInfo& si = scenes_[q];
+    r.k = make_const(si.params, si.nf, si.nf + si.nb, si.params.max_bins ? si.params.max_bins : (1u << 21));
+    r.k.mass = si.particle_mass;
+    r.dt = dt.empty() ? 0.f : dt[q];
+    r.vmax = r.dt > 0.f ? si.params.max_speed_frac * r.k.h / r.dt : 0.f;  // fluid_step.rs:112
+    r.vmax2 = r.vmax * r.vmax;
+    r.base = si.base;
+    r.count = si.nf + si.nb;
+  }
+  if (!scenes_.empty()) {
+    CU(cudaMemcpy2DAsync(sc_d_, sizeof(SceneDev), sc_h_, sizeof(SceneDev), kSceneHostBytes, scenes_.size(),
+                         cudaMemcpyHostToDevice, stream_));
+    CU(cudaStreamSynchronize(stream_));
+  }
+  return VXL_OK;
+}
+
+vxl_status Engine::recompute_scene_boxes(uint32_t q) {
+  static const uint32_t init[6] = {0xffffffffu, 0xffffffffu, 0xffffffffu, 0u, 0u, 0u};
+  const SceneInfo& si = scenes_[q];
+  const uint32_t n = si.nf + si.nb;
+  CU(cudaMemcpyAsync(sc_d_[q].fbox, init, sizeof(init), cudaMemcpyHostToDevice, stream_));
+  CU(cudaMemcpyAsync(sc_d_[q].bbox, init, sizeof(init), cudaMemcpyHostToDevice, stream_));
+  if (n) {
+    k_e_bbox<<<blocks_for(n), kThreads, 0, stream_>>>((const float4*)pos_[0], si.base, n, 1, sc_d_[q].fbox);
+    k_e_bbox<<<blocks_for(n), kThreads, 0, stream_>>>((const float4*)pos_[0], si.base, n, 0, sc_d_[q].bbox);
+  }
+  CU(cudaGetLastError());
+  CU(cudaStreamSynchronize(stream_));
+  return VXL_OK;
+}
+
+vxl_status Engine::add_scene(const vxl_sph_params& p, uint64_t nf, uint64_t nb, const float* pos, const float* vel,
+                             const float* pmass, uint64_t id, uint32_t* out_index) {
+  const uint64_t nt = nf + nb;
+  if (nt > 0 && (!pos || !vel)) return set_error(VXL_NULL_POINTER, "pos/vel is NULL");
+  if (nb > 0 && !pmass) return set_error(VXL_NULL_POINTER, "pmass is NULL with boundary particles");
+  const uint32_t max_bins = p.max_bins ? p.max_bins : (1u << 21);
+  if (max_bins > (1u << 21)) return set_error(VXL_INVALID_ARGUMENT, "max_bins above 2^21");
+  if (!(p.particle_mass > 0.0f) || !(p.rest_density > 0.0f) || !(p.gamma_tait > 0.0f))
+    return set_error(VXL_INVALID_ARGUMENT, "particle_mass, rest_density and gamma_tait must be positive");
+  if (pmass)
+    for (uint64_t i = 0; i < nf; ++i)
+      if (pmass[i] != p.particle_mass) return set_error(VXL_INVALID_ARGUMENT, "fluid pmass must equal params.particle_mass");
+  for (uint64_t i = nf; i < nt; ++i)
+    if (!(pmass[i] > 0.0f)) return set_error(VXL_INVALID_ARGUMENT, "boundary pmass must be positive");
+  if (used_ + nt > slot_cap_) return set_error(VXL_OUT_OF_MEMORY, "particle pool full");
+  if (scenes_.size() >= scene_cap_) return set_error(VXL_OUT_OF_MEMORY, "scene table full");
+  CU(cudaSetDevice(device_));
+  prof_collect();
+  CU(cudaStreamSynchronize(stream_));
+  SceneInfo si;
+  si.id = id;
+  si.base = (uint32_t)used_;
+  si.nf = (uint32_t)nf;
+  si.nb = (uint32_t)nb;
+  si.substeps = p.substeps ? p.substeps : 1;
+  si.particle_mass = p.particle_mass;
+  si.params = p;
+  si.params.max_bins = max_bins;
+  const uint32_t q = (uint32_t)scenes_.size();
+  scenes_.push_back(si);
+  used_ += nt;
+  if (nt) {
+    CU(cudaMemcpyAsync(stage_, pos, nt * 12, cudaMemcpyHostToDevice, stream_));
+    CU(cudaMemcpyAsync(stage_ + 3 * nt, vel, nt * 12, cudaMemcpyHostToDevice, stream_));
+    if (nb) CU(cudaMemcpyAsync(stage_ + 6 * nt, pmass, nt * 4, cudaMemcpyHostToDevice, stream_));
+    k_e_init_scene<<<blocks_for(nt), kThreads, 0, stream_>>>(stage_, stage_ + 3 * nt, stage_ + 6 * nt,
+                                                              (float4*)pos_[0], (float4*)vel_[0], orig_, slot_of_,
+                                                              (float4*)bpos_, si.base, (uint32_t)nt, (uint32_t)nf,
+                                                              p.particle_mass);
+    CU(cudaGetLastError());
+  }
+  vxl_status s = push_scene_records({});
+  if (s == VXL_OK) s = recompute_scene_boxes(q);
+  if (s == VXL_OK) s = rebuild_tiles();
+  spans_local_.resize(scenes_.size());
+  spans_dirty_ = true;
+  if (out_index) *out_index = q;
+  return s;
+}
+
+vxl_status Engine::remove_scenes(const std::vector<uint32_t>& indices) {
+  if (indices.empty()) return VXL_OK;
+  CU(cudaSetDevice(device_));
+  prof_collect();
+  CU(cudaStreamSynchronize(stream_));
+  std::vector<bool> drop(scenes_.size(), false);
+  for (uint32_t i : indices)
+    if (i < scenes_.size()) drop[i] = true;
+  std::vector<SceneInfo> keep;
+  std::vector<std::vector<vxl_sph_span>> keep_spans;
+  std::vector<uint4> moves;
+  uint32_t next = 0;
+  for (uint32_t q = 0; q < scenes_.size(); ++q) {
+    if (drop[q]) continue;
+    SceneInfo si = scenes_[q];
+    const uint32_t n = si.nf + si.nb;
+    moves.push_back(make_uint4(si.base, next, n, 0u));
+    si.base = next;
+    next += n;
+    keep.push_back(si);
+    keep_spans.push_back(q < spans_local_.size() ? spans_local_[q] : std::vector<vxl_sph_span>());
+  }
+  // copy every kept scene into the second buffer set at its new base, then back
+  if (!moves.empty() && next > 0) {
+    uint4* moves_d = (uint4*)stage_;  // staging holds >= 8 floats per slot
+    CU(cudaMemcpyAsync(moves_d, moves.data(), moves.size() * sizeof(uint4), cudaMemcpyHostToDevice, stream_));
+    uint32_t* orig_tmp = (uint32_t*)items_;
+    float4* bpos_tmp = (float4*)bforce_;
+    uint32_t maxn = 0;
+    for (auto& m : moves) maxn = std::max(maxn, m.z);
+    dim3 grid(std::max(1u, std::min(blocks_for(maxn), 1024u)), (uint32_t)moves.size());
+    k_e_move<<<grid, kThreads, 0, stream_>>>((const float4*)pos_[0], (const float4*)vel_[0], orig_,
+                                             (const float4*)bpos_, (float4*)pos_[1], (float4*)vel_[1], orig_tmp,
+                                             bpos_tmp, moves_d);
+    CU(cudaGetLastError());
+    CU(cudaMemcpyAsync(pos_[0], pos_[1], (size_t)next * 16, cudaMemcpyDeviceToDevice, stream_));
+    CU(cudaMemcpyAsync(vel_[0], vel_[1], (size_t)next * 16, cudaMemcpyDeviceToDevice, stream_));
+    CU(cudaMemcpyAsync(orig_, orig_tmp, (size_t)next * 4, cudaMemcpyDeviceToDevice, stream_));
+    CU(cudaMemcpyAsync(bpos_, bpos_tmp, (size_t)next * 16, cudaMemcpyDeviceToDevice, stream_));
+    k_e_slot_of<<<blocks_for(next), kThreads, 0, stream_>>>(orig_, slot_of_, next);
+    CU(cudaGetLastError());
+  }
+  scenes_.swap(keep);
+  spans_local_.swap(keep_spans);
+  used_ = next;
+  spans_dirty_ = true;
+  vxl_status s = push_scene_records({});
+  for (uint32_t q = 0; s == VXL_OK && q < scenes_.size(); ++q) s = recompute_scene_boxes(q);
+  if (s == VXL_OK) s = rebuild_tiles();
+  return s;
+}
+
+vxl_status Engine::upload_boundary(uint32_t q, const float* pos, const float* vel, uint64_t nb) {
+  if (q >= scenes_.size()) return set_error(VXL_INVALID_ARGUMENT, "scene index out of range");
+  const SceneInfo& si = scenes_[q];
+  if (nb != si.nb) return set_error(VXL_SIZE_MISMATCH, "boundary segment length differs from the scene (rebuild the scene)");
+  if (nb == 0) return VXL_OK;
+  if (!pos || !vel) return set_error(VXL_NULL_POINTER, "pos/vel is NULL");
+  CU(cudaSetDevice(device_));
+  static const uint32_t init[6] = {0xffffffffu, 0xffffffffu, 0xffffffffu, 0u, 0u, 0u};
+  CU(cudaMemcpyAsync(stage_, pos, nb * 12, cudaMemcpyHostToDevice, stream_));
+  CU(cudaMemcpyAsync(stage_ + 3 * nb, vel, nb * 12, cudaMemcpyHostToDevice, stream_));
+  CU(cudaMemcpyAsync(sc_d_[q].bbox, init, sizeof(init), cudaMemcpyHostToDevice, stream_));
+  k_e_upload_boundary<<<blocks_for(nb), kThreads, 0, stream_>>>(stage_, stage_ + 3 * nb, (float4*)pos_[0],
+                                                                 (float4*)vel_[0], slot_of_, (float4*)bpos_,
+                                                                 sc_d_[q].bbox, si.base, si.nf, si.nb);
+  CU(cudaGetLastError());
+  CU(cudaStreamSynchronize(stream_));  // the caller's arrays are borrowed for this call only
+  return VXL_OK;
+}
+
+vxl_status Engine::write_state(uint32_t q, const float* pos, const float* vel) {
+  if (q >= scenes_.size()) return set_error(VXL_INVALID_ARGUMENT, "scene index out of range");
+  const SceneInfo& si = scenes_[q];
+  const uint32_t n = si.nf + si.nb;
+  if (n == 0) return VXL_OK;
+  CU(cudaSetDevice(device_));
+  if (pos) CU(cudaMemcpyAsync(stage_, pos, (size_t)n * 12, cudaMemcpyHostToDevice, stream_));
+  if (vel) CU(cudaMemcpyAsync(stage_ + 3 * (size_t)n, vel, (size_t)n * 12, cudaMemcpyHostToDevice, stream_));
+  k_e_write_scene<<<blocks_for(n), kThreads, 0, stream_>>>(pos ? stage_ : nullptr, vel ? stage_ + 3 * (size_t)n : nullptr,
+                                                            (float4*)pos_[0], (float4*)vel_[0], orig_, (float4*)bpos_,
+                                                            si.base, n, si.nf);
+  CU(cudaGetLastError());
+  if (pos) return recompute_scene_boxes(q);  // synchronises
+  CU(cudaStreamSynchronize(stream_));
+  return VXL_OK;
+}
+
+vxl_status Engine::read_state(uint32_t q, float* pos, float* vel) {
+  if (q >= scenes_.size()) return set_error(VXL_INVALID_ARGUMENT, "scene index out of range");
+  const SceneInfo& si = scenes_[q];
+  const uint32_t n = si.nf + si.nb;
+  if (n == 0) return VXL_OK;
+  CU(cudaSetDevice(device_));
+  float* dp = stage_;
+  float* dv = stage_ + 3 * (size_t)n;
+  k_e_read_scene<<<blocks_for(n), kThreads, 0, stream_>>>((const float4*)pos_[0], (const float4*)vel_[0], orig_,
+                                                           pos ? dp : nullptr, vel ? dv : nullptr, si.base, n);
+  if (pos) CU(cudaMemcpyAsync(pos, dp, (size_t)n * 12, cudaMemcpyDeviceToHost, stream_));
+  if (vel) CU(cudaMemcpyAsync(vel, dv, (size_t)n * 12, cudaMemcpyDeviceToHost, stream_));
+  CU(cudaStreamSynchronize(stream_));
+  return VXL_OK;
+}
+
+vxl_status Engine::read_fields(uint32_t q, float* dens, float* press, float* acc, float* xsph, float* bforce) {
+  if (q >= scenes_.size()) return set_error(VXL_INVALID_ARGUMENT, "scene index out of range");
+  const SceneInfo& si = scenes_[q];
+  const uint32_t n = si.nf + si.nb;
+  if (n == 0) return VXL_OK;
+  if ((acc || xsph) && !record_) return set_error(VXL_NOT_READY, "acc/xsph are recorded only with set_record(1)");
+  CU(cudaSetDevice(device_));
+  float* d_d = stage_;
+  float* d_p = stage_ + (size_t)n;
+  float* d_a = stage_ + 2 * (size_t)n;
+  float* d_x = stage_ + 5 * (size_t)n;
+  k_e_read_fields<<<blocks_for(n), kThreads, 0, stream_>>>((const float2*)rc_, press_, (const float4*)acc_,
+                                                            (const float4*)xsph_, orig_, dens ? d_d : nullptr,
+                                                            press ? d_p : nullptr, acc ? d_a : nullptr,
+                                                            xsph ? d_x : nullptr, si.base, n);
+  if (dens) CU(cudaMemcpyAsync(dens, d_d, (size_t)n * 4, cudaMemcpyDeviceToHost, stream_));
+  if (press) CU(cudaMemcpyAsync(press, d_p, (size_t)n * 4, cudaMemcpyDeviceToHost, stream_));
+  if (acc) CU(cudaMemcpyAsync(acc, d_a, (size_t)n * 12, cudaMemcpyDeviceToHost, stream_));
+  if (xsph) CU(cudaMemcpyAsync(xsph, d_x, (size_t)n * 12, cudaMemcpyDeviceToHost, stream_));
+  if (bforce && si.nb) {
+    std::vector<float> tmp((size_t)si.nb * 4);
+    CU(cudaMemcpyAsync(tmp.data(), (float4*)bforce_ + si.base + si.nf, (size_t)si.nb * 16, cudaMemcpyDeviceToHost,
+                       stream_));
+    CU(cudaStreamSynchronize(stream_));
+    for (uint32_t k = 0; k < si.nb; ++k)
+      for (int a = 0; a < 3; ++a) bforce[3 * k + a] = tmp[4 * k + a];
+  }
+  CU(cudaStreamSynchronize(stream_));
+  return VXL_OK;
+}
+
+vxl_status Engine::export_grid(uint32_t q, uint32_t* items, uint32_t* start, uint64_t start_cap, uint32_t* bins,
+                               vxl_sph_grid_info* info) {
+  if (q >= scenes_.size()) return set_error(VXL_INVALID_ARGUMENT, "scene index out of range");
+  if (!ran_substep_) return set_error(VXL_NOT_READY, "no substep has run yet");
+  const SceneInfo& si = scenes_[q];
+  const uint32_t n = si.nf + si.nb;
+  CU(cudaSetDevice(device_));
+  SceneDev rec;
+  CU(cudaMemcpyAsync(&rec, sc_d_ + q, sizeof(SceneDev), cudaMemcpyDeviceToHost, stream_));
+  CU(cudaStreamSynchronize(stream_));
+  const uint64_t total = rec.cells;
+  if (info) {
+    info->min[0] = rec.g.minx;
+    info->min[1] = rec.g.miny;
+    info->min[2] = rec.g.minz;
+    info->inv = rec.g.inv;
+    info->bin = rec.g.bin;
+    info->dims[0] = rec.g.nx;
+    info->dims[1] = rec.g.ny;
+    info->dims[2] = rec.g.nz;
+    info->total = total;
+  }
+  uint32_t* tmp = (uint32_t*)stage_;
+  if (start) {
+    if (start_cap < total + 1) return set_error(VXL_SIZE_MISMATCH, "start buffer smaller than cells + 1");
+    if (total + 1 > 8ull * slot_cap_) return set_error(VXL_SIZE_MISMATCH, "table larger than the staging buffer");
+    k_e_export_start<<<blocks_for(total + 1), kThreads, 0, stream_>>>(start_, sc_d_, q, tmp);
+    CU(cudaMemcpyAsync(start, tmp, (total + 1) * 4, cudaMemcpyDeviceToHost, stream_));
+    CU(cudaStreamSynchronize(stream_));
+  }
+  if (items && n) {
+    k_e_export_items<<<blocks_for(n), kThreads, 0, stream_>>>(orig_, si.base, n, tmp);
+    CU(cudaMemcpyAsync(items, tmp, (size_t)n * 4, cudaMemcpyDeviceToHost, stream_));
+    CU(cudaStreamSynchronize(stream_));
+  }
+  if (bins && n) {
+    k_e_export_bins<<<blocks_for(std::max<uint64_t>(total, 1)), kThreads, 0, stream_>>>(start_, orig_, sc_d_, q, tmp);
+    CU(cudaMemcpyAsync(bins, tmp, (size_t)n * 4, cudaMemcpyDeviceToHost, stream_));
+    CU(cudaStreamSynchronize(stream_));
+  }
+  CU(cudaGetLastError());
+  return VXL_OK;
+}
+
+vxl_status Engine::bounds(uint32_t q, float lo[3], float hi[3]) {
+  if (q >= scenes_.size()) return set_error(VXL_INVALID_ARGUMENT, "scene index out of range");
+  CU(cudaSetDevice(device_));
+  uint32_t box[6];
+  CU(cudaMemcpyAsync(box, sc_d_[q].fbox, sizeof(box), cudaMemcpyDeviceToHost, stream_));
+  CU(cudaStreamSynchronize(stream_));
+  for (int a = 0; a < 3; ++a) {
+    lo[a] = vxl_o2f_host(box[a]);
+    hi[a] = vxl_o2f_host(box[3 + a]);
+  }
+  if (!(std::isfinite(lo[0]) && std::isfinite(hi[0]))) return set_error(VXL_NOT_READY, "no fluid bounds");
+  return VXL_OK;
+}
+
+vxl_status Engine::set_spans(uint32_t q, const vxl_sph_span* spans, uint32_t n) {
+  if (q >= scenes_.size()) return set_error(VXL_INVALID_ARGUMENT, "scene index out of range");
+  if (n && !spans) return set_error(VXL_NULL_POINTER, "spans is NULL with nspans > 0");
+  const SceneInfo& si = scenes_[q];
+  std::vector<vxl_sph_span> v(spans, spans + n);
+  for (uint32_t k = 0; k < n; ++k)
+    if (v[k].start < si.nf || v[k].end < v[k].start || v[k].end > si.nf + si.nb)
+      return set_error(VXL_INVALID_ARGUMENT, "span " + std::to_string(k) + " is outside the boundary segment");
+  if (spans_local_.size() < scenes_.size()) spans_local_.resize(scenes_.size());
+  const auto& old = spans_local_[q];
+  bool same = old.size() == v.size() && (v.empty() || std::memcmp(old.data(), v.data(), v.size() * sizeof(vxl_sph_span)) == 0);
+  if (!same) {
+    spans_local_[q] = v;
+    spans_dirty_ = true;
+  }
+  return VXL_OK;
+}
+
+// Global span and chunk tables (pinned mirrors, copied inside the tick graph).
+vxl_status Engine::stage_spans() {
+  if (!spans_dirty_) return VXL_OK;
+  prof_collect();
+  CU(cudaStreamSynchronize(stream_));
+  std::vector<SpanDev> sp;
+  std::vector<SpanChunk> ch;
+  std::vector<uint32_t> first;
+  span_scene_.clear();
+  for (uint32_t q = 0; q < scenes_.size() && q < spans_local_.size(); ++q)
+    for (const vxl_sph_span& s : spans_local_[q]) {
+      const uint32_t gs = scenes_[q].base + s.start, ge = scenes_[q].base + s.end;
+      const uint32_t idx = (uint32_t)sp.size();
+      sp.push_back(SpanDev{s.body, s.origin[0], s.origin[1], s.origin[2], gs, ge});
+      span_scene_.push_back(q);
+      first.push_back((uint32_t)ch.size());
+      for (uint32_t b = gs; b < ge; b += kReactChunk) ch.push_back(SpanChunk{idx, b, std::min(ge, b + kReactChunk), 0u});
+    }
+  first.push_back((uint32_t)ch.size());
+  const uint32_t ns = (uint32_t)sp.size(), nc = (uint32_t)ch.size();
+  if (ns > spans_cap_ || nc > chunks_cap_) {
+    void* d[] = {spans_d_, chunks_d_, chunk_first_d_, react_partial_, breact_d_};
+    for (void* p : d)
+      if (p) cudaFree(p);
+    void* hp[] = {spans_h_, chunks_h_, chunk_first_h_, breact_h_};
+    for (void* p : hp)
+      if (p) cudaFreeHost(p);
+    spans_d_ = nullptr; chunks_d_ = nullptr; chunk_first_d_ = nullptr; react_partial_ = nullptr; breact_d_ = nullptr;
+    spans_h_ = nullptr; chunks_h_ = nullptr; chunk_first_h_ = nullptr; breact_h_ = nullptr;
+    const uint32_t cap = std::max<uint32_t>(ns, 64), ccap = std::max<uint32_t>(nc, 256);
+    vxl_status s;
+    if ((s = dalloc(&spans_d_, cap)) != VXL_OK) return s;
+    if ((s = dalloc(&chunks_d_, ccap)) != VXL_OK) return s;
+    if ((s = dalloc(&chunk_first_d_, (size_t)cap + 1)) != VXL_OK) return s;
+    if ((s = dalloc(&react_partial_, (size_t)ccap * 6)) != VXL_OK) return s;
+    if ((s = dalloc(&breact_d_, (size_t)cap * 6)) != VXL_OK) return s;
+    CU(cudaMallocHost((void**)&spans_h_, cap * sizeof(SpanDev)));
+    CU(cudaMallocHost((void**)&chunks_h_, ccap * sizeof(SpanChunk)));
+    CU(cudaMallocHost((void**)&chunk_first_h_, (cap + 1) * sizeof(uint32_t)));
+    CU(cudaMallocHost((void**)&breact_h_, cap * 6 * sizeof(float)));
+    spans_cap_ = cap;
+    chunks_cap_ = ccap;
+  }
+  if (ns) std::memcpy(spans_h_, sp.data(), ns * sizeof(SpanDev));
+  if (nc) std::memcpy(chunks_h_, ch.data(), nc * sizeof(SpanChunk));
+  std::memcpy(chunk_first_h_, first.data(), first.size() * sizeof(uint32_t));
+  nspans_ = ns;
+  nchunks_ = nc;
+  spans_dirty_ = false;
+  if (graph_) {
+    cudaGraphExecDestroy(graph_);
+    graph_ = nullptr;
+  }
+  return VXL_OK;
+}
+
+// ---------------------------------------------------------------- profiling
+
+void Engine::record_event(cudaEvent_t e) {
+  if (capturing_) cudaEventRecordWithFlags(e, stream_, cudaEventRecordExternal);
+  else cudaEventRecord(e, stream_);
+}
+
+int Engine::prof_begin(int kid) {
+  if (!prof_) return -1;
+  if (2 * prof_used_ + 2 > prof_ev_.size()) return -1;  // pre-created in set_profile
+  const size_t i = prof_used_++;
+  prof_kid_[i] = kid;
+  record_event(prof_ev_[2 * i]);
+  return (int)i;
+}
+
+void Engine::prof_end(int i) {
+  if (i >= 0) record_event(prof_ev_[2 * i + 1]);
+}
+
+void Engine::prof_collect() {
+  if (!prof_pending_) return;
+  cudaStreamSynchronize(stream_);
+  for (size_t i = 0; i < prof_used_; ++i) {
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, prof_ev_[2 * i], prof_ev_[2 * i + 1]) == cudaSuccess) {
+      prof_ms_[prof_kid_[i]] += ms;
+      prof_n_[prof_kid_[i]] += 1;
+    } else {
+      cudaGetLastError();
+    }
+  }
+  prof_pending_ = false;
+}
+
+vxl_status Engine::set_profile(bool on) {
+  CU(cudaSetDevice(device_));
+  prof_collect();
+  prof_ = on;
+  uint32_t sub = 1;
+  for (auto& s : scenes_) sub = std::max(sub, s.substeps);
+  const size_t need = 2 * ((size_t)sub * (KID_COUNT + 2) + 8);
+  while (prof_ && prof_ev_.size() < need) {
+    cudaEvent_t e;
+    CU(cudaEventCreate(&e));
+    prof_ev_.push_back(e);
+  }
+  prof_kid_.resize(prof_ev_.size() / 2);
+  for (int k = 0; k < KID_COUNT; ++k) {
+    prof_ms_[k] = 0.0;
+    prof_n_[k] = 0;
+  }
+  if (graph_) {
+    cudaGraphExecDestroy(graph_);
+    graph_ = nullptr;
+  }
+  return VXL_OK;
+}
+
+vxl_status Engine::profile_read(uint32_t k, const char** name, double* ms, uint64_t* launches) {
+  if (k >= (uint32_t)KID_COUNT) return set_error(VXL_INVALID_ARGUMENT, "kernel index past the table");
+  CU(cudaSetDevice(device_));
+  prof_collect();
+  if (name) *name = kKernelNames[k];
+  if (ms) *ms = prof_ms_[k];
+  if (launches) *launches = prof_n_[k];
+  return VXL_OK;
+}
+
+#define LAUNCH(kid, ...)          \
+  do {                            \
+    int pe_ = prof_begin(kid);    \
+    __VA_ARGS__;                  \
+    prof_end(pe_);                \
+    launches_counter_ += 1;       \
+  } while (0)
+
+// ---------------------------------------------------------------- stepping
+
+void Engine::enqueue_substep(bool with_reactions) {
+  cudaStream_t st = stream_;
+  const uint32_t S = (uint32_t)scenes_.size();
+  const uint32_t key_blocks = std::min<uint32_t>(std::max<uint32_t>(ntiles_, 1), 148 * 8);
+  uint64_t nb_total = 0;
+  for (auto& s : scenes_) nb_total += s.nb;
+  const float4* p0 = (const float4*)pos_[0];
+  const float4* v0 = (const float4*)vel_[0];
+  const float4* p1 = (const float4*)pos_[1];
+  const float4* v1 = (const float4*)vel_[1];
+  cudaMemsetAsync(ctl_d_->work, 0, sizeof(ctl_d_->work), st);
+  LAUNCH(KID_GRIDBOX, k_e_gridbox<<<blocks_for(S, 128), 128, 0, st>>>(sc_d_, S, ctl_d_));
+  LAUNCH(KID_CELLOFF, k_e_celloff<<<1, 1024, 0, st>>>(sc_d_, S, ctl_d_, (uint32_t)cell_cap_));
+  LAUNCH(KID_KEYS, k_e_keys<<<key_blocks, kThreads, 0, st>>>(p0, sc_d_, tiles_d_, ntiles_, ctl_d_, counts_,
+                                                             (uint2*)cellrank_));
+  LAUNCH(KID_SCAN_PARTIAL, k_e_scan_partial<<<148 * 4, kScanThreads, 0, st>>>(counts_, ctl_d_, partial_));
+  LAUNCH(KID_SCAN_TOP, k_e_scan_top<<<1, 1024, 0, st>>>(partial_, ctl_d_, start_));
+  LAUNCH(KID_SCAN_FINAL, k_e_scan_final<<<148 * 4, kScanThreads, 0, st>>>(counts_, ctl_d_, partial_, start_));
+  LAUNCH(KID_PLACE, k_e_place<<<key_blocks, kThreads, 0, st>>>((const uint2*)cellrank_, start_, orig_, tiles_d_,
+                                                               ntiles_, ctl_d_, (uint2*)items_));
+  LAUNCH(KID_CANON, k_e_canon<<<148 * 8, 256, 0, st>>>((const uint2*)items_, start_, ctl_d_, p0, v0, (float4*)pos_[1],
+                                                       (float4*)vel_[1], orig_, slot_of_));
+  const uint32_t stride = (uint32_t)slot_cap_;
+  const bool rec = record_;
+  if (tuning_.block == 128) {
+    LAUNCH(KID_DENSITY, k_e_density<128><<<grid_density_, 128, 0, st>>>(p1, start_, sc_d_, tiles_d_, ntiles_, ctl_d_,
+                                                                        (float2*)rc_, press_, nbr_, nbr_n_, nbr_cap_,
+                                                                        stride));
+    LAUNCH(KID_FORCE, k_e_force<128><<<grid_force_, 128, 0, st>>>(
+                          p1, v1, (const float2*)rc_, start_, nbr_, nbr_n_, nbr_cap_, stride, sc_d_, tiles_d_,
+                          ntiles_, ctl_d_, (float4*)pos_[0], (float4*)vel_[0], rec ? (float4*)acc_ : nullptr,
+                          rec ? (float4*)xsph_ : nullptr));
+  } else {
+    LAUNCH(KID_DENSITY, k_e_density<256><<<grid_density_, 256, 0, st>>>(p1, start_, sc_d_, tiles_d_, ntiles_, ctl_d_,
+                                                                        (float2*)rc_, press_, nbr_, nbr_n_, nbr_cap_,
+                                                                        stride));
+    LAUNCH(KID_FORCE, k_e_force<256><<<grid_force_, 256, 0, st>>>(
+                          p1, v1, (const float2*)rc_, start_, nbr_, nbr_n_, nbr_cap_, stride, sc_d_, tiles_d_,
+                          ntiles_, ctl_d_, (float4*)pos_[0], (float4*)vel_[0], rec ? (float4*)acc_ : nullptr,
+                          rec ? (float4*)xsph_ : nullptr));
+  }
+  if (nb_total > 0 && ((with_reactions && nspans_ > 0) || rec)) {
+    LAUNCH(KID_BFORCE, k_e_bforce<<<grid_bforce_, 128, 0, st>>>(p1, v1, (const float2*)rc_, start_, orig_, nbr_,
+                                                                nbr_n_, nbr_cap_, stride, sc_d_, tiles_d_, ntiles_,
+                                                                ctl_d_, (float4*)bforce_));
+  }
+  if (with_reactions && nspans_ > 0 && nchunks_ > 0) {
+    LAUNCH(KID_REACT_CHUNKS, k_react_chunks<<<nchunks_, kReactThreads, 0, st>>>(
+                                 (const float4*)bforce_, (const float4*)bpos_, spans_d_, chunks_d_, ctl_d_,
+                                 react_partial_));
+    LAUNCH(KID_REACT_SPANS, k_react_spans<<<blocks_for(nspans_, 64), 64, 0, st>>>(react_partial_, chunk_first_d_,
+                                                                                  ctl_d_, breact_d_, nspans_));
+  }
+}
+
+void Engine::enqueue_tick(float /*dt_tick*/) {
+  cudaStream_t st = stream_;
+  const uint32_t sub = scenes_.empty() ? 1 : scenes_[0].substeps;
+  if (nspans_ > 0) {
+    cudaMemcpyAsync(spans_d_, spans_h_, nspans_ * sizeof(SpanDev), cudaMemcpyHostToDevice, st);
+    if (nchunks_) cudaMemcpyAsync(chunks_d_, chunks_h_, nchunks_ * sizeof(SpanChunk), cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(chunk_first_d_, chunk_first_h_, (nspans_ + 1) * sizeof(uint32_t), cudaMemcpyHostToDevice, st);
+    cudaMemsetAsync(breact_d_, 0, nspans_ * 6 * sizeof(float), st);
+  }
+  for (uint32_t s = 0; s < sub; ++s) enqueue_substep(true);
+  if (nspans_ > 0) {
+    if (sub > 1) {
+      const float inv = 1.0f / (float)sub;  // fluid_step.rs:85
+      LAUNCH(KID_SCALE, k_scale<<<blocks_for(nspans_ * 6), kThreads, 0, st>>>(breact_d_, nspans_ * 6, inv));
+    }
+    cudaMemcpyAsync(breact_h_, breact_d_, nspans_ * 6 * sizeof(float), cudaMemcpyDeviceToHost, st);
+  }
+  cudaMemcpyAsync(ctl_h_, ctl_d_, sizeof(EngineCtl), cudaMemcpyDeviceToHost, st);
+}
+
+vxl_status Engine::step_tick_async(float dt_tick) {
+  if (!(dt_tick > 0.0f) || !std::isfinite(dt_tick)) return set_error(VXL_INVALID_ARGUMENT, "dt_tick must be > 0");
+  CU(cudaSetDevice(device_));
+  if (scenes_.empty()) return VXL_OK;
+  const uint32_t sub = scenes_[0].substeps;
+  bool any_fluid = false;
+  for (auto& s : scenes_) {
+    if (s.substeps != sub) return set_error(VXL_INVALID_ARGUMENT, "scenes of one tick must share substeps");
+    any_fluid = any_fluid || s.nf > 0;
+  }
+  if (!any_fluid) return VXL_OK;  // fluid_step.rs:93-95: boundary particles are not driven alone
+  // per-scene substep dt = dt_tick / substeps (fluid_step.rs:77)
+  const float dt = dt_tick / (float)sub;
+  bool push = false;
+  for (uint32_t q = 0; q < scenes_.size(); ++q)
+    if (sc_h_[q].dt != dt) push = true;
+  prof_collect();
+  if (push) {
+    CU(cudaStreamSynchronize(stream_));
+    vxl_status s = push_scene_records(std::vector<float>(scenes_.size(), dt));
+    if (s != VXL_OK) return s;
+  }
+  vxl_status s = stage_spans();
+  if (s != VXL_OK) return s;
+  const uint32_t key = (record_ ? 1u : 0u) | (prof_ ? 2u : 0u) | (sub << 2);
+  launches_counter_ = 0;
+  if (!use_graph_) {
+    prof_used_ = 0;
+    enqueue_tick(dt_tick);
+    prof_pending_ = prof_;
+    launches_last_tick_ = launches_counter_;
+    CU(cudaGetLastError());
+    ran_substep_ = true;
+    return VXL_OK;
+  }
+  if (!graph_ || graph_key_ != key || graph_epoch_ != membership_epoch_) {
+    if (graph_) {
+      cudaGraphExecDestroy(graph_);
+      graph_ = nullptr;
+    }
+    cudaGraph_t g = nullptr;
+    prof_used_ = 0;
+    CU(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
+    capturing_ = true;
+    enqueue_tick(dt_tick);
+    capturing_ = false;
+    CU(cudaStreamEndCapture(stream_, &g));
+    cudaError_t e = cudaGraphInstantiate(&graph_, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return set_error(VXL_CUDA_ERROR, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
+    graph_key_ = key;
+    graph_epoch_ = membership_epoch_;
+    launches_last_tick_ = launches_counter_;
+  }
+  CU(cudaGraphLaunch(graph_, stream_));
+  prof_pending_ = prof_;
+  ran_substep_ = true;
+  return VXL_OK;
+}
+
+vxl_status Engine::finish() {
+  CU(cudaStreamSynchronize(stream_));
+  prof_collect();
+  if (ctl_h_->err & kErrGridLoop) return set_error(VXL_DEVICE_FAULT_FLAG, "grid box doubling loop did not settle");
+  if (ctl_h_->err & kErrCellCap) {
+    ctl_h_->err = 0;
+    cudaMemsetAsync(&ctl_d_->err, 0, 4, stream_);
+    cudaStreamSynchronize(stream_);
+    return set_error(VXL_DEVICE_FAULT_FLAG, "the scenes' cells exceed the engine's cell capacity; the substep was skipped");
+  }
+  return VXL_OK;
+}
+
+vxl_status Engine::sync(std::vector<vxl_sph_reaction>* out) {
+  CU(cudaSetDevice(device_));
+  vxl_status s = finish();
+  if (s != VXL_OK) return s;
+  if (out) {
+    out->resize(nspans_);
+    for (uint32_t q = 0; q < nspans_; ++q) {
+      (*out)[q].body = spans_h_[q].body;
+      for (int a = 0; a < 3; ++a) {
+        (*out)[q].force[a] = breact_h_[6 * q + a];
+        (*out)[q].torque[a] = breact_h_[6 * q + 3 + a];
+      }
+    }
+  }
+  return VXL_OK;
+}
+
+vxl_status Engine::substep(const std::vector<float>& dt) {
+  CU(cudaSetDevice(device_));
+  if (scenes_.empty()) return VXL_OK;
+  if (dt.size() != scenes_.size()) return set_error(VXL_SIZE_MISMATCH, "one dt per scene");
+  bool any_fluid = false;
+  for (auto& s : scenes_) any_fluid = any_fluid || s.nf > 0;
+  if (!any_fluid) return VXL_OK;
+  prof_collect();
+  bool push = false;
+  for (uint32_t q = 0; q < scenes_.size(); ++q)
+    if (sc_h_[q].dt != dt[q]) push = true;
+  if (push) {
+    CU(cudaStreamSynchronize(stream_));
+    vxl_status s = push_scene_records(dt);
+    if (s != VXL_OK) return s;
+  }
+  prof_used_ = 0;
+  launches_counter_ = 0;
+  enqueue_substep(false);
+  cudaMemcpyAsync(ctl_h_, ctl_d_, sizeof(EngineCtl), cudaMemcpyDeviceToHost, stream_);
+  prof_pending_ = prof_;
+  launches_last_tick_ = launches_counter_;
+  CU(cudaGetLastError());
+  ran_substep_ = true;
+  return finish();
+}
+
+vxl_status Engine::autotune(float dt_tick, uint32_t trials, Tuning* best, float* best_ms) {
+  if (!(dt_tick > 0.0f)) return set_error(VXL_INVALID_ARGUMENT, "dt_tick must be > 0");
+  CU(cudaSetDevice(device_));
+  if (scenes_.empty() || used_ == 0) return set_error(VXL_NOT_READY, "no scene to tune on");
+  prof_collect();
+  CU(cudaStreamSynchronize(stream_));
+  const bool prof_was = prof_;
+  prof_ = false;
+  const uint32_t S = (uint32_t)scenes_.size();
+  std::vector<float> dt(S);
+  for (uint32_t q = 0; q < S; ++q) dt[q] = dt_tick / (float)scenes_[q].substeps;
+  vxl_status st = push_scene_records(dt);
+  if (st != VXL_OK) return st;
+  // snapshot of the state the trials start from
+  const size_t n = used_;
+  void* snap = nullptr;
+  const size_t bytes = n * (16 + 16 + 4 + 16) + S * sizeof(SceneDev);
+  if (cudaMalloc(&snap, bytes) != cudaSuccess) {
+    cudaGetLastError();
+    return set_error(VXL_OUT_OF_MEMORY, "autotune snapshot");
+  }
+  char* sp = (char*)snap;
+  float4* s_pos = (float4*)sp;
+  float4* s_vel = (float4*)(sp + n * 16);
+  float4* s_bpos = (float4*)(sp + n * 32);
+  uint32_t* s_orig = (uint32_t*)(sp + n * 48);
+  SceneDev* s_sc = (SceneDev*)(sp + n * 52);
+  auto copy_all = [&](bool save) -> vxl_status {
+    cudaMemcpyKind k = cudaMemcpyDeviceToDevice;
+    CU(cudaMemcpyAsync(save ? (void*)s_pos : pos_[0], save ? pos_[0] : (void*)s_pos, n * 16, k, stream_));
+    CU(cudaMemcpyAsync(save ? (void*)s_vel : vel_[0], save ? vel_[0] : (void*)s_vel, n * 16, k, stream_));
+    CU(cudaMemcpyAsync(save ? (void*)s_bpos : bpos_, save ? bpos_ : (void*)s_bpos, n * 16, k, stream_));
+    CU(cudaMemcpyAsync(save ? (void*)s_orig : (void*)orig_, save ? (void*)orig_ : (void*)s_orig, n * 4, k, stream_));
+    CU(cudaMemcpyAsync(save ? (void*)s_sc : (void*)sc_d_, save ? (void*)sc_d_ : (void*)s_sc, S * sizeof(SceneDev), k,
+                       stream_));
+    if (!save) k_e_slot_of<<<blocks_for(n), kThreads, 0, stream_>>>(orig_, slot_of_, (uint32_t)n);
+    CU(cudaStreamSynchronize(stream_));
+    return VXL_OK;
+  };
+  st = copy_all(true);
+  const Tuning was = tuning_;
+  Tuning best_t = was;
+  float best_v = 1e30f;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  const uint32_t blocks[2] = {128, 256};
+  const uint32_t tiles_c[5] = {256, 512, 1024, 2048, 4096};
+  const uint32_t waves_c[2] = {1, 2};
+  for (uint32_t bi = 0; st == VXL_OK && bi < 2; ++bi)
+    for (uint32_t ti = 0; st == VXL_OK && ti < 5; ++ti)
+      for (uint32_t wi = 0; st == VXL_OK && wi < 2; ++wi) {
+        st = copy_all(false);
+        if (st != VXL_OK) break;
+        set_tuning(Tuning{blocks[bi], tiles_c[ti], waves_c[wi]});
+        enqueue_substep(false);  // warm-up
+        cudaEventRecord(e0, stream_);
+        for (uint32_t r = 0; r < trials; ++r) enqueue_substep(false);
+        cudaEventRecord(e1, stream_);
+        if (cudaStreamSynchronize(stream_) != cudaSuccess) {
+          st = set_error(VXL_CUDA_ERROR, "autotune trial failed");
+          break;
+        }
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        ms /= (float)trials;
+        if (ms < best_v) {
+          best_v = ms;
+          best_t = tuning_;
+        }
+      }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (st == VXL_OK) st = copy_all(false);
+  set_tuning(st == VXL_OK ? best_t : was);
+  cudaFree(snap);
+  prof_ = prof_was;
+  if (st != VXL_OK) return st;
+  CU(cudaMemcpyAsync(ctl_h_, ctl_d_, sizeof(EngineCtl), cudaMemcpyDeviceToHost, stream_));
+  st = finish();
+  if (st != VXL_OK) return st;
+  if (best) *best = best_t;
+  if (best_ms) *best_ms = best_v;
+  return VXL_OK;
+}
+
+uint32_t Engine::cells_last() {
+  EngineCtl c;
+  cudaMemcpyAsync(&c, ctl_d_, sizeof(EngineCtl), cudaMemcpyDeviceToHost, stream_);
+  cudaStreamSynchronize(stream_);
+  return c.cells;
+}
+
+uint32_t Engine::slow_gathers() {
+  EngineCtl c;
+  cudaMemcpyAsync(&c, ctl_d_, sizeof(EngineCtl), cudaMemcpyDeviceToHost, stream_);
+  cudaStreamSynchronize(stream_);
+  return c.slow_gathers;
+}
+
+}  // namespace vxl

@@ -1,0 +1,1007 @@
+// Multi-scene WCSPH engine: the device kernels of one substep for any number of
+// resident scenes (sm_100a). One scene is the plain drop-in; many scenes are the
+// batched and served forms.
+//
+// Layout. All scenes share one pool of particle slots, packed without gaps in scene
+// order: scene q owns slots [base_q, base_q + n_q) and its particles never leave that
+// range. Per slot (structure of arrays):
+//   pos[s]  float4 (x, y, z, m)   m = +particle mass for fluid, -pmass for boundary
+//   vel[s]  float4 (vx, vy, vz, 0)
+//   orig[s] global reference index (base_q + the particle's index in its scene);
+//           slot_of[orig[s]] == s
+// Each substep every scene gets its own grid (the reference's grid rule on its own
+// AABB, crates/vxl-phys-core/src/grid.rs:34-50) and a range of a global cell space
+// [cell_off_q, cell_off_q + cells_q), assigned in scene order. A particle's key is
+// cell_off_q + its cell, so one counting sort over the global cells is a segmented sort
+// that keeps each scene inside its slot range, and inside every cell the slots ascend by
+// reference index: the reference's table (crates/vxl-phys-fluid/src/grid.rs:29-76).
+// Walking a scene's 27 cells in the reference's (dz, dy, dx) order over those ranges
+// visits neighbours in the order of UniformGrid::for_neighbors_in (grid.rs:115-155),
+// so every per-particle sum matches the reference's CPU path bit for bit.
+//
+// Work list. The particle kernels run persistent blocks over a list of tiles
+// (scene, first slot, count): a block takes the next tile from an atomic counter, so the
+// scene of a tile is uniform and scenes of very different sizes balance across SMs.
+//
+// Substep: gridbox (per scene) -> cell offsets -> keys -> scan -> place -> canon ->
+// density + EOS (+ neighbour lists) -> force + XSPH + integrate -> boundary reactions ->
+// per-span reduction.
+#pragma once
+
+#include "sph_device.cuh"
+
+namespace vxl {
+
+constexpr uint32_t kErrCellCap = 1u << 3;  // the scenes' cells exceed the cell capacity
+
+// Per-scene device record (one per scene of the engine). The fields up to `g` are
+// written by the host (constants, substep dt, slot range); the rest by the kernels.
+struct SceneDev {
+  SphConst k;
+  float dt, vmax, vmax2, pad0;
+  uint32_t base;        // first slot
+  uint32_t count;       // slots (fluid + boundary)
+  uint32_t pad1[2];
+  GridBox g;            // this substep's grid
+  uint32_t cell_off;    // first global cell this substep
+  uint32_t cells;       // cells this substep
+  uint32_t fbox[6];     // fluid AABB accumulator (ordered uint)
+  uint32_t bbox[6];     // boundary AABB (fixed within a tick)
+};
+
+struct TileDev {
+  uint32_t scene, first, count, pad;
+};
+
+// Body span (global reference indices [start, end)) and its reduction chunks.
+struct SpanDev {
+  uint32_t body;
+  float ox, oy, oz;
+  uint32_t start, end;
+};
+
+struct SpanChunk {
+  uint32_t span, begin, end, pad;
+};
+
+constexpr uint32_t kReactChunk = 4096;
+constexpr int kReactThreads = 256;
+
+// Engine-wide control block.
+constexpr int kWorkSlots = 16;  // persistent-kernel work counters per substep
+struct EngineCtl {
+  uint32_t cells;  // sum of the scenes' cells this substep
+  uint32_t err;
+  uint32_t slow_gathers;
+  uint32_t pad;
+  uint32_t work[kWorkSlots];
+};
+
+// Work counter indices.
+enum WorkId : int { kWorkDensity = 0, kWorkForce = 1, kWorkBforce = 2 };
+
+namespace {
+
+constexpr int kScanTile = 2048;
+constexpr int kScanThreads = 256;
+constexpr int kCanonSmem = 1024;
+constexpr int kBGatherCap = 64;
+
+// Block-level ordered-uint min/max of (x, y, z), one atomic per component into acc.
+__device__ __forceinline__ void block_bbox_accumulate(uint32_t* acc, float x, float y, float z, bool valid) {
+  uint32_t mn[3], mx[3];
+  const float v[3] = {x, y, z};
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    const bool ok = valid && (v[a] == v[a]);  // NaN never wins (Rust f32::min/max ignore NaN)
+    mn[a] = ok ? f2o(v[a]) : 0xffffffffu;
+    mx[a] = ok ? f2o(v[a]) : 0u;
+  }
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      mn[a] = min(mn[a], __shfl_xor_sync(0xffffffffu, mn[a], off));
+      mx[a] = max(mx[a], __shfl_xor_sync(0xffffffffu, mx[a], off));
+    }
+  }
+  __shared__ uint32_t s_mn[3][32], s_mx[3][32];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+  if (lane == 0) {
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      s_mn[a][wid] = mn[a];
+      s_mx[a][wid] = mx[a];
+    }
+  }
+  __syncthreads();
+  if (wid == 0) {
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      mn[a] = lane < nw ? s_mn[a][lane] : 0xffffffffu;
+      mx[a] = lane < nw ? s_mx[a][lane] : 0u;
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        mn[a] = min(mn[a], __shfl_xor_sync(0xffffffffu, mn[a], off));
+        mx[a] = max(mx[a], __shfl_xor_sync(0xffffffffu, mx[a], off));
+      }
+    }
+    if (lane == 0) {
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        if (mn[a] != 0xffffffffu) atomicMin(&acc[a], mn[a]);
+        if (mx[a] != 0u) atomicMax(&acc[3 + a], mx[a]);
+      }
+    }
+  }
+  __syncthreads();
+}
+
+// Next tile of a persistent kernel (block-uniform); >= ntiles means done.
+__device__ __forceinline__ uint32_t next_tile(uint32_t* counter) {
+  __shared__ uint32_t s_tile;
+  if (threadIdx.x == 0) s_tile = atomicAdd(counter, 1u);
+  __syncthreads();
+  const uint32_t t = s_tile;
+  __syncthreads();
+  return t;
+}
+
+// ---------------------------------------------------------------- set-up kernels
+
+// Scatter one scene's host-order input (xyz triples, scene-local index) into its slots
+// [base, base + n) in reference order.
+__global__ void k_e_init_scene(const float* __restrict__ pin, const float* __restrict__ vin,
+                               const float* __restrict__ pm, float4* __restrict__ pos, float4* __restrict__ vel,
+                               uint32_t* __restrict__ orig, uint32_t* __restrict__ slot_of,
+                               float4* __restrict__ bpos, uint32_t base, uint32_t n, uint32_t nf, float mass) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float x = pin[3 * i], y = pin[3 * i + 1], z = pin[3 * i + 2];
+  const bool fluid = i < nf;
+  const uint32_t g = base + i;
+  pos[g] = make_float4(x, y, z, fluid ? mass : -pm[i]);
+  vel[g] = make_float4(vin[3 * i], vin[3 * i + 1], vin[3 * i + 2], 0.0f);
+  orig[g] = g;
+  slot_of[g] = g;
+  if (!fluid) bpos[g] = make_float4(x, y, z, 0.0f);
+}
+
+// Overwrite one scene's positions/velocities (scene-local reference order input),
+// keeping its current slot order.
+__global__ void k_e_write_scene(const float* __restrict__ pin, const float* __restrict__ vin,
+                                float4* __restrict__ pos, float4* __restrict__ vel,
+                                const uint32_t* __restrict__ orig, float4* __restrict__ bpos, uint32_t base,
+                                uint32_t n, uint32_t nf) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint32_t s = base + i;
+  const uint32_t o = orig[s] - base;
+  if (pin) {
+    float4 p = pos[s];
+    p.x = pin[3 * o];
+    p.y = pin[3 * o + 1];
+    p.z = pin[3 * o + 2];
+    pos[s] = p;
+    if (o >= nf) bpos[base + o] = make_float4(p.x, p.y, p.z, 0.0f);
+  }
+  if (vin) vel[s] = make_float4(vin[3 * o], vin[3 * o + 1], vin[3 * o + 2], 0.0f);
+}
+
+// Boundary segment re-upload of one scene (crates/vxl-phys-gpu/src/pipeline/coupling.rs:
+// 20-50): boundary particle k of the scene sits in slot slot_of[base + nf + k].
+__global__ void k_e_upload_boundary(const float* __restrict__ pin, const float* __restrict__ vin,
+                                    float4* __restrict__ pos, float4* __restrict__ vel,
+                                    const uint32_t* __restrict__ slot_of, float4* __restrict__ bpos,
+                                    uint32_t* __restrict__ bbox_acc, uint32_t base, uint32_t nf, uint32_t nb) {
+  const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool valid = q < nb;
+  float x = 0, y = 0, z = 0;
+  if (valid) {
+    const uint32_t g = base + nf + q;
+    const uint32_t s = slot_of[g];
+    x = pin[3 * q];
+    y = pin[3 * q + 1];
+    z = pin[3 * q + 2];
+    float4 p = pos[s];
+    p.x = x;
+    p.y = y;
+    p.z = z;
+    pos[s] = p;
+    vel[s] = make_float4(vin[3 * q], vin[3 * q + 1], vin[3 * q + 2], 0.0f);
+    bpos[g] = make_float4(x, y, z, 0.0f);
+  }
+  block_bbox_accumulate(bbox_acc, x, y, z, valid);
+}
+
+// AABB of one scene's fluid (pos.w > 0) or boundary (pos.w < 0) slots into acc.
+__global__ void k_e_bbox(const float4* __restrict__ pos, uint32_t base, uint32_t n, int want_fluid,
+                         uint32_t* __restrict__ acc) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  float4 p = make_float4(0, 0, 0, 0);
+  bool valid = false;
+  if (i < n) {
+    p = pos[base + i];
+    valid = want_fluid ? (p.w > 0.0f) : (p.w < 0.0f);
+  }
+  block_bbox_accumulate(acc, p.x, p.y, p.z, valid);
+}
+
+// Move whole scenes to new bases (the served form's repack): slot ranges are copied into
+// the second buffer set, reference indices shifted by the move. from_base/to_base/count
+// per moved scene; one block row per scene (blockIdx.y).
+__global__ void k_e_move(const float4* __restrict__ pos_in, const float4* __restrict__ vel_in,
+                         const uint32_t* __restrict__ orig_in, const float4* __restrict__ bpos_in,
+                         float4* __restrict__ pos_out, float4* __restrict__ vel_out, uint32_t* __restrict__ orig_out,
+                         float4* __restrict__ bpos_out, const uint4* __restrict__ moves) {
+  const uint4 m = moves[blockIdx.y];  // from, to, count, -
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < m.z; i += gridDim.x * blockDim.x) {
+    pos_out[m.y + i] = pos_in[m.x + i];
+    vel_out[m.y + i] = vel_in[m.x + i];
+    orig_out[m.y + i] = orig_in[m.x + i] - m.x + m.y;
+    bpos_out[m.y + i] = bpos_in[m.x + i];
+  }
+}
+
+__global__ void k_e_slot_of(const uint32_t* __restrict__ orig, uint32_t* __restrict__ slot_of, uint32_t n) {
+  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s < n) slot_of[orig[s]] = s;
+}
+
+// ---------------------------------------------------------------- substep kernels
+
+// Per scene: grid box of this substep from the AABB of all its particles
+// (crates/vxl-phys-fluid/src/grid.rs:37-44 -> crates/vxl-phys-core/src/grid.rs:34-50),
+// then reset the fluid accumulator for the force kernel's epilogue.
+__global__ void k_e_gridbox(SceneDev* __restrict__ sc, uint32_t nscenes, EngineCtl* ctl) {
+  const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= nscenes) return;
+  SceneDev& s = sc[q];
+  float lo[3], hi[3];
+  for (int a = 0; a < 3; ++a) {
+    lo[a] = fminf(o2f(s.fbox[a]), o2f(s.bbox[a]));
+    hi[a] = fmaxf(o2f(s.fbox[3 + a]), o2f(s.bbox[3 + a]));
+  }
+  GridBox g;
+  if (!grid_box(lo[0], lo[1], lo[2], hi[0], hi[1], hi[2], s.k.h, s.k.max_bins, g)) atomicOr(&ctl->err, kErrGridLoop);
+  s.g = g;
+  s.cells = g.total;
+  for (int a = 0; a < 3; ++a) {
+    s.fbox[a] = 0xffffffffu;
+    s.fbox[3 + a] = 0u;
+  }
+}
+
+// Cell offsets: exclusive scan of the scenes' cell counts (one block, any scene count);
+// flags the substep when the total exceeds the cell capacity (every later kernel then
+// returns without touching memory).
+__global__ void k_e_celloff(SceneDev* __restrict__ sc, uint32_t nscenes, EngineCtl* ctl, uint32_t cell_cap) {
+  __shared__ uint32_t sh[1024];
+  __shared__ unsigned long long carry;
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  for (uint32_t b0 = 0; b0 < nscenes; b0 += 1024) {
+    const uint32_t q = b0 + threadIdx.x;
+    const uint32_t v = q < nscenes ? sc[q].cells : 0u;
+    sh[threadIdx.x] = v;
+    __syncthreads();
+    for (uint32_t off = 1; off < 1024; off <<= 1) {
+      const uint32_t add = threadIdx.x >= off ? sh[threadIdx.x - off] : 0u;
+      __syncthreads();
+      sh[threadIdx.x] += add;
+      __syncthreads();
+    }
+    const unsigned long long ex = carry + (unsigned long long)(sh[threadIdx.x] - v);
+    if (q < nscenes) sc[q].cell_off = ex > 0xffffffffull ? 0xffffffffu : (uint32_t)ex;
+    __syncthreads();
+    if (threadIdx.x == 1023) carry += sh[1023];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    if (carry > (unsigned long long)cell_cap) {
+      atomicOr(&ctl->err, kErrCellCap);
+      ctl->cells = 0;
+    } else {
+      ctl->cells = (uint32_t)carry;
+    }
+  }
+}
+
+// Cell key + arrival rank per slot (tiles, one block per tile in turn). Lanes with equal
+// keys share one atomic (warp-aggregated); the rank is only a placement ticket — canon
+// makes the final order deterministic.
+__global__ void k_e_keys(const float4* __restrict__ pos, const SceneDev* __restrict__ sc,
+                         const TileDev* __restrict__ tiles, uint32_t ntiles, const EngineCtl* __restrict__ ctl,
+                         uint32_t* __restrict__ counts, uint2* __restrict__ cellrank) {
+  if (ctl->err & kErrCellCap) return;
+  for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const TileDev td = tiles[t];
+    const GridBox g = sc[td.scene].g;
+    const uint32_t off = sc[td.scene].cell_off;
+    for (uint32_t b0 = 0; b0 < td.count; b0 += blockDim.x) {
+      const uint32_t i = b0 + threadIdx.x;
+      const bool valid = i < td.count;
+      uint32_t c = 0xffffffffu;
+      if (valid) {
+        const float4 p = pos[td.first + i];
+        c = off + cell_index(g, p.x, p.y, p.z);
+      }
+      const uint32_t active = __ballot_sync(0xffffffffu, valid);
+      if (valid) {
+        const uint32_t peers = __match_any_sync(active, c);
+        const int lane = threadIdx.x & 31;
+        const int leader = __ffs(peers) - 1;
+        uint32_t base = 0;
+        if (lane == leader) base = atomicAdd(&counts[c], (uint32_t)__popc(peers));
+        base = __shfl_sync(peers, base, leader);
+        cellrank[td.first + i] = make_uint2(c, base + __popc(peers & ((1u << lane) - 1u)));
+      }
+    }
+  }
+}
+
+// Exclusive scan of the global cell counts -> start (phase 1: tile sums).
+__global__ void k_e_scan_partial(const uint32_t* __restrict__ counts, const EngineCtl* __restrict__ ctl,
+                                 uint32_t* __restrict__ partial) {
+  if (ctl->err & kErrCellCap) return;
+  const uint32_t total = ctl->cells;
+  for (uint32_t tile = blockIdx.x; (size_t)tile * kScanTile < total; tile += gridDim.x) {
+    const uint32_t base = tile * kScanTile;
+    uint32_t sum = 0;
+    for (uint32_t i = base + threadIdx.x; i < min(base + kScanTile, total); i += kScanThreads) sum += counts[i];
+    for (int off = 16; off > 0; off >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, off);
+    __shared__ uint32_t ws[kScanThreads / 32];
+    if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = sum;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      uint32_t t = 0;
+      for (int w = 0; w < kScanThreads / 32; ++w) t += ws[w];
+      partial[tile] = t;
+    }
+    __syncthreads();
+  }
+}
+
+// Phase 2: one block scans the tile sums (any count, 1024 at a time with a carry).
+__global__ void k_e_scan_top(uint32_t* __restrict__ partial, const EngineCtl* __restrict__ ctl,
+                             uint32_t* __restrict__ start) {
+  if (ctl->err & kErrCellCap) return;
+  const uint32_t total = ctl->cells;
+  const uint32_t ntiles = (total + kScanTile - 1) / kScanTile;
+  __shared__ uint32_t sh[1024];
+  __shared__ uint32_t carry;
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  for (uint32_t b0 = 0; b0 < ntiles; b0 += 1024) {
+    const uint32_t t = b0 + threadIdx.x;
+    const uint32_t v = t < ntiles ? partial[t] : 0u;
+    sh[threadIdx.x] = v;
+    __syncthreads();
+    for (uint32_t off = 1; off < 1024; off <<= 1) {
+      const uint32_t add = threadIdx.x >= off ? sh[threadIdx.x - off] : 0u;
+      __syncthreads();
+      sh[threadIdx.x] += add;
+      __syncthreads();
+    }
+    if (t < ntiles) partial[t] = carry + sh[threadIdx.x] - v;
+    __syncthreads();
+    if (threadIdx.x == 1023) carry += sh[1023];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) start[total] = carry;
+}
+
+// Phase 3: per-tile exclusive scan + tile offset -> start; zero counts for the next substep.
+__global__ void k_e_scan_final(uint32_t* __restrict__ counts, const EngineCtl* __restrict__ ctl,
+                               const uint32_t* __restrict__ partial, uint32_t* __restrict__ start) {
+  if (ctl->err & kErrCellCap) return;
+  const uint32_t total = ctl->cells;
+  constexpr int kPer = kScanTile / kScanThreads;
+  __shared__ uint32_t ws[kScanThreads / 32];
+  for (uint32_t tile = blockIdx.x; (size_t)tile * kScanTile < total; tile += gridDim.x) {
+    const uint32_t i0 = tile * kScanTile + threadIdx.x * kPer;
+    uint32_t v[kPer], local = 0;
+#pragma unroll
+    for (int q = 0; q < kPer; ++q) {
+      v[q] = (i0 + q) < total ? counts[i0 + q] : 0u;
+      local += v[q];
+    }
+    uint32_t incl = local;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, incl, off);
+      if (lane >= off) incl += y;
+    }
+    if (lane == 31) ws[wid] = incl;
+    __syncthreads();
+    uint32_t woff = 0;
+    for (int w = 0; w < wid; ++w) woff += ws[w];
+    uint32_t run = partial[tile] + woff + incl - local;
+#pragma unroll
+    for (int q = 0; q < kPer; ++q) {
+      if ((i0 + q) < total) {
+        start[i0 + q] = run;
+        counts[i0 + q] = 0u;
+      }
+      run += v[q];
+    }
+    __syncthreads();
+  }
+}
+
+// Place each slot's (reference index, old slot) at start[cell] + rank (tiles).
+__global__ void k_e_place(const uint2* __restrict__ cellrank, const uint32_t* __restrict__ start,
+                          const uint32_t* __restrict__ orig, const TileDev* __restrict__ tiles, uint32_t ntiles,
+                          const EngineCtl* __restrict__ ctl, uint2* __restrict__ items) {
+  if (ctl->err & kErrCellCap) return;
+  for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const TileDev td = tiles[t];
+    for (uint32_t i = threadIdx.x; i < td.count; i += blockDim.x) {
+      const uint32_t s = td.first + i;
+      const uint2 cr = cellrank[s];
+      items[start[cr.x] + cr.y] = make_uint2(orig[s], s);
+    }
+  }
+}
+
+// Per cell: order the placed entries by reference index (grid.rs:56-62) and gather
+// position/velocity into the sorted buffer. A warp scans 32 consecutive cells at a time
+// and handles each non-empty one cooperatively; rank = entries with a smaller index.
+__device__ __forceinline__ void canon_cell(uint32_t b, uint32_t n, int lane, uint32_t* skeys, EngineCtl* ctl,
+                                           const uint2* __restrict__ items, const float4* __restrict__ pos_in,
+                                           const float4* __restrict__ vel_in, float4* __restrict__ pos_out,
+                                           float4* __restrict__ vel_out, uint32_t* __restrict__ orig,
+                                           uint32_t* __restrict__ slot_of) {
+  if (n <= 32) {
+    uint2 it = make_uint2(0xffffffffu, 0u);
+    if ((uint32_t)lane < n) it = items[b + lane];
+    uint32_t rank = 0;
+    for (uint32_t j = 0; j < n; ++j) {
+      const uint32_t kj = __shfl_sync(0xffffffffu, it.x, j);
+      rank += (kj < it.x) ? 1u : 0u;
+    }
+    if ((uint32_t)lane < n) {
+      const uint32_t dst = b + rank;
+      pos_out[dst] = pos_in[it.y];
+      vel_out[dst] = vel_in[it.y];
+      orig[dst] = it.x;
+      slot_of[it.x] = dst;
+    }
+  } else if (n <= (uint32_t)kCanonSmem) {
+    for (uint32_t e = lane; e < n; e += 32) skeys[e] = items[b + e].x;
+    __syncwarp();
+    for (uint32_t e = lane; e < n; e += 32) {
+      const uint2 it = items[b + e];
+      uint32_t rank = 0;
+      for (uint32_t j = 0; j < n; ++j) rank += (skeys[j] < it.x) ? 1u : 0u;
+      const uint32_t dst = b + rank;
+      pos_out[dst] = pos_in[it.y];
+      vel_out[dst] = vel_in[it.y];
+      orig[dst] = it.x;
+      slot_of[it.x] = dst;
+    }
+    __syncwarp();
+  } else {
+    if (lane == 0) atomicOr(&ctl->err, kErrCanonLarge);
+    for (uint32_t e = lane; e < n; e += 32) {
+      const uint2 it = items[b + e];
+      uint32_t rank = 0;
+      for (uint32_t j = 0; j < n; ++j) rank += (items[b + j].x < it.x) ? 1u : 0u;
+      const uint32_t dst = b + rank;
+      pos_out[dst] = pos_in[it.y];
+      vel_out[dst] = vel_in[it.y];
+      orig[dst] = it.x;
+      slot_of[it.x] = dst;
+    }
+  }
+}
+
+__global__ void k_e_canon(const uint2* __restrict__ items, const uint32_t* __restrict__ start, EngineCtl* ctl,
+                          const float4* __restrict__ pos_in, const float4* __restrict__ vel_in,
+                          float4* __restrict__ pos_out, float4* __restrict__ vel_out, uint32_t* __restrict__ orig,
+                          uint32_t* __restrict__ slot_of) {
+  __shared__ uint32_t skeys[8][kCanonSmem];
+  if (ctl->err & kErrCellCap) return;
+  const uint32_t total = ctl->cells;
+  const int lane = threadIdx.x & 31;
+  const int wib = threadIdx.x >> 5;
+  const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t base = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32u; base < total; base += warps * 32u) {
+    const uint32_t c = base + lane;
+    uint32_t b = 0, n = 0;
+    if (c < total) {
+      b = start[c];
+      n = start[c + 1] - b;
+    }
+    uint32_t mask = __ballot_sync(0xffffffffu, n > 0);
+    while (mask) {
+      const int l = __ffs(mask) - 1;
+      mask &= mask - 1;
+      const uint32_t cb = __shfl_sync(0xffffffffu, b, l);
+      const uint32_t cn = __shfl_sync(0xffffffffu, n, l);
+      canon_cell(cb, cn, lane, skeys[wib], ctl, items, pos_in, vel_in, pos_out, vel_out, orig, slot_of);
+    }
+  }
+}
+
+// Walk the 27 cells around position p (cell (cx, cy, cz)) in the reference order
+// (dz outer, dy, dx inner; crates/vxl-phys-fluid/src/grid.rs:123-153), calling f(j) for
+// every slot j in them — except cells whose nominal box lies farther than h from p.
+// Such a cell holds no particle with r2 <= h2, so skipping it changes neither the set nor
+// the order of accepted neighbours. The test is conservative: per-axis gaps to the
+// neighbouring cell faces are clamped at 0 and compared with (h + bin/1024)^2, a margin
+// far above the f32 rounding of cell faces and bin assignment. `start` is the scene's
+// slice of the global cell table.
+template <class F>
+__device__ __forceinline__ void walk27(const GridBox& g, const uint32_t* __restrict__ start, float px, float py,
+                                       float pz, uint32_t cx, uint32_t cy, uint32_t cz, float h, F&& f) {
+  const float lx = g.minx + (float)cx * g.bin, ly = g.miny + (float)cy * g.bin, lz = g.minz + (float)cz * g.bin;
+  const float gxl = fmaxf(px - lx, 0.0f), gxr = fmaxf(lx + g.bin - px, 0.0f);
+  const float gyl = fmaxf(py - ly, 0.0f), gyr = fmaxf(ly + g.bin - py, 0.0f);
+  const float gzl = fmaxf(pz - lz, 0.0f), gzr = fmaxf(lz + g.bin - pz, 0.0f);
+  const float reach = h + g.bin * (1.0f / 1024.0f);
+  const float reach2 = reach * reach;
+  for (int dz = -1; dz <= 1; ++dz) {
+    const int z = (int)cz + dz;
+    if (z < 0 || z >= (int)g.nz) continue;
+    const float gz = dz < 0 ? gzl : (dz > 0 ? gzr : 0.0f);
+    const float dz2 = gz * gz;
+    for (int dy = -1; dy <= 1; ++dy) {
+      const int y = (int)cy + dy;
+      if (y < 0 || y >= (int)g.ny) continue;
+      const float gy = dy < 0 ? gyl : (dy > 0 ? gyr : 0.0f);
+      const float dyz2 = dz2 + gy * gy;
+      for (int dx = -1; dx <= 1; ++dx) {
+        const int x = (int)cx + dx;
+        if (x < 0 || x >= (int)g.nx) continue;
+        const float gx = dx < 0 ? gxl : (dx > 0 ? gxr : 0.0f);
+        if (dyz2 + gx * gx > reach2) continue;
+        const uint32_t idx = ((uint32_t)x * g.ny + (uint32_t)y) * g.nz + (uint32_t)z;
+        const uint32_t j1 = start[idx + 1];
+        for (uint32_t j = start[idx]; j < j1; ++j) f(j);
+      }
+    }
+  }
+}
+
+// Density (poly6 with self term) + Tait EOS, persistent over tiles, one thread per slot.
+// Fluid: rho = mass * (w0 + sum_fluid W) + sum_boundary pmass_j W
+// (crates/vxl-phys-fluid/src/fluid_density.rs:24-51); boundary: rho = pmass_i w0 +
+// sum_fluid pmass_j W (fluid_density.rs:59-69). Writes (rho, p / rho^2) for the force
+// pass (the reference recomputes press/(rho*rho) per pair: same value). Also records, in
+// walk order, the slots of the neighbours that contributed (all for fluid, fluid ones for
+// boundary particles): nbr[k * stride + s], k < cap, with the full count in nbr_n[s]
+// (a count above cap sends the consumers back to walking the cells).
+template <int kBlock>
+__global__ void __launch_bounds__(kBlock, 1024 / kBlock) k_e_density(
+    const float4* __restrict__ pos, const uint32_t* __restrict__ start, const SceneDev* __restrict__ sc,
+    const TileDev* __restrict__ tiles, uint32_t ntiles, EngineCtl* ctl, float2* __restrict__ rc,
+    float* __restrict__ press_out, uint32_t* __restrict__ nbr, uint32_t* __restrict__ nbr_n, uint32_t cap,
+    uint32_t stride) {
+  if (ctl->err & kErrCellCap) return;
+  for (;;) {
+    const uint32_t t = next_tile(&ctl->work[kWorkDensity]);
+    if (t >= ntiles) break;
+    const TileDev td = tiles[t];
+    const SceneDev& S = sc[td.scene];
+    const GridBox g = S.g;
+    const SphConst& k = S.k;
+    const uint32_t* cst = start + S.cell_off;
+    const float h = k.h, h2 = k.h2, k6 = k.k6, w0 = k.w0, mass = k.mass;
+    for (uint32_t i = threadIdx.x; i < td.count; i += kBlock) {
+      const uint32_t s = td.first + i;
+      const float4 pi = pos[s];
+      const bool fluid_i = pi.w > 0.0f;
+      uint32_t cx, cy, cz;
+      bin_of(g, pi.x, pi.y, pi.z, cx, cy, cz);
+      float sum = fluid_i ? w0 : 0.0f;
+      float sum_b = 0.0f;
+      uint32_t cnt = 0;
+      walk27(g, cst, pi.x, pi.y, pi.z, cx, cy, cz, h, [&](uint32_t j) {
+        if (j == s) return;
+        const float4 pj = pos[j];
+        const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
+        const float r2 = dx * dx + dy * dy + dz * dz;
+        if (r2 <= h2) {
+          const float tt = h2 - r2;
+          const float w = k6 * tt * tt * tt;
+          bool rec = true;
+          if (fluid_i) {
+            if (pj.w > 0.0f) sum += w;
+            else sum_b += (-pj.w) * w;
+          } else if (pj.w > 0.0f) {
+            sum += pj.w * w;
+          } else {
+            rec = false;
+          }
+          if (rec) {
+            if (cnt < cap) nbr[(size_t)cnt * stride + s] = j;
+            ++cnt;
+          }
+        }
+      });
+      nbr_n[s] = cnt;
+      const float rho = fluid_i ? (mass * sum + sum_b) : ((-pi.w) * w0 + sum);
+      const float p = tait(k, rho);
+      rc[s] = make_float2(rho, p / (rho * rho));
+      if (press_out) press_out[s] = p;
+    }
+  }
+}
+
+// Force (gravity + spiky pressure + Monaghan viscosity + XSPH, fluid_force.rs:165-214)
+// fused with integration (semi-implicit Euler + CFL clamp, fluid_step.rs:112-123) for
+// fluid slots; boundary slots are copied unchanged (kinematic within the tick).
+// Neighbours come from the density pass's list (same walk order, so the same sums); a
+// particle whose list overflowed walks the 27 cells again. Reads the sorted buffer and
+// writes the integrated state to (pos_out, vel_out) in the same slot order; accumulates
+// each tile's fluid AABB into its scene's accumulator for the next grid box.
+template <int kBlock>
+__global__ void __launch_bounds__(kBlock, 768 / kBlock) k_e_force(
+    const float4* __restrict__ pos, const float4* __restrict__ vel, const float2* __restrict__ rc,
+    const uint32_t* __restrict__ start, const uint32_t* __restrict__ nbr, const uint32_t* __restrict__ nbr_n,
+    uint32_t cap, uint32_t stride, SceneDev* __restrict__ sc, const TileDev* __restrict__ tiles, uint32_t ntiles,
+    EngineCtl* ctl, float4* __restrict__ pos_out, float4* __restrict__ vel_out, float4* __restrict__ acc_out,
+    float4* __restrict__ xsph_out) {
+  if (ctl->err & kErrCellCap) return;
+  for (;;) {
+    const uint32_t t = next_tile(&ctl->work[kWorkForce]);
+    if (t >= ntiles) break;
+    const TileDev td = tiles[t];
+    SceneDev& S = sc[td.scene];
+    const SphConst& k = S.k;
+    const float dt = S.dt, vmax = S.vmax, vmax2 = S.vmax2;
+    for (uint32_t b0 = 0; b0 < td.count; b0 += kBlock) {
+      const uint32_t i = b0 + threadIdx.x;
+      const bool valid = i < td.count;
+      float nx = 0, ny = 0, nz = 0;
+      bool fluid_i = false;
+      if (valid) {
+        const uint32_t s = td.first + i;
+        const float4 pi = pos[s];
+        const float4 vi = vel[s];
+        fluid_i = pi.w > 0.0f;
+        if (!fluid_i) {
+          pos_out[s] = pi;
+          vel_out[s] = vi;
+        } else {
+          const float2 rci = rc[s];
+          const float rho_i = rci.x, ci2 = rci.y;
+          const float h = k.h, h2 = k.h2, ks = k.ks, k6 = k.k6, alpha_c = k.alpha_c, h001 = k.h001;
+          float ax = k.gx, ay = k.gy, az = k.gz;
+          float xx = 0.0f, xy = 0.0f, xz = 0.0f;
+          auto pair = [&](uint32_t j, const float4& pj, float dx, float dy, float dz, float r2) {
+            const float2 rcj = rc[j];
+            const float4 vj = vel[j];
+            const float rho_j = rcj.x, cj2 = rcj.y;
+            const float mj = fabsf(pj.w);
+            const float r = sqrtf(r2);
+            const float tt = h - r;
+            const float coef = mj * (ks * tt * tt) * (ci2 + cj2);
+            const float denom = fmaxf(r, 1e-9f);
+            const float q = coef / denom;
+            ax = ax + dx * q;
+            ay = ay + dy * q;
+            az = az + dz * q;
+            const float vx = vi.x - vj.x, vy = vi.y - vj.y, vz = vi.z - vj.z;
+            const float vdn = -(vx * dx + vy * dy + vz * dz);
+            if (vdn > 0.0f) {
+              const float mu = vdn * h / (r2 + h001);
+              const float c = mj * (alpha_c * mu / (0.5f * (rho_i + rho_j))) * (ks * tt * tt);
+              const float q2 = c / denom;
+              ax = ax + dx * q2;
+              ay = ay + dy * q2;
+              az = az + dz * q2;
+            }
+            const float t2 = h2 - r2;
+            const float w = k6 * t2 * t2 * t2;
+            const float f = mj * 2.0f / (rho_i + rho_j) * w;
+            xx = xx + (vj.x - vi.x) * f;
+            xy = xy + (vj.y - vi.y) * f;
+            xz = xz + (vj.z - vi.z) * f;
+          };
+          const uint32_t cnt = nbr_n[s];
+          if (cnt <= cap) {
+            for (uint32_t q = 0; q < cnt; ++q) {
+              const uint32_t j = nbr[(size_t)q * stride + s];
+              const float4 pj = pos[j];
+              const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
+              pair(j, pj, dx, dy, dz, dx * dx + dy * dy + dz * dz);
+            }
+          } else {
+            const GridBox g = S.g;
+            uint32_t cx, cy, cz;
+            bin_of(g, pi.x, pi.y, pi.z, cx, cy, cz);
+            walk27(g, start + S.cell_off, pi.x, pi.y, pi.z, cx, cy, cz, h, [&](uint32_t j) {
+              if (j == s) return;
+              const float4 pj = pos[j];
+              const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
+              const float r2 = dx * dx + dy * dy + dz * dz;
+              if (r2 <= h2) pair(j, pj, dx, dy, dz, r2);
+            });
+          }
+          if (acc_out) {
+            acc_out[s] = make_float4(ax, ay, az, 0.0f);
+            xsph_out[s] = make_float4(xx, xy, xz, 0.0f);
+          }
+          const float eps = k.eps;
+          float ux = vi.x + ax * dt + xx * eps;
+          float uy = vi.y + ay * dt + xy * eps;
+          float uz = vi.z + az * dt + xz * eps;
+          const float s2 = ux * ux + uy * uy + uz * uz;
+          if (s2 > vmax2) {
+            const float scl = vmax / sqrtf(s2);
+            ux = ux * scl;
+            uy = uy * scl;
+            uz = uz * scl;
+          }
+          nx = pi.x + ux * dt;
+          ny = pi.y + uy * dt;
+          nz = pi.z + uz * dt;
+          pos_out[s] = make_float4(nx, ny, nz, pi.w);
+          vel_out[s] = make_float4(ux, uy, uz, 0.0f);
+        }
+      }
+      block_bbox_accumulate(S.fbox, nx, ny, nz, valid && fluid_i);
+    }
+  }
+}
+
+// Pair term of the boundary reaction for fluid i on boundary j, from i's side of the
+// reference loop (crates/vxl-phys-fluid/src/fluid_force.rs:182-207): returns
+// q = m_i (coef + cv) / denom, with d = p_i - p_j; the caller applies bforce -= d * q.
+__device__ __forceinline__ float bforce_pair(const SphConst& k, float r2, float dx, float dy, float dz,
+                                             float rho_i, float ci2, float mi, float4 vi, float rho_j, float cj2,
+                                             float mj, float4 vj) {
+  const float r = sqrtf(r2);
+  const float t = k.h - r;
+  const float coef = mj * (k.ks * t * t) * (ci2 + cj2);
+  const float denom = fmaxf(r, 1e-9f);
+  float cv = 0.0f;
+  const float vx = vi.x - vj.x, vy = vi.y - vj.y, vz = vi.z - vj.z;
+  const float vdn = -(vx * dx + vy * dy + vz * dz);
+  if (vdn > 0.0f) {
+    const float mu = vdn * k.h / (r2 + k.h001);
+    cv = mj * (k.alpha_c * mu / (0.5f * (rho_i + rho_j))) * (k.ks * t * t);
+  }
+  return mi * (coef + cv) / denom;
+}
+
+// Reaction on each boundary particle j: the reference accumulates bforce[j] -= F_ij over
+// fluid i in ascending reference index (the outer loop of force_pass_serial). Here the
+// boundary particle takes its fluid neighbours (recorded by the density pass, or found by
+// walking the 27 cells when that list overflowed), orders them by reference index and sums
+// in that order, so the result is the same sum. Output by global reference index.
+__global__ void __launch_bounds__(128) k_e_bforce(
+    const float4* __restrict__ pos, const float4* __restrict__ vel, const float2* __restrict__ rc,
+    const uint32_t* __restrict__ start, const uint32_t* __restrict__ orig, const uint32_t* __restrict__ nbr,
+    const uint32_t* __restrict__ nbr_n, uint32_t cap, uint32_t stride, const SceneDev* __restrict__ sc,
+    const TileDev* __restrict__ tiles, uint32_t ntiles, EngineCtl* ctl, float4* __restrict__ bforce) {
+  if (ctl->err & kErrCellCap) return;
+  for (;;) {
+    const uint32_t t = next_tile(&ctl->work[kWorkBforce]);
+    if (t >= ntiles) break;
+    const TileDev td = tiles[t];
+    const SceneDev& S = sc[td.scene];
+    const SphConst& k = S.k;
+    const GridBox g = S.g;
+    const uint32_t* cst = start + S.cell_off;
+    const float h2 = k.h2;
+    for (uint32_t i = threadIdx.x; i < td.count; i += blockDim.x) {
+      const uint32_t s = td.first + i;
+      const float4 pj = pos[s];
+      if (pj.w > 0.0f) continue;  // fluid slot
+      const float4 vj = vel[s];
+      const float2 rcj = rc[s];
+      const float mj = -pj.w;
+      uint32_t cx, cy, cz;
+      bin_of(g, pj.x, pj.y, pj.z, cx, cy, cz);
+      uint32_t key[kBGatherCap] = {};
+      uint32_t slot[kBGatherCap];
+      int n = 0;
+      bool overflow = false;
+      auto insert = [&](uint32_t ii) {
+        if (n < kBGatherCap) {
+          const uint32_t o = orig[ii];
+          int q = n++;
+          while (q > 0 && key[q - 1] > o) {
+            key[q] = key[q - 1];
+            slot[q] = slot[q - 1];
+            --q;
+          }
+          key[q] = o;
+          slot[q] = ii;
+        } else {
+          overflow = true;
+        }
+      };
+      const uint32_t cnt = nbr_n[s];
+      if (cnt <= cap) {
+        for (uint32_t q = 0; q < cnt; ++q) insert(nbr[(size_t)q * stride + s]);
+      } else {
+        walk27(g, cst, pj.x, pj.y, pj.z, cx, cy, cz, k.h, [&](uint32_t ii) {
+          const float4 p = pos[ii];
+          if (!(p.w > 0.0f)) return;
+          const float dx = p.x - pj.x, dy = p.y - pj.y, dz = p.z - pj.z;
+          if (!(dx * dx + dy * dy + dz * dz <= h2)) return;
+          insert(ii);
+        });
+      }
+      float bx = 0.0f, by = 0.0f, bz = 0.0f;
+      auto apply = [&](uint32_t ii) {
+        const float4 p = pos[ii];
+        const float dx = p.x - pj.x, dy = p.y - pj.y, dz = p.z - pj.z;
+        const float r2 = dx * dx + dy * dy + dz * dz;
+        const float2 rci = rc[ii];
+        const float q = bforce_pair(k, r2, dx, dy, dz, rci.x, rci.y, p.w, vel[ii], rcj.x, rcj.y, mj, vj);
+        bx = bx - dx * q;
+        by = by - dy * q;
+        bz = bz - dz * q;
+      };
+      if (!overflow) {
+        for (int q = 0; q < n; ++q) apply(slot[q]);
+      } else {
+        // Slow path: fluid neighbours in ascending reference index by repeated minimum
+        // search (O(neighbours x candidates)); counted in ctl->slow_gathers.
+        atomicAdd(&ctl->slow_gathers, 1u);
+        uint32_t last = 0;
+        bool first = true;
+        for (;;) {
+          uint32_t best = 0xffffffffu, best_slot = 0;
+          walk27(g, cst, pj.x, pj.y, pj.z, cx, cy, cz, k.h, [&](uint32_t ii) {
+            const float4 p = pos[ii];
+            if (!(p.w > 0.0f)) return;
+            const uint32_t o = orig[ii];
+            if (!first && o <= last) return;
+            if (o >= best) return;
+            const float dx = p.x - pj.x, dy = p.y - pj.y, dz = p.z - pj.z;
+            if (!(dx * dx + dy * dy + dz * dz <= h2)) return;
+            best = o;
+            best_slot = ii;
+          });
+          if (best == 0xffffffffu) break;
+          apply(best_slot);
+          last = best;
+          first = false;
+        }
+      }
+      bforce[orig[s]] = make_float4(bx, by, bz, 0.0f);
+    }
+  }
+}
+
+// Per-span force and torque about the body origin (fluid_boundary.rs:10-28), added to
+// the tick accumulator. Fixed-shape two-level reduction, deterministic run to run:
+// level 1, one block per chunk of <= kReactChunk consecutive particles of a span (thread
+// t sums t, t + blockDim, ... in order, then a fixed tree); level 2, one thread per span
+// adds its chunk partials in chunk order. Span ranges are global reference indices.
+
+__global__ void __launch_bounds__(kReactThreads) k_react_chunks(const float4* __restrict__ bforce,
+                                                                const float4* __restrict__ bpos,
+                                                                const SpanDev* __restrict__ spans,
+                                                                const SpanChunk* __restrict__ chunks,
+                                                                const EngineCtl* __restrict__ ctl,
+                                                                float* __restrict__ partial) {
+  if (ctl->err & kErrCellCap) return;
+  const SpanChunk ch = chunks[blockIdx.x];
+  const SpanDev sp = spans[ch.span];
+  float f[6] = {0, 0, 0, 0, 0, 0};
+  for (uint32_t kk = ch.begin + threadIdx.x; kk < ch.end; kk += kReactThreads) {
+    const float4 fk = bforce[kk];
+    const float4 p = bpos[kk];
+    const float rx = p.x - sp.ox, ry = p.y - sp.oy, rz = p.z - sp.oz;
+    f[0] = f[0] + fk.x;
+    f[1] = f[1] + fk.y;
+    f[2] = f[2] + fk.z;
+    f[3] = f[3] + (ry * fk.z - rz * fk.y);
+    f[4] = f[4] + (rz * fk.x - rx * fk.z);
+    f[5] = f[5] + (rx * fk.y - ry * fk.x);
+  }
+  __shared__ float sh[6][kReactThreads];
+  for (int a = 0; a < 6; ++a) sh[a][threadIdx.x] = f[a];
+  __syncthreads();
+  for (uint32_t w = kReactThreads / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w)
+      for (int a = 0; a < 6; ++a) sh[a][threadIdx.x] = sh[a][threadIdx.x] + sh[a][threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x < 6) partial[6 * blockIdx.x + threadIdx.x] = sh[threadIdx.x][0];
+}
+
+// chunk_first[q] .. chunk_first[q + 1]: the chunks of span q (in order).
+__global__ void k_react_spans(const float* __restrict__ partial, const uint32_t* __restrict__ chunk_first,
+                              const EngineCtl* __restrict__ ctl, float* __restrict__ breact, uint32_t nspans) {
+  if (ctl->err & kErrCellCap) return;
+  const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= nspans) return;
+  float f[6] = {0, 0, 0, 0, 0, 0};
+  for (uint32_t c = chunk_first[q]; c < chunk_first[q + 1]; ++c)
+    for (int a = 0; a < 6; ++a) f[a] = f[a] + partial[6 * c + a];
+  for (int a = 0; a < 6; ++a) breact[6 * q + a] = breact[6 * q + a] + f[a];
+}
+
+// Tick average (fluid_step.rs:84-88): e *= 1 / substeps.
+__global__ void k_scale(float* __restrict__ breact, uint32_t n, float inv) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) breact[i] = breact[i] * inv;
+}
+
+// ---------------------------------------------------------------- export kernels
+
+// One scene's state in its reference order (scene-local index).
+__global__ void k_e_read_scene(const float4* __restrict__ pos, const float4* __restrict__ vel,
+                               const uint32_t* __restrict__ orig, float* __restrict__ pout, float* __restrict__ vout,
+                               uint32_t base, uint32_t n) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint32_t s = base + i;
+  const uint32_t o = orig[s] - base;
+  if (pout) {
+    const float4 p = pos[s];
+    pout[3 * o] = p.x;
+    pout[3 * o + 1] = p.y;
+    pout[3 * o + 2] = p.z;
+  }
+  if (vout) {
+    const float4 v = vel[s];
+    vout[3 * o] = v.x;
+    vout[3 * o + 1] = v.y;
+    vout[3 * o + 2] = v.z;
+  }
+}
+
+__global__ void k_e_read_fields(const float2* __restrict__ rc, const float* __restrict__ press,
+                                const float4* __restrict__ acc, const float4* __restrict__ xsph,
+                                const uint32_t* __restrict__ orig, float* __restrict__ dout, float* __restrict__ pout,
+                                float* __restrict__ aout, float* __restrict__ xout, uint32_t base, uint32_t n) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint32_t s = base + i;
+  const uint32_t o = orig[s] - base;
+  if (dout) dout[o] = rc[s].x;
+  if (pout) pout[o] = press[s];
+  if (aout) {
+    const float4 a = acc[s];
+    aout[3 * o] = a.x;
+    aout[3 * o + 1] = a.y;
+    aout[3 * o + 2] = a.z;
+  }
+  if (xout) {
+    const float4 x = xsph[s];
+    xout[3 * o] = x.x;
+    xout[3 * o + 1] = x.y;
+    xout[3 * o + 2] = x.z;
+  }
+}
+
+// Per-particle cell (scene-local cell index) of one scene, from its slice of the table.
+__global__ void k_e_export_bins(const uint32_t* __restrict__ start, const uint32_t* __restrict__ orig,
+                                const SceneDev* __restrict__ sc, uint32_t scene, uint32_t* __restrict__ bins) {
+  const SceneDev& S = sc[scene];
+  const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= S.cells) return;
+  const uint32_t gc = S.cell_off + c;
+  for (uint32_t q = start[gc]; q < start[gc + 1]; ++q) bins[orig[q] - S.base] = c;
+}
+
+// One scene's slice of the cell table, rebased to the scene's first slot.
+__global__ void k_e_export_start(const uint32_t* __restrict__ start, const SceneDev* __restrict__ sc, uint32_t scene,
+                                 uint32_t* __restrict__ out) {
+  const SceneDev& S = sc[scene];
+  const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c > S.cells) return;
+  out[c] = start[S.cell_off + c] - S.base;
+}
+
+__global__ void k_e_export_items(const uint32_t* __restrict__ orig, uint32_t base, uint32_t n,
+                                 uint32_t* __restrict__ out) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = orig[base + i] - base;
+}
+
+}  // namespace
+}  // namespace vxl

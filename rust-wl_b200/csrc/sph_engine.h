@@ -1,0 +1,190 @@
+// Host side of the multi-scene WCSPH engine (sph_engine.cuh holds the kernels).
+//
+// An Engine owns one pool of particle slots on one GPU and any number of resident
+// scenes packed into it without gaps. It steps all active scenes together, one launch
+// per kernel per substep, and captures whole ticks as CUDA graphs. The plain C ABI handle
+// is an Engine holding one scene; the batched and served forms hold many.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "vxl_sph.h"
+
+namespace vxl {
+
+struct SceneDev;
+struct TileDev;
+struct EngineCtl;
+struct SpanDev;
+struct SpanChunk;
+
+// Launch shape of the particle passes (chosen by the autotuner for batches).
+struct Tuning {
+  uint32_t block = 256;   // threads per block of the density/force passes (128 or 256)
+  uint32_t tile = 1024;   // slots per work item of the persistent passes
+  uint32_t waves = 1;     // persistent blocks per SM, as a multiple of the occupancy limit / 2
+};
+
+struct SceneInfo {
+  uint64_t id = 0;
+  uint32_t base = 0, nf = 0, nb = 0;
+  uint32_t substeps = 1;
+  float particle_mass = 0.f;
+  vxl_sph_params params{};
+};
+
+class Engine {
+ public:
+  // slot_cap particles and cell_cap cells of capacity; nbr_cap neighbour-list entries per
+  // particle. Allocates everything up front.
+  static vxl_status create(int device, uint64_t slot_cap, uint64_t cell_cap, uint32_t scene_cap,
+                           Engine** out);
+  ~Engine();
+
+  int device() const { return device_; }
+  cudaStream_t stream() const { return stream_; }
+  void set_stream(cudaStream_t s);
+  uint64_t used_slots() const { return used_; }
+  uint64_t slot_cap() const { return slot_cap_; }
+  uint64_t cell_cap() const { return cell_cap_; }
+  uint64_t device_bytes() const { return device_bytes_; }
+  uint64_t launches_last_tick() const { return launches_last_tick_; }
+  const std::vector<SceneInfo>& scenes() const { return scenes_; }
+  static uint64_t bytes_per_slot(uint32_t nbr_cap);
+  static uint64_t bytes_per_cell();
+
+  // Append a scene at the end of the pool (reference order input: fluid prefix then
+  // boundary suffix, xyz triples). Validates like vxl_sph_create.
+  vxl_status add_scene(const vxl_sph_params& p, uint64_t nf, uint64_t nb, const float* pos, const float* vel,
+                       const float* pmass, uint64_t id, uint32_t* out_index);
+  // Drop scenes (by index) and close the gaps by moving the later scenes down.
+  vxl_status remove_scenes(const std::vector<uint32_t>& indices);
+
+  vxl_status upload_boundary(uint32_t scene, const float* pos, const float* vel, uint64_t nb);
+  vxl_status write_state(uint32_t scene, const float* pos, const float* vel);
+  vxl_status read_state(uint32_t scene, float* pos, float* vel);
+  vxl_status read_fields(uint32_t scene, float* dens, float* press, float* acc, float* xsph, float* bforce);
+  vxl_status export_grid(uint32_t scene, uint32_t* items, uint32_t* start, uint64_t start_cap, uint32_t* bins,
+                         vxl_sph_grid_info* info);
+  vxl_status bounds(uint32_t scene, float lo[3], float hi[3]);
+
+  // Spans in scene-local particle indices, per scene (reactions of the plain/batched tick).
+  vxl_status set_spans(uint32_t scene, const vxl_sph_span* spans, uint32_t n);
+  // One tick of every scene (all scenes must share `substeps`), tick-averaged reactions.
+  vxl_status step_tick_async(float dt_tick);
+  vxl_status sync(std::vector<vxl_sph_reaction>* reactions);
+  // One substep of every scene with per-scene dt (the served form), or of one scene
+  // count (the plain vxl_sph_substep).
+  vxl_status substep(const std::vector<float>& dt_per_scene);
+
+  void set_record(bool on) { record_ = on; }
+  bool record() const { return record_; }
+  void set_use_graph(bool on) { use_graph_ = on; }
+  void set_tuning(const Tuning& t);
+  const Tuning& tuning() const { return tuning_; }
+  vxl_status set_profile(bool on);
+  vxl_status profile_read(uint32_t k, const char** name, double* ms, uint64_t* launches);
+  bool ran_substep() const { return ran_substep_; }
+  // Time every candidate launch shape over `trials` substeps on the resident scenes
+  // (from a snapshot that is restored afterwards) and keep the fastest.
+  vxl_status autotune(float dt_tick, uint32_t trials, Tuning* best, float* best_ms);
+  uint32_t cells_last() ;
+  uint32_t slow_gathers();
+
+ private:
+  Engine() = default;
+  vxl_status alloc_all();
+  void free_all();
+  vxl_status recompute_scene_boxes(uint32_t scene);
+  vxl_status rebuild_tiles();
+  vxl_status stage_spans();
+  vxl_status push_scene_records(const std::vector<float>& dt);
+  void enqueue_substep(bool with_reactions);
+  void enqueue_tick(float dt_tick);
+  vxl_status finish();
+  void prof_collect();
+  int prof_begin(int kid);
+  void prof_end(int i);
+  void record_event(cudaEvent_t e);
+
+  template <class T>
+  vxl_status dalloc(T** p, size_t count);
+
+  int device_ = 0;
+  cudaStream_t stream_ = nullptr, own_stream_ = nullptr;
+  uint64_t slot_cap_ = 0, cell_cap_ = 0, used_ = 0;
+  uint32_t scene_cap_ = 0, nbr_cap_ = 64;
+  uint64_t device_bytes_ = 0;
+  std::vector<SceneInfo> scenes_;
+
+  // pool (slot_cap_)
+  void* pos_[2] = {nullptr, nullptr};
+  void* vel_[2] = {nullptr, nullptr};
+  uint32_t* orig_ = nullptr;
+  uint32_t* slot_of_ = nullptr;
+  void* cellrank_ = nullptr;
+  void* items_ = nullptr;
+  void* rc_ = nullptr;
+  float* press_ = nullptr;
+  void* acc_ = nullptr;
+  void* xsph_ = nullptr;
+  void* bforce_ = nullptr;
+  void* bpos_ = nullptr;
+  uint32_t* nbr_ = nullptr;
+  uint32_t* nbr_n_ = nullptr;
+  float* stage_ = nullptr;  // 8 floats per slot: staging for host transfers
+  // cells (cell_cap_ + 1)
+  uint32_t* counts_ = nullptr;
+  uint32_t* start_ = nullptr;
+  uint32_t* partial_ = nullptr;
+  // scenes / tiles / control
+  SceneDev* sc_d_ = nullptr;
+  SceneDev* sc_h_ = nullptr;  // pinned mirror (pushed when dt or membership changes)
+  TileDev* tiles_d_ = nullptr;
+  std::vector<TileDev>* tiles_h_ = nullptr;
+  uint32_t ntiles_ = 0, tiles_cap_ = 0;
+  EngineCtl* ctl_d_ = nullptr;
+  EngineCtl* ctl_h_ = nullptr;  // pinned
+  // reactions
+  std::vector<std::vector<vxl_sph_span>> spans_local_;
+  SpanDev* spans_d_ = nullptr;
+  SpanDev* spans_h_ = nullptr;  // pinned
+  SpanChunk* chunks_d_ = nullptr;
+  SpanChunk* chunks_h_ = nullptr;  // pinned
+  uint32_t* chunk_first_d_ = nullptr;
+  uint32_t* chunk_first_h_ = nullptr;  // pinned
+  float* react_partial_ = nullptr;
+  float* breact_d_ = nullptr;
+  float* breact_h_ = nullptr;  // pinned
+  uint32_t nspans_ = 0, nchunks_ = 0, spans_cap_ = 0, chunks_cap_ = 0;
+  bool spans_dirty_ = true;
+  std::vector<uint32_t> span_scene_;  // scene of each global span (for the results)
+
+  bool record_ = false;
+  bool ran_substep_ = false;
+  bool use_graph_ = true;
+  Tuning tuning_;
+  int grid_density_ = 0, grid_force_ = 0, grid_bforce_ = 0;
+  // graph of one tick
+  cudaGraphExec_t graph_ = nullptr;
+  uint32_t graph_epoch_ = 0;
+  uint32_t graph_key_ = 0;
+  uint32_t membership_epoch_ = 0;
+  uint64_t launches_counter_ = 0, launches_last_tick_ = 0;
+  // profiling
+  bool prof_ = false, capturing_ = false, prof_pending_ = false;
+  std::vector<cudaEvent_t> prof_ev_;
+  std::vector<int> prof_kid_;
+  size_t prof_used_ = 0;
+  double prof_ms_[24] = {};
+  uint64_t prof_n_[24] = {};
+};
+
+// Thread-local error message shared by all entry points (vxl_sph_last_error).
+vxl_status set_error(vxl_status s, const std::string& msg);
+
+}  // namespace vxl

@@ -26,5 +26,6 @@ inline float vxl_o2f_host(uint32_t o) {
   return f;
 }
 
-// Sets the thread-local message returned by vxl_sph_last_error() (defined in sph_capi.cu).
+// The thread-local message returned by vxl_sph_last_error() (defined in sph_engine.cu).
 void vxl_set_last_error(const char* msg);
+const char* vxl_get_last_error();

@@ -102,6 +102,22 @@ class Stats(C.Structure):
     ]
 
 
+class Tuning(C.Structure):
+    _fields_ = [("hdr", BlockHeader), ("block", C.c_uint32), ("tile", C.c_uint32), ("waves", C.c_uint32),
+                ("ms_per_substep", C.c_float)]
+
+
+class RequestStatus(C.Structure):
+    _fields_ = [("hdr", BlockHeader), ("state", C.c_uint32), ("ticks_done", C.c_uint32),
+                ("ticks_total", C.c_uint32), ("pad", C.c_uint32), ("submit_s", C.c_double), ("admit_s", C.c_double),
+                ("done_s", C.c_double), ("tick_p50_ms", C.c_double), ("tick_p99_ms", C.c_double)]
+
+
+class ServeReport(C.Structure):
+    _fields_ = [("hdr", BlockHeader), ("active", C.c_uint32), ("queued", C.c_uint32), ("admitted", C.c_uint32),
+                ("retired", C.c_uint32), ("particles", C.c_uint64), ("device_bytes_in_use", C.c_uint64)]
+
+
 def header(struct_type) -> BlockHeader:
     return BlockHeader(C.sizeof(struct_type), ABI_VERSION)
 
@@ -138,6 +154,24 @@ SIGNATURES = {
                                        C.POINTER(C.c_uint64)]),
     "vxl_sph_build_grid_static": (C.c_int, [C.c_void_p, C.c_uint32, C.c_float, C.c_uint32, C.c_void_p, C.c_void_p,
                                             C.c_uint64, C.POINTER(GridInfo), C.c_void_p]),
+    "vxl_sph_create_batch": (C.c_int, [C.POINTER(Desc), C.c_uint32, C.c_int32, C.c_uint64, C.POINTER(_H)]),
+    "vxl_sph_scene_count": (C.c_uint32, [_H]),
+    "vxl_sph_read_state_scene": (C.c_int, [_H, C.c_uint32, _FP, _FP]),
+    "vxl_sph_write_state_scene": (C.c_int, [_H, C.c_uint32, _FP, _FP]),
+    "vxl_sph_upload_boundary_scene": (C.c_int, [_H, C.c_uint32, _FP, _FP, C.c_uint64]),
+    "vxl_sph_set_spans_scene": (C.c_int, [_H, C.c_uint32, C.POINTER(Span), C.c_uint32]),
+    "vxl_sph_export_grid_scene": (C.c_int, [_H, C.c_uint32, _U32P, _U32P, C.c_uint64, _U32P, C.POINTER(GridInfo)]),
+    "vxl_sph_read_fields_scene": (C.c_int, [_H, C.c_uint32, _FP, _FP, _FP, _FP, _FP]),
+    "vxl_sph_reactions_all": (C.c_int, [_H, C.POINTER(Reaction), C.c_uint32, C.POINTER(C.c_uint32)]),
+    "vxl_sph_set_tuning": (C.c_int, [_H, C.POINTER(Tuning)]),
+    "vxl_sph_get_tuning": (C.c_int, [_H, C.POINTER(Tuning)]),
+    "vxl_sph_autotune": (C.c_int, [_H, C.c_float, C.c_uint32, C.POINTER(Tuning)]),
+    "vxl_sph_serve_create": (C.c_int, [C.c_int32, C.c_uint64, C.c_uint32, C.POINTER(C.c_void_p)]),
+    "vxl_sph_serve_destroy": (C.c_int, [C.c_void_p]),
+    "vxl_sph_serve_submit": (C.c_int, [C.c_void_p, C.POINTER(Desc), C.c_uint32, C.POINTER(C.c_uint64)]),
+    "vxl_sph_serve_step": (C.c_int, [C.c_void_p, C.c_float, C.POINTER(ServeReport)]),
+    "vxl_sph_serve_poll": (C.c_int, [C.c_void_p, C.c_uint64, C.POINTER(RequestStatus)]),
+    "vxl_sph_serve_read": (C.c_int, [C.c_void_p, C.c_uint64, _FP, _FP]),
 }
 
 _lib = None
@@ -387,6 +421,191 @@ class Scene:
         s.hdr = header(Stats)
         _check(self.lib.vxl_sph_get_stats(self._h, C.byref(s)))
         return s
+
+
+def _desc_of(params: Params, pos, vel, pmass, n_fluid: int, device: int = 0, keep: list | None = None) -> Desc:
+    pos = np.ascontiguousarray(pos, dtype=np.float32).reshape(-1, 3)
+    vel = np.ascontiguousarray(vel, dtype=np.float32).reshape(-1, 3)
+    pmass = np.ascontiguousarray(pmass, dtype=np.float32).reshape(-1)
+    if params.particle_mass == 0.0 and n_fluid > 0:
+        params.particle_mass = float(pmass[0])
+    d = Desc()
+    d.hdr = header(Desc)
+    d.params = params
+    d.n_fluid = n_fluid
+    d.n_boundary = pos.shape[0] - n_fluid
+    d.pos_xyz = _fptr(pos)
+    d.vel_xyz = _fptr(vel)
+    d.pmass = _fptr(pmass)
+    d.device = device
+    if keep is not None:
+        keep.extend([pos, vel, pmass])
+    return d
+
+
+class Batch:
+    """Many independent scenes in one handle (the batched form): stepped together, one
+    launch per kernel per substep for all scenes."""
+
+    def __init__(self, specs, device: int = 0, cell_capacity: int = 0):
+        lib = load()
+        keep: list = []
+        arr = (Desc * len(specs))()
+        for i, sp in enumerate(specs):
+            arr[i] = _desc_of(sp.params, sp.pos, sp.vel, sp.pmass, sp.n_fluid, device, keep)
+        h = C.c_void_p()
+        _check(lib.vxl_sph_create_batch(arr, len(specs), device, cell_capacity, C.byref(h)))
+        self._h = h
+        self.lib = lib
+        self.specs = list(specs)
+        for q, sp in enumerate(specs):
+            if sp.spans:
+                a, n = spans_array(sp.spans)  # scene-local particle indices
+                _check(lib.vxl_sph_set_spans_scene(h, q, a, n))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _check(self.lib.vxl_sph_destroy(self._h))
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def n_scenes(self) -> int:
+        return int(self.lib.vxl_sph_scene_count(self._h))
+
+    def step_tick(self, dt_tick: float):
+        _check(self.lib.vxl_sph_step_tick(self._h, dt_tick, None, 0, None))
+        return self.reactions()
+
+    def step_tick_async(self, dt_tick: float):
+        _check(self.lib.vxl_sph_step_tick_async(self._h, dt_tick, None, 0))
+
+    def sync(self):
+        _check(self.lib.vxl_sph_sync(self._h, None, 0))
+
+    def reactions(self):
+        n = C.c_uint32()
+        _check(self.lib.vxl_sph_reactions_all(self._h, None, 0, C.byref(n)))
+        out = (Reaction * max(n.value, 1))()
+        _check(self.lib.vxl_sph_reactions_all(self._h, out, n.value, C.byref(n)))
+        return [(out[q].body, np.array(out[q].force[:], np.float32), np.array(out[q].torque[:], np.float32))
+                for q in range(n.value)]
+
+    def substep(self, dt: float):
+        _check(self.lib.vxl_sph_substep(self._h, dt))
+
+    def read_state(self, scene: int):
+        n = self.specs[scene].n_total
+        p = np.empty((n, 3), np.float32)
+        v = np.empty((n, 3), np.float32)
+        _check(self.lib.vxl_sph_read_state_scene(self._h, scene, _fptr(p), _fptr(v)))
+        return p, v
+
+    def write_state(self, scene: int, pos, vel):
+        pp = None if pos is None else np.ascontiguousarray(pos, dtype=np.float32).reshape(-1, 3)
+        vv = None if vel is None else np.ascontiguousarray(vel, dtype=np.float32).reshape(-1, 3)
+        _check(self.lib.vxl_sph_write_state_scene(self._h, scene, _fptr(pp), _fptr(vv)))
+
+    def export_grid(self, scene: int):
+        info = GridInfo()
+        info.hdr = header(GridInfo)
+        _check(self.lib.vxl_sph_export_grid_scene(self._h, scene, None, None, 0, None, C.byref(info)))
+        n = self.specs[scene].n_total
+        items = np.empty(n, np.uint32)
+        start = np.empty(info.total + 1, np.uint32)
+        bins = np.empty(n, np.uint32)
+        _check(self.lib.vxl_sph_export_grid_scene(self._h, scene, _u32ptr(items), _u32ptr(start), info.total + 1,
+                                                  _u32ptr(bins), C.byref(info)))
+        return items, start, bins, info
+
+    def set_tuning(self, block: int, tile: int, waves: int = 1):
+        t = Tuning()
+        t.hdr = header(Tuning)
+        t.block, t.tile, t.waves = block, tile, waves
+        _check(self.lib.vxl_sph_set_tuning(self._h, C.byref(t)))
+
+    def tuning(self):
+        t = Tuning()
+        t.hdr = header(Tuning)
+        _check(self.lib.vxl_sph_get_tuning(self._h, C.byref(t)))
+        return t.block, t.tile, t.waves
+
+    def autotune(self, dt_tick: float, trials: int = 3):
+        t = Tuning()
+        t.hdr = header(Tuning)
+        _check(self.lib.vxl_sph_autotune(self._h, dt_tick, trials, C.byref(t)))
+        return {"block": t.block, "tile": t.tile, "waves": t.waves, "ms_per_substep": t.ms_per_substep}
+
+    def set_stream(self, stream_handle: int | None) -> None:
+        _check(self.lib.vxl_sph_set_stream(self._h, C.c_void_p(stream_handle or 0)))
+
+    def set_profile(self, on: bool) -> None:
+        _check(self.lib.vxl_sph_set_profile(self._h, 1 if on else 0))
+
+    profile = Scene.profile
+
+    def stats(self) -> Stats:
+        s = Stats()
+        s.hdr = header(Stats)
+        _check(self.lib.vxl_sph_get_stats(self._h, C.byref(s)))
+        return s
+
+
+class Server:
+    """The served form: a request loop with continuous batching under an HBM budget."""
+
+    QUEUED, RUNNING, DONE, REJECTED = range(4)
+
+    def __init__(self, budget_bytes: int, device: int = 0, max_scenes: int = 4096):
+        lib = load()
+        h = C.c_void_p()
+        _check(lib.vxl_sph_serve_create(device, budget_bytes, max_scenes, C.byref(h)))
+        self._h = h
+        self.lib = lib
+        self.n_total = {}
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _check(self.lib.vxl_sph_serve_destroy(self._h))
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def submit(self, spec, ticks: int) -> int:
+        keep: list = []
+        d = _desc_of(spec.params, spec.pos, spec.vel, spec.pmass, spec.n_fluid, 0, keep)
+        rid = C.c_uint64()
+        _check(self.lib.vxl_sph_serve_submit(self._h, C.byref(d), ticks, C.byref(rid)))
+        self.n_total[rid.value] = spec.n_total
+        return rid.value
+
+    def step(self, dt_tick: float) -> ServeReport:
+        r = ServeReport()
+        r.hdr = header(ServeReport)
+        _check(self.lib.vxl_sph_serve_step(self._h, dt_tick, C.byref(r)))
+        return r
+
+    def poll(self, rid: int) -> RequestStatus:
+        st = RequestStatus()
+        st.hdr = header(RequestStatus)
+        _check(self.lib.vxl_sph_serve_poll(self._h, rid, C.byref(st)))
+        return st
+
+    def read(self, rid: int):
+        n = self.n_total[rid]
+        p = np.empty((n, 3), np.float32)
+        v = np.empty((n, 3), np.float32)
+        _check(self.lib.vxl_sph_serve_read(self._h, rid, _fptr(p), _fptr(v)))
+        return p, v
 
 
 class PhysGpuBackend:

@@ -18,8 +18,8 @@ CSRC = PKG / "csrc"
 LIB_DIR = PKG / "lib"
 LIB = LIB_DIR / "libvxl_sph.so"
 
-SOURCES = ["sph_capi.cu", "lattice.cpp", "sph_static_grid.cu"]
-HEADERS = ["sph_device.cuh", "sph_kernels.cuh", "vxl_sph_internal.h"]
+SOURCES = ["sph_capi.cu", "sph_engine.cu", "sph_serve.cu", "lattice.cpp", "sph_static_grid.cu"]
+HEADERS = ["sph_device.cuh", "sph_engine.cuh", "sph_engine.h", "vxl_sph_internal.h"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
