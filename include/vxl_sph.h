@@ -228,7 +228,7 @@ vxl_status vxl_sph_profile_read(vxl_sph_handle* h, uint32_t k, const char** name
                                 uint64_t* launches);
 
 /* ------------------------------------------------------------------ batched form
- * One handle can hold many independent scenes: they are packed
+ * One handle can hold many independent scenes (the batched workload): they are packed
  * into one particle pool and stepped together, one launch per kernel per substep for
  * all scenes, with each scene's own constants and grid (a segmented sort on
  * scene-offset cell keys) and the particle passes run as persistent kernels over a
@@ -258,9 +258,10 @@ vxl_status vxl_sph_read_fields_scene(vxl_sph_handle* h, uint32_t scene, float* d
  * order; *n receives the count (call with cap = 0 to size). */
 vxl_status vxl_sph_reactions_all(vxl_sph_handle* h, vxl_sph_reaction* out, uint32_t cap, uint32_t* n);
 
-/* Launch shape of the particle passes: threads per block (128 or 256), slots per work
- * item of the persistent passes (multiple of 128) and persistent blocks per SM (as a
- * multiple of the occupancy limit). */
+/* Launch shape of the particle passes: threads per block (128 or 256), slots per tile
+ * (a multiple of 128, at least one block) and the scheduling: waves = 0 runs one block
+ * per tile, waves = k > 0 runs k x the occupancy limit of persistent blocks that draw
+ * tiles from a counter. Default {256, 256, 0}. */
 typedef struct vxl_sph_tuning {
   vxl_block_header hdr;
   uint32_t block;
@@ -276,7 +277,7 @@ vxl_status vxl_sph_get_tuning(vxl_sph_handle* h, vxl_sph_tuning* t);
 vxl_status vxl_sph_autotune(vxl_sph_handle* h, float dt_tick, uint32_t trials, vxl_sph_tuning* best);
 
 /* ------------------------------------------------------------------ served form
- * A request loop: scene-step requests are submitted at any time,
+ * A request loop (the served workload): scene-step requests are submitted at any time,
  * admitted while their device footprint fits an HBM budget, stepped together with
  * every other admitted scene, and retired when their tick count is reached; the set of
  * scenes is repacked at substep boundaries (admission and retirement happen between

@@ -318,8 +318,8 @@ vxl_status vxl_sph_set_tuning(vxl_sph_handle* h, const vxl_sph_tuning* t) {
   HANDLE_OR_FAIL(h);
   if (!t) return set_error(VXL_NULL_POINTER, "tuning is NULL");
   if (!check_header(t->hdr, sizeof(vxl_sph_tuning))) return set_error(VXL_SIZE_MISMATCH, "tuning header");
-  if ((t->block != 128 && t->block != 256) || t->tile < 128 || t->tile % 128 != 0 || t->waves < 1 || t->waves > 4)
-    return set_error(VXL_INVALID_ARGUMENT, "block must be 128/256, tile a multiple of 128, waves 1..4");
+  if ((t->block != 128 && t->block != 256) || t->tile < t->block || t->tile % 128 != 0 || t->waves > 4)
+    return set_error(VXL_INVALID_ARGUMENT, "block must be 128/256, tile a multiple of 128 and >= block, waves 0..4");
   h->e->set_tuning(vxl::Tuning{t->block, t->tile, t->waves});
   return VXL_OK;
 }

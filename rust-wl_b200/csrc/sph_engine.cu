@@ -27,6 +27,7 @@ thread_local std::string g_last_error;
   } while (0)
 
 constexpr int kThreads = 256;
+constexpr uint32_t kBoundaryTile = 128;  // boundary particles per tile of the reaction pass
 inline uint32_t blocks_for(uint64_t n, int t = kThreads) { return (uint32_t)((n + t - 1) / t); }
 
 enum KernelId : int {
@@ -163,7 +164,7 @@ vxl_status Engine::alloc_all() {
   A(dalloc(&start_, cell_cap_ + 1));
   A(dalloc(&partial_, cell_cap_ / kScanTile + 2));
   A(dalloc(&sc_d_, scene_cap_));
-  tiles_cap_ = (uint32_t)(n / 64 + scene_cap_ + 1);
+  tiles_cap_ = (uint32_t)(n / 64 + 2ull * scene_cap_ + 2);  // particle tiles (>= 128 slots) + boundary tiles
   A(dalloc(&tiles_d_, tiles_cap_));
   A(dalloc(&ctl_d_, 1));
   if (s != VXL_OK) return s;
@@ -217,9 +218,9 @@ void Engine::set_stream(cudaStream_t s) {
 void Engine::set_tuning(const Tuning& t) {
   tuning_ = t;
   if (tuning_.block != 128 && tuning_.block != 256) tuning_.block = 256;
-  if (tuning_.tile < 128) tuning_.tile = 128;
+  if (tuning_.tile < tuning_.block) tuning_.tile = tuning_.block;
   tuning_.tile = (tuning_.tile / 128) * 128;
-  if (tuning_.waves < 1) tuning_.waves = 1;
+  if (tuning_.waves > 4) tuning_.waves = 4;
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device_);
   int occ_d = 1, occ_f = 1, occ_b = 1;
@@ -232,9 +233,10 @@ void Engine::set_tuning(const Tuning& t) {
   }
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_b, k_e_bforce, 128, 0);
   cudaGetLastError();
+  // waves == 0: one block per tile (the grid is sized from the tile count at launch)
   grid_density_ = sms * std::max(1, occ_d) * (int)tuning_.waves;
   grid_force_ = sms * std::max(1, occ_f) * (int)tuning_.waves;
-  grid_bforce_ = sms * std::max(1, occ_b);
+  grid_bforce_ = tuning_.waves ? sms * std::max(1, occ_b) : 0;
   if (graph_) {
     cudaGraphExecDestroy(graph_);
     graph_ = nullptr;
@@ -251,9 +253,17 @@ vxl_status Engine::rebuild_tiles() {
       tiles_h_->push_back(TileDev{q, si.base + f, std::min(tuning_.tile, n - f), 0u});
   }
   ntiles_ = (uint32_t)tiles_h_->size();
-  if (ntiles_ > tiles_cap_) return set_error(VXL_INVALID_ARGUMENT, "tile list above capacity");
-  if (ntiles_) {
-    CU(cudaMemcpyAsync(tiles_d_, tiles_h_->data(), ntiles_ * sizeof(TileDev), cudaMemcpyHostToDevice, stream_));
+  // boundary tiles (reference order) of the reaction pass, after the particle tiles
+  for (uint32_t q = 0; q < scenes_.size(); ++q) {
+    const SceneInfo& si = scenes_[q];
+    for (uint32_t f = 0; f < si.nb; f += kBoundaryTile)
+      tiles_h_->push_back(TileDev{q, si.base + si.nf + f, std::min(kBoundaryTile, si.nb - f), 0u});
+  }
+  nbtiles_ = (uint32_t)tiles_h_->size() - ntiles_;
+  if (ntiles_ + nbtiles_ > tiles_cap_) return set_error(VXL_INVALID_ARGUMENT, "tile list above capacity");
+  if (!tiles_h_->empty()) {
+    CU(cudaMemcpyAsync(tiles_d_, tiles_h_->data(), tiles_h_->size() * sizeof(TileDev), cudaMemcpyHostToDevice,
+                       stream_));
     CU(cudaStreamSynchronize(stream_));
   }
   ++membership_epoch_;
@@ -506,10 +516,10 @@ vxl_status Engine::export_grid(uint32_t q, uint32_t* items, uint32_t* start, uin
   uint32_t* tmp = (uint32_t*)stage_;
   if (start) {
     if (start_cap < total + 1) return set_error(VXL_SIZE_MISMATCH, "start buffer smaller than cells + 1");
-    if (total + 1 > 8ull * slot_cap_) return set_error(VXL_SIZE_MISMATCH, "table larger than the staging buffer");
-    k_e_export_start<<<blocks_for(total + 1), kThreads, 0, stream_>>>(start_, sc_d_, q, tmp);
-    CU(cudaMemcpyAsync(start, tmp, (total + 1) * 4, cudaMemcpyDeviceToHost, stream_));
+    // the scene's slice of the global table, rebased to scene-local slots on the host
+    CU(cudaMemcpyAsync(start, start_ + rec.cell_off, (total + 1) * 4, cudaMemcpyDeviceToHost, stream_));
     CU(cudaStreamSynchronize(stream_));
+    for (uint64_t c = 0; c <= total; ++c) start[c] -= rec.base;
   }
   if (items && n) {
     k_e_export_items<<<blocks_for(n), kThreads, 0, stream_>>>(orig_, si.base, n, tmp);
@@ -577,7 +587,7 @@ vxl_status Engine::stage_spans() {
     }
   first.push_back((uint32_t)ch.size());
   const uint32_t ns = (uint32_t)sp.size(), nc = (uint32_t)ch.size();
-  if (ns > spans_cap_ || nc > chunks_cap_) {
+  if (!spans_h_ || ns > spans_cap_ || nc > chunks_cap_) {
     void* d[] = {spans_d_, chunks_d_, chunk_first_d_, react_partial_, breact_d_};
     for (void* p : d)
       if (p) cudaFree(p);
@@ -716,27 +726,31 @@ void Engine::enqueue_substep(bool with_reactions) {
                                                        (float4*)vel_[1], orig_, slot_of_));
   const uint32_t stride = (uint32_t)slot_cap_;
   const bool rec = record_;
+  const uint32_t per_tile = std::max<uint32_t>(ntiles_, 1);
+  const uint32_t gd = grid_density_ ? (uint32_t)grid_density_ : per_tile;
+  const uint32_t gf = grid_force_ ? (uint32_t)grid_force_ : per_tile;
+  const uint32_t gb = grid_bforce_ ? (uint32_t)grid_bforce_ : std::max<uint32_t>(nbtiles_, 1);
   if (tuning_.block == 128) {
-    LAUNCH(KID_DENSITY, k_e_density<128><<<grid_density_, 128, 0, st>>>(p1, start_, sc_d_, tiles_d_, ntiles_, ctl_d_,
+    LAUNCH(KID_DENSITY, k_e_density<128><<<gd, 128, 0, st>>>(p1, start_, sc_d_, tiles_d_, ntiles_, ctl_d_,
                                                                         (float2*)rc_, press_, nbr_, nbr_n_, nbr_cap_,
                                                                         stride));
-    LAUNCH(KID_FORCE, k_e_force<128><<<grid_force_, 128, 0, st>>>(
+    LAUNCH(KID_FORCE, k_e_force<128><<<gf, 128, 0, st>>>(
                           p1, v1, (const float2*)rc_, start_, nbr_, nbr_n_, nbr_cap_, stride, sc_d_, tiles_d_,
                           ntiles_, ctl_d_, (float4*)pos_[0], (float4*)vel_[0], rec ? (float4*)acc_ : nullptr,
                           rec ? (float4*)xsph_ : nullptr));
   } else {
-    LAUNCH(KID_DENSITY, k_e_density<256><<<grid_density_, 256, 0, st>>>(p1, start_, sc_d_, tiles_d_, ntiles_, ctl_d_,
+    LAUNCH(KID_DENSITY, k_e_density<256><<<gd, 256, 0, st>>>(p1, start_, sc_d_, tiles_d_, ntiles_, ctl_d_,
                                                                         (float2*)rc_, press_, nbr_, nbr_n_, nbr_cap_,
                                                                         stride));
-    LAUNCH(KID_FORCE, k_e_force<256><<<grid_force_, 256, 0, st>>>(
+    LAUNCH(KID_FORCE, k_e_force<256><<<gf, 256, 0, st>>>(
                           p1, v1, (const float2*)rc_, start_, nbr_, nbr_n_, nbr_cap_, stride, sc_d_, tiles_d_,
                           ntiles_, ctl_d_, (float4*)pos_[0], (float4*)vel_[0], rec ? (float4*)acc_ : nullptr,
                           rec ? (float4*)xsph_ : nullptr));
   }
   if (nb_total > 0 && ((with_reactions && nspans_ > 0) || rec)) {
-    LAUNCH(KID_BFORCE, k_e_bforce<<<grid_bforce_, 128, 0, st>>>(p1, v1, (const float2*)rc_, start_, orig_, nbr_,
-                                                                nbr_n_, nbr_cap_, stride, sc_d_, tiles_d_, ntiles_,
-                                                                ctl_d_, (float4*)bforce_));
+    LAUNCH(KID_BFORCE, k_e_bforce<<<gb, 128, 0, st>>>(p1, v1, (const float2*)rc_, start_, orig_, nbr_, nbr_n_,
+                                                      nbr_cap_, stride, sc_d_, slot_of_, tiles_d_ + ntiles_,
+                                                      nbtiles_, ctl_d_, (float4*)bforce_));
   }
   if (with_reactions && nspans_ > 0 && nchunks_ > 0) {
     LAUNCH(KID_REACT_CHUNKS, k_react_chunks<<<nchunks_, kReactThreads, 0, st>>>(
@@ -930,15 +944,17 @@ vxl_status Engine::autotune(float dt_tick, uint32_t trials, Tuning* best, float*
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
+  // candidates: block {128, 256} x tile {1, 2, 4} blocks x (one block per tile, or
+  // persistent at 1 or 2 x the occupancy limit)
   const uint32_t blocks[2] = {128, 256};
-  const uint32_t tiles_c[5] = {256, 512, 1024, 2048, 4096};
-  const uint32_t waves_c[2] = {1, 2};
+  const uint32_t tile_mult[3] = {1, 2, 4};
+  const uint32_t waves_c[3] = {0, 1, 2};
   for (uint32_t bi = 0; st == VXL_OK && bi < 2; ++bi)
-    for (uint32_t ti = 0; st == VXL_OK && ti < 5; ++ti)
-      for (uint32_t wi = 0; st == VXL_OK && wi < 2; ++wi) {
+    for (uint32_t ti = 0; st == VXL_OK && ti < 3; ++ti)
+      for (uint32_t wi = 0; st == VXL_OK && wi < 3; ++wi) {
         st = copy_all(false);
         if (st != VXL_OK) break;
-        set_tuning(Tuning{blocks[bi], tiles_c[ti], waves_c[wi]});
+        set_tuning(Tuning{blocks[bi], blocks[bi] * tile_mult[ti], waves_c[wi]});
         enqueue_substep(false);  // warm-up
         cudaEventRecord(e0, stream_);
         for (uint32_t r = 0; r < trials; ++r) enqueue_substep(false);

@@ -30,6 +30,15 @@
 
 #include "sph_device.cuh"
 
+// Resident threads per SM the density and force passes are compiled for (register
+// budget = 65536 / this).
+#ifndef VXL_DENSITY_THREADS_PER_SM
+#define VXL_DENSITY_THREADS_PER_SM 2048
+#endif
+#ifndef VXL_FORCE_THREADS_PER_SM
+#define VXL_FORCE_THREADS_PER_SM 1024
+#endif
+
 namespace vxl {
 
 constexpr uint32_t kErrCellCap = 1u << 3;  // the scenes' cells exceed the cell capacity
@@ -148,6 +157,16 @@ __device__ __forceinline__ uint32_t next_tile(uint32_t* counter) {
   const uint32_t t = s_tile;
   __syncthreads();
   return t;
+}
+
+// Tile scheduling of the particle passes. A grid of at least ntiles blocks runs one
+// block per tile (the hardware block scheduler balances); a smaller grid is persistent
+// and its blocks draw tiles from the atomic counter until the list is exhausted.
+__device__ __forceinline__ uint32_t first_tile(uint32_t* counter, uint32_t ntiles) {
+  return gridDim.x >= ntiles ? blockIdx.x : next_tile(counter);
+}
+__device__ __forceinline__ uint32_t following_tile(uint32_t* counter, uint32_t ntiles) {
+  return gridDim.x >= ntiles ? ntiles : next_tile(counter);
 }
 
 // ---------------------------------------------------------------- set-up kernels
@@ -577,15 +596,13 @@ __device__ __forceinline__ void walk27(const GridBox& g, const uint32_t* __restr
 // boundary particles): nbr[k * stride + s], k < cap, with the full count in nbr_n[s]
 // (a count above cap sends the consumers back to walking the cells).
 template <int kBlock>
-__global__ void __launch_bounds__(kBlock, 1024 / kBlock) k_e_density(
+__global__ void __launch_bounds__(kBlock, VXL_DENSITY_THREADS_PER_SM / kBlock) k_e_density(
     const float4* __restrict__ pos, const uint32_t* __restrict__ start, const SceneDev* __restrict__ sc,
     const TileDev* __restrict__ tiles, uint32_t ntiles, EngineCtl* ctl, float2* __restrict__ rc,
     float* __restrict__ press_out, uint32_t* __restrict__ nbr, uint32_t* __restrict__ nbr_n, uint32_t cap,
     uint32_t stride) {
   if (ctl->err & kErrCellCap) return;
-  for (;;) {
-    const uint32_t t = next_tile(&ctl->work[kWorkDensity]);
-    if (t >= ntiles) break;
+  for (uint32_t t = first_tile(&ctl->work[kWorkDensity], ntiles); t < ntiles; t = following_tile(&ctl->work[kWorkDensity], ntiles)) {
     const TileDev td = tiles[t];
     const SceneDev& S = sc[td.scene];
     const GridBox g = S.g;
@@ -641,16 +658,14 @@ __global__ void __launch_bounds__(kBlock, 1024 / kBlock) k_e_density(
 // writes the integrated state to (pos_out, vel_out) in the same slot order; accumulates
 // each tile's fluid AABB into its scene's accumulator for the next grid box.
 template <int kBlock>
-__global__ void __launch_bounds__(kBlock, 768 / kBlock) k_e_force(
+__global__ void __launch_bounds__(kBlock, VXL_FORCE_THREADS_PER_SM / kBlock) k_e_force(
     const float4* __restrict__ pos, const float4* __restrict__ vel, const float2* __restrict__ rc,
     const uint32_t* __restrict__ start, const uint32_t* __restrict__ nbr, const uint32_t* __restrict__ nbr_n,
     uint32_t cap, uint32_t stride, SceneDev* __restrict__ sc, const TileDev* __restrict__ tiles, uint32_t ntiles,
     EngineCtl* ctl, float4* __restrict__ pos_out, float4* __restrict__ vel_out, float4* __restrict__ acc_out,
     float4* __restrict__ xsph_out) {
   if (ctl->err & kErrCellCap) return;
-  for (;;) {
-    const uint32_t t = next_tile(&ctl->work[kWorkForce]);
-    if (t >= ntiles) break;
+  for (uint32_t t = first_tile(&ctl->work[kWorkForce], ntiles); t < ntiles; t = following_tile(&ctl->work[kWorkForce], ntiles)) {
     const TileDev td = tiles[t];
     SceneDev& S = sc[td.scene];
     const SphConst& k = S.k;
@@ -775,26 +790,27 @@ __device__ __forceinline__ float bforce_pair(const SphConst& k, float r2, float 
 // fluid i in ascending reference index (the outer loop of force_pass_serial). Here the
 // boundary particle takes its fluid neighbours (recorded by the density pass, or found by
 // walking the 27 cells when that list overflowed), orders them by reference index and sums
-// in that order, so the result is the same sum. Output by global reference index.
+// in that order, so the result is the same sum. Runs over boundary tiles in reference
+// order (every lane a boundary particle; slot_of finds its sorted slot); output by global
+// reference index.
 __global__ void __launch_bounds__(128) k_e_bforce(
     const float4* __restrict__ pos, const float4* __restrict__ vel, const float2* __restrict__ rc,
     const uint32_t* __restrict__ start, const uint32_t* __restrict__ orig, const uint32_t* __restrict__ nbr,
     const uint32_t* __restrict__ nbr_n, uint32_t cap, uint32_t stride, const SceneDev* __restrict__ sc,
-    const TileDev* __restrict__ tiles, uint32_t ntiles, EngineCtl* ctl, float4* __restrict__ bforce) {
+    const uint32_t* __restrict__ slot_of, const TileDev* __restrict__ btiles, uint32_t ntiles, EngineCtl* ctl,
+    float4* __restrict__ bforce) {
   if (ctl->err & kErrCellCap) return;
-  for (;;) {
-    const uint32_t t = next_tile(&ctl->work[kWorkBforce]);
-    if (t >= ntiles) break;
-    const TileDev td = tiles[t];
+  for (uint32_t t = first_tile(&ctl->work[kWorkBforce], ntiles); t < ntiles; t = following_tile(&ctl->work[kWorkBforce], ntiles)) {
+    const TileDev td = btiles[t];
     const SceneDev& S = sc[td.scene];
     const SphConst& k = S.k;
     const GridBox g = S.g;
     const uint32_t* cst = start + S.cell_off;
     const float h2 = k.h2;
     for (uint32_t i = threadIdx.x; i < td.count; i += blockDim.x) {
-      const uint32_t s = td.first + i;
+      const uint32_t o = td.first + i;  // global reference index of a boundary particle
+      const uint32_t s = slot_of[o];
       const float4 pj = pos[s];
-      if (pj.w > 0.0f) continue;  // fluid slot
       const float4 vj = vel[s];
       const float2 rcj = rc[s];
       const float mj = -pj.w;
@@ -869,7 +885,7 @@ __global__ void __launch_bounds__(128) k_e_bforce(
           first = false;
         }
       }
-      bforce[orig[s]] = make_float4(bx, by, bz, 0.0f);
+      bforce[o] = make_float4(bx, by, bz, 0.0f);
     }
   }
 }
@@ -989,14 +1005,6 @@ __global__ void k_e_export_bins(const uint32_t* __restrict__ start, const uint32
 }
 
 // One scene's slice of the cell table, rebased to the scene's first slot.
-__global__ void k_e_export_start(const uint32_t* __restrict__ start, const SceneDev* __restrict__ sc, uint32_t scene,
-                                 uint32_t* __restrict__ out) {
-  const SceneDev& S = sc[scene];
-  const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c > S.cells) return;
-  out[c] = start[S.cell_off + c] - S.base;
-}
-
 __global__ void k_e_export_items(const uint32_t* __restrict__ orig, uint32_t base, uint32_t n,
                                  uint32_t* __restrict__ out) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;

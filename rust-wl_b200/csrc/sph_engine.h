@@ -25,8 +25,8 @@ struct SpanChunk;
 // Launch shape of the particle passes (chosen by the autotuner for batches).
 struct Tuning {
   uint32_t block = 256;   // threads per block of the density/force passes (128 or 256)
-  uint32_t tile = 1024;   // slots per work item of the persistent passes
-  uint32_t waves = 1;     // persistent blocks per SM, as a multiple of the occupancy limit / 2
+  uint32_t tile = 256;    // slots per tile (a multiple of 128, at least one block)
+  uint32_t waves = 0;     // 0: one block per tile; k > 0: persistent, k x the occupancy limit
 };
 
 struct SceneInfo {
@@ -146,7 +146,7 @@ class Engine {
   SceneDev* sc_h_ = nullptr;  // pinned mirror (pushed when dt or membership changes)
   TileDev* tiles_d_ = nullptr;
   std::vector<TileDev>* tiles_h_ = nullptr;
-  uint32_t ntiles_ = 0, tiles_cap_ = 0;
+  uint32_t ntiles_ = 0, nbtiles_ = 0, tiles_cap_ = 0;
   EngineCtl* ctl_d_ = nullptr;
   EngineCtl* ctl_h_ = nullptr;  // pinned
   // reactions

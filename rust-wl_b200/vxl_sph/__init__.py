@@ -523,7 +523,7 @@ class Batch:
                                                   _u32ptr(bins), C.byref(info)))
         return items, start, bins, info
 
-    def set_tuning(self, block: int, tile: int, waves: int = 1):
+    def set_tuning(self, block: int, tile: int, waves: int = 0):
         t = Tuning()
         t.hdr = header(Tuning)
         t.block, t.tile, t.waves = block, tile, waves
