@@ -9,7 +9,13 @@ particle through one full substep), summed over ranks, divided by the slowest ra
 device time. Multi-GPU runs are independent replicas (each rank steps its own scene;
 no collective on the data path), so scaling is weak.
 
+The plain run also carries two comparisons (single GPU only): "batched", 256 uneven
+tanks stepped in one handle against looping the plain step over them, and "served",
+Poisson-arriving requests under continuous batching against running them one by one on
+plain handles (p50/p99 per-tick latency beside aggregate throughput).
+
   python bench.py [--gpus N] [--steps K] [--warmup W] [--workload dam1|dam0|dam10m]
+  python bench.py --workload batched|served ...   # the batched or served form as the headline
   python bench.py --impl reference ...   # the reference CPU path (C++ restatement) on the host cores
 """
 from __future__ import annotations
@@ -226,6 +232,8 @@ def run_ours(args) -> None:
     scene.set_profile(True)
     scene.step_tick_async(dt_tick, spec.spans)  # capture the profiled graph outside the timed region
     scene.sync()
+    # the timed ticks start from the workload's initial state (the states the CPU arm times)
+    scene.write_state(spec.pos, spec.vel)
     scene.set_profile(True)  # reset accumulators
 
     clocks = ClockSampler(local)
@@ -308,6 +316,12 @@ def run_ours(args) -> None:
            "d2h_bytes_per_step": spec.n_total * 24,
            "api": "vxl_sph_write_state + vxl_sph_step_tick + vxl_sph_read_state, pinned host buffers"}
 
+    mix = {}
+    if world == 1 and not args.no_mix:
+        scene.close()
+        mix["batched"] = measure_batched(local, steps=3, warmup=3)
+        mix["served"] = measure_served(local, n_requests=args.requests, rate=args.rate, tick_scale=args.tick_scale)
+
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(spec)
@@ -329,11 +343,245 @@ def run_ours(args) -> None:
             "gpu_launches": int(stats.launches_last_tick) * args.steps,
             "clocks": clk,
             "step_ms": step_ms,
+            **mix,
         }
         print(json.dumps(line), flush=True)
     scene.close()
     if dist:
         dist.destroy_process_group()
+
+
+def _pct(v, q):
+    return float(np.percentile(np.asarray(v, np.float64), q)) if len(v) else None
+
+
+def measure_batched(local: int, steps: int, warmup: int, n_scenes: int = 256, seed: int = 7,
+                    plain_loop: bool = True) -> dict:
+    """The batched workload (n_scenes uneven dam-break tanks in one handle, autotuned launch
+    shape, one graph per tick) against looping the plain step scene by scene.
+
+    Batched: device time of `steps` ticks (CUDA events on the handle's stream, L2 flushed
+    between ticks) and the wall time of the same ticks through the synchronous C ABI call.
+    Plain loop: `steps` ticks of every scene on its own plain handle, one synchronous
+    vxl_sph_step_tick after another (the reference's per-stepper call pattern), wall time.
+    """
+    import torch
+    import vxl_sph
+    from vxl_sph import scenes
+
+    t_build = time.perf_counter()
+    specs = scenes.batched_mix(n_scenes, seed)
+    t_build = time.perf_counter() - t_build
+    nf = sum(s.n_fluid for s in specs)
+    nb = sum(s.n_boundary for s in specs)
+    sub = specs[0].params.substeps
+    dt_tick = float(np.float32(1.0) / np.float32(60.0))
+    batch = vxl_sph.Batch(specs, device=local)
+    stream = torch.cuda.Stream(device=local)
+    batch.set_stream(stream.cuda_stream)
+    t0 = time.perf_counter()
+    tune = batch.autotune(dt_tick, trials=2)
+    tune_s = time.perf_counter() - t0
+    for _ in range(max(warmup, 3)):
+        batch.step_tick(dt_tick)
+    l2_flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
+    batch.set_profile(True)
+    batch.step_tick(dt_tick)
+    for q, sp in enumerate(specs):  # timed ticks start from the initial state
+        batch.write_state(q, sp.pos, sp.vel)
+    batch.set_profile(True)
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    torch.cuda.synchronize()
+    for k in range(steps):
+        batch.profile()
+        with torch.cuda.stream(stream):
+            l2_flush.zero_()
+            evs[k][0].record(stream)
+        batch.step_tick_async(dt_tick)
+        with torch.cuda.stream(stream):
+            evs[k][1].record(stream)
+    torch.cuda.synchronize()
+    batch.sync()
+    dev_ms = sum(a.elapsed_time(b) for a, b in evs)
+    prof = batch.profile()
+    batch.set_profile(False)
+    stats = batch.stats()
+    cells = int(stats.cells)
+    launches = int(stats.launches_last_tick)
+    batch.step_tick(dt_tick)  # re-capture the tick graph without profiling events
+    for q, sp in enumerate(specs):
+        batch.write_state(q, sp.pos, sp.vel)
+    # wall time through the synchronous call (what a caller sees)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        batch.step_tick(dt_tick)
+    wall_s = time.perf_counter() - t0
+    batch.close()
+    del batch
+    updates = nf * sub * steps
+    peak, _ = hbm_peak()
+    sb = substep_bytes(nf, nb, cells)
+    out = {
+        "workload": f"{n_scenes} dam-break tanks, N log-U[4096, 262144], aspect U[0.5, 2], fill U[0.2, 0.6], "
+                    f"s U[0.005, 0.02] m, h = 2 s, closed tanks, seed {seed}",
+        "scenes": n_scenes, "n_fluid": nf, "n_boundary": nb, "cells": cells, "substeps": sub, "ticks": steps,
+        "value": updates / (dev_ms / 1e3), "unit": UNIT, "ms_per_tick": dev_ms / steps,
+        "wall_value": updates / wall_s, "wall_ms_per_tick": 1e3 * wall_s / steps,
+        "tuning": tune, "autotune_s": tune_s, "build_s": t_build, "gpu_launches_per_tick": launches,
+        "substep_roofline": {"bytes": sb, "ms": dev_ms / (steps * sub),
+                             "achieved_gbs": sb / (dev_ms / (steps * sub) / 1e3) / 1e9, "peak": peak},
+        "kernels_ms_per_substep": {k: v[0] / max(steps * sub, 1) for k, v in sorted(prof.items())},
+    }
+    out["substep_roofline"]["frac"] = out["substep_roofline"]["achieved_gbs"] / peak
+    if plain_loop:
+        plain = [vxl_sph.Scene(s.params, s.pos, s.vel, s.pmass, s.n_fluid, device=local) for s in specs]
+        for sc, s in zip(plain, specs):
+            sc.step_tick(dt_tick, s.spans)  # graph capture + warm-up
+            sc.write_state(s.pos, s.vel)  # back to the initial state
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            for sc, s in zip(plain, specs):
+                sc.step_tick(dt_tick, s.spans)
+        plain_s = time.perf_counter() - t0
+        for sc, s in zip(plain, specs):
+            sc.write_state(s.pos, s.vel)
+        torch.cuda.synchronize()
+        # the same loop with every scene's tick enqueued before any is awaited
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            for sc, s in zip(plain, specs):
+                sc.step_tick_async(dt_tick, s.spans)
+            for sc in plain:
+                sc.sync()
+        plain_async_s = time.perf_counter() - t0
+        for sc in plain:
+            sc.close()
+        out["plain_loop"] = {"value": updates / plain_s, "ms_per_tick": 1e3 * plain_s / steps,
+                             "call": "vxl_sph_step_tick per scene, synchronous, one after another"}
+        out["plain_loop_async"] = {"value": updates / plain_async_s, "ms_per_tick": 1e3 * plain_async_s / steps,
+                                   "call": "vxl_sph_step_tick_async on every scene, then vxl_sph_sync on each"}
+        out["speedup_vs_plain_loop"] = plain_s / wall_s
+        out["speedup_vs_plain_async"] = plain_async_s / wall_s
+    return out
+
+
+def measure_served(local: int, n_requests: int = 48, rate: float = 200.0, tick_scale: float = 0.1,
+                   budget_bytes: int = 150 * 10**9, seed: int = 11, plain: bool = True) -> dict:
+    """The served workload: Poisson arrivals submitted as wall time reaches them, one
+    vxl_sph_serve_step (retire, admit, one substep of every admitted scene) after another
+    until every request is done. Reports aggregate fluid particle-updates/s over the
+    makespan (first arrival to last completion), per-tick latency percentiles pooled over
+    every tick of every request, and request latency (completion - arrival). The plain path
+    runs the same requests one after another on plain handles (FIFO from their arrival
+    times: each starts when it has arrived and the previous one is done)."""
+    import torch
+    import vxl_sph
+    from vxl_sph import scenes
+
+    reqs = scenes.served_stream(n_requests, rate, seed, tick_scale=tick_scale)
+    dt_tick = float(np.float32(1.0) / np.float32(60.0))
+    sub = reqs[0].spec.params.substeps
+    updates = sum(r.spec.n_fluid * sub * r.ticks for r in reqs)
+    srv = vxl_sph.Server(budget_bytes=budget_bytes, device=local)
+    torch.cuda.synchronize()
+    ids, py_submit = [], []
+    i = 0
+    steps = 0
+    peak_active = 0
+    t0 = time.perf_counter()
+    while True:
+        now = time.perf_counter() - t0
+        while i < len(reqs) and reqs[i].arrival_s <= now:
+            ids.append(srv.submit(reqs[i].spec, reqs[i].ticks))
+            py_submit.append(time.perf_counter() - t0)
+            i += 1
+        rep = srv.step(dt_tick)
+        steps += 1
+        peak_active = max(peak_active, rep.active)
+        if rep.active == 0 and rep.queued == 0:
+            if i >= len(reqs):
+                break
+            time.sleep(max(0.0, reqs[i].arrival_s - (time.perf_counter() - t0)))
+    t_end = time.perf_counter() - t0
+    sts = [srv.poll(q) for q in ids]
+    ticks_ms = np.concatenate([srv.tick_times(q) for q in ids])
+    # server clock -> this loop's clock (both steady; offset from the submit times)
+    off = float(np.median([st.submit_s - ps for st, ps in zip(sts, py_submit)]))
+    done = [st.done_s - off for st in sts]
+    makespan = t_end - reqs[0].arrival_s
+    req_lat = [d - r.arrival_s for d, r in zip(done, reqs)]
+    assert all(st.state == vxl_sph.Server.DONE for st in sts)
+    srv.close()
+    del srv
+    out = {
+        "workload": f"{n_requests} requests, Poisson rate {rate}/s, N log-U[8192, 1048576], ticks U[60, 600] x "
+                    f"{tick_scale}, dam-break or sloshing (closed tanks), budget {budget_bytes / 1e9:.0f} GB, "
+                    f"seed {seed}",
+        "requests": n_requests, "rate_per_s": rate, "fluid_particles": sum(r.spec.n_fluid for r in reqs),
+        "ticks_total": sum(r.ticks for r in reqs), "serve_steps": steps, "peak_active": peak_active,
+        "value": updates / makespan, "unit": UNIT, "makespan_s": makespan,
+        "tick_p50_ms": _pct(ticks_ms, 50), "tick_p99_ms": _pct(ticks_ms, 99),
+        "request_p50_s": _pct(req_lat, 50), "request_p99_s": _pct(req_lat, 99),
+    }
+    if plain:
+        free_at = 0.0
+        p_ticks, p_lat = [], []
+        busy = 0.0
+        for r in reqs:
+            t_start = time.perf_counter()
+            sc = vxl_sph.Scene(r.spec.params, r.spec.pos, r.spec.vel, r.spec.pmass, r.spec.n_fluid, device=local)
+            for _ in range(r.ticks):
+                ta = time.perf_counter()
+                sc.step_tick(dt_tick, r.spec.spans)
+                p_ticks.append(1e3 * (time.perf_counter() - ta))
+            sc.read_state()
+            sc.close()
+            run = time.perf_counter() - t_start
+            busy += run
+            start = max(r.arrival_s, free_at)
+            free_at = start + run
+            p_lat.append(free_at - r.arrival_s)
+        p_makespan = free_at - reqs[0].arrival_s
+        out["plain"] = {"value": updates / p_makespan, "makespan_s": p_makespan, "busy_s": busy,
+                        "tick_p50_ms": _pct(p_ticks, 50), "tick_p99_ms": _pct(p_ticks, 99),
+                        "request_p50_s": _pct(p_lat, 50), "request_p99_s": _pct(p_lat, 99),
+                        "call": "per request: vxl_sph_create, ticks of vxl_sph_step_tick, read_state, destroy"}
+        out["speedup_vs_plain"] = p_makespan / makespan
+    return out
+
+
+def run_mix(args) -> None:
+    """--workload batched|served: the batched or served form as the headline line."""
+    import torch
+    import vxl_sph
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    torch.cuda.set_device(local)
+    vxl_sph.load()
+    clocks = ClockSampler(local)
+    clocks.start()
+    if args.workload == "batched":
+        m = measure_batched(local, args.steps, args.warmup)
+        value, ms = m["value"], m["ms_per_tick"]
+        cfg = {"workload": "batched", **{k: m[k] for k in ("scenes", "n_fluid", "n_boundary", "cells", "substeps")},
+               "step": "one 60 Hz tick of every scene", "l2": "flushed between ticks",
+               "parallelism": "scenes packed in one handle, one GPU"}
+    else:
+        m = measure_served(local, n_requests=args.requests, rate=args.rate, tick_scale=args.tick_scale)
+        value, ms = m["value"], None
+        cfg = {"workload": "served", "requests": m["requests"], "rate_per_s": m["rate_per_s"],
+               "step": "one serve step = one substep of every admitted scene",
+               "parallelism": "continuous batching, one GPU"}
+    clk = clocks.stop()
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic: seeded tanks (no public dataset exists)",
+                "config": cfg, args.workload: m, "clocks": clk}
+        print(json.dumps(line), flush=True)
 
 
 def run_ncu_case(args) -> None:
@@ -356,7 +604,11 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", default="dam1", choices=["dam0", "dam1", "dam10m"])
+    ap.add_argument("--workload", default="dam1", choices=["dam0", "dam1", "dam10m", "batched", "served"])
+    ap.add_argument("--requests", type=int, default=48, help="served: number of requests")
+    ap.add_argument("--rate", type=float, default=200.0, help="served: Poisson arrival rate (1/s)")
+    ap.add_argument("--tick-scale", type=float, default=0.1, help="served: factor on the 60-600 tick counts")
+    ap.add_argument("--no-mix", action="store_true", help="skip the batched/served comparison in the plain run")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ncu-case", action="store_true", help="build + warm-up ticks only (for ncu captures)")
     args = ap.parse_args()
@@ -364,6 +616,8 @@ def main():
         run_ncu_case(args)
     elif args.impl == "reference":
         run_reference(args)
+    elif args.workload in ("batched", "served"):
+        run_mix(args)
     else:
         run_ours(args)
 

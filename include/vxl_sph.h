@@ -322,6 +322,10 @@ vxl_status vxl_sph_serve_step(vxl_sph_server* s, float dt_tick, vxl_sph_serve_re
 vxl_status vxl_sph_serve_poll(vxl_sph_server* s, uint64_t id, vxl_sph_request_status* out);
 /* Positions/velocities of a running or finished request (scene-local order). */
 vxl_status vxl_sph_serve_read(vxl_sph_server* s, uint64_t id, float* pos_xyz, float* vel_xyz);
+/* Wall time of each completed tick of a request, in milliseconds, in tick order (from
+ * its admission, or the end of its previous tick, to the end of the substep that
+ * completed the tick). Writes min(cap, ticks done) values and sets *n to ticks done. */
+vxl_status vxl_sph_serve_tick_times(vxl_sph_server* s, uint64_t id, double* out_ms, uint32_t cap, uint32_t* n);
 
 /* Neighbour-table build that allocates nothing. No counterpart in the reference: it is
  * for callers that cannot allocate device memory while they run — an engine that

@@ -265,4 +265,15 @@ vxl_status vxl_sph_serve_read(vxl_sph_server* s, uint64_t id, float* pos_xyz, fl
   return set_error(VXL_NOT_READY, "request was rejected");
 }
 
+vxl_status vxl_sph_serve_tick_times(vxl_sph_server* s, uint64_t id, double* out_ms, uint32_t cap, uint32_t* n) {
+  if (!s || !n) return set_error(VXL_NULL_POINTER, "NULL argument");
+  if (cap > 0 && !out_ms) return set_error(VXL_NULL_POINTER, "out_ms is NULL with cap > 0");
+  auto it = s->req.find(id);
+  if (it == s->req.end()) return set_error(VXL_INVALID_ARGUMENT, "unknown request id");
+  const std::vector<double>& t = it->second.tick_ms;
+  *n = (uint32_t)t.size();
+  for (uint32_t q = 0; q < cap && q < t.size(); ++q) out_ms[q] = t[q];
+  return VXL_OK;
+}
+
 }  // extern "C"

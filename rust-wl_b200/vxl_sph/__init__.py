@@ -172,6 +172,8 @@ SIGNATURES = {
     "vxl_sph_serve_step": (C.c_int, [C.c_void_p, C.c_float, C.POINTER(ServeReport)]),
     "vxl_sph_serve_poll": (C.c_int, [C.c_void_p, C.c_uint64, C.POINTER(RequestStatus)]),
     "vxl_sph_serve_read": (C.c_int, [C.c_void_p, C.c_uint64, _FP, _FP]),
+    "vxl_sph_serve_tick_times": (C.c_int, [C.c_void_p, C.c_uint64, C.POINTER(C.c_double), C.c_uint32,
+                                           C.POINTER(C.c_uint32)]),
 }
 
 _lib = None
@@ -606,6 +608,16 @@ class Server:
         v = np.empty((n, 3), np.float32)
         _check(self.lib.vxl_sph_serve_read(self._h, rid, _fptr(p), _fptr(v)))
         return p, v
+
+    def tick_times(self, rid: int) -> np.ndarray:
+        """Wall time (ms) of each completed tick of a request."""
+        n = C.c_uint32()
+        _check(self.lib.vxl_sph_serve_tick_times(self._h, rid, None, 0, C.byref(n)))
+        out = np.empty(n.value, np.float64)
+        if n.value:
+            _check(self.lib.vxl_sph_serve_tick_times(self._h, rid, out.ctypes.data_as(C.POINTER(C.c_double)),
+                                                     n.value, C.byref(n)))
+        return out
 
 
 class PhysGpuBackend:

@@ -135,6 +135,18 @@ def tank_bodies(inner, t: float, first_id: int = 0) -> list:
     ]
 
 
+def closed_tank_bodies(inner, t: float, first_id: int = 0) -> list:
+    """tank_bodies plus a lid over [0, inner] (a sixth static box at y = ly): the batched
+    and served tanks run for hundreds of ticks with the reference constants, whose
+    acoustic CFL number c0 dt / h exceeds 1 at most spacings, and the lid keeps
+    splashing particles inside the tank."""
+    lx, ly, lz = (F(x) for x in inner)
+    t = F(t)
+    th = t * F(0.5)
+    lid = Body(first_id + 5, (lx * F(0.5) + t, th, lz * F(0.5) + t), (lx * F(0.5), ly + th, lz * F(0.5)))
+    return tank_bodies(inner, t, first_id) + [lid]
+
+
 def baseline_params(spacing: float, substeps: int = 10, layers: int = 1, **over) -> Params:
     kw = dict(rest_density=1000.0, smoothing_radius=2.0 * spacing, xsph_viscosity=0.5, sound_speed=20.0,
               gamma_tait=7.0, substeps=substeps, boundary_layers=layers, gravity=(0.0, -9.81, 0.0),
@@ -201,6 +213,93 @@ def small_dam(n=(8, 8, 8), spacing: float = 0.05, tank=(0.8, 0.6, 0.6), seed: in
               ticks: int = 10, **over) -> SceneSpec:
     """A small tank scene for parity tests (same construction, smaller sizes)."""
     return dam_break("small", n, spacing, tank, ticks, seed, substeps=substeps, **over)
+
+
+def tank_scene(kind: str, n_target: int, spacing: float, aspect: float, fill: float, seed: int,
+               ticks: int = 300, substeps: int = 10, closed: bool = True, name: str | None = None) -> SceneSpec:
+    """One tank of the batched and served workloads. The tank (W, H, D) = (aspect L, L, L)
+    holds n_target s^3 / fill of volume; the fluid (about n_target particles) is either a
+    dam-break column over the full depth at the x = 0 end, 0.9 H tall, or a sloshing layer
+    over the whole floor (fill H deep) with horizontal velocity u = U0 sin(pi x / W),
+    U0 ~ U(0.2, 0.6) m/s from the seed. Spacing s is rounded to float32; h = 2 s."""
+    s = float(F(spacing))
+    vol = n_target * s ** 3 / fill
+    L = (vol / aspect) ** (1.0 / 3.0)
+    W, H, D = aspect * L, L, L
+    nz = max(1, int(D / s))
+    if kind == "dam":
+        ny = max(1, int(0.9 * H / s))
+        nx = max(1, int(round(n_target / (ny * nz))))
+        nx = min(nx, max(1, int(W / s)))
+    elif kind == "slosh":
+        nx = max(1, int(W / s))
+        ny = max(1, min(int(round(n_target / (nx * nz))), int(0.9 * H / s)))
+    else:
+        raise ValueError(kind)
+    tank = (float(F(W)), float(F(H)), float(F(D)))
+    params = baseline_params(s, substeps=substeps)
+    fluid = jitter(fluid_block((0.0, 0.0, 0.0), (nx, ny, nz), s), s, seed)
+    walls = (closed_tank_bodies if closed else tank_bodies)(tank, 2.0 * s)
+    meta = {"kind": kind, "dims": (nx, ny, nz), "tank": tank, "fill": float(nx * ny * nz * s ** 3 / (W * H * D)),
+            "aspect": aspect, "seed": seed, "closed": closed}
+    spec = assemble(name or f"{kind}{n_target}", params, fluid, walls, s, ticks, meta)
+    if kind == "slosh":
+        rng = np.random.Generator(np.random.PCG64(seed + 7919))
+        u0 = F(rng.uniform(0.2, 0.6))
+        x = spec.pos[:spec.n_fluid, 0]
+        spec.vel[:spec.n_fluid, 0] = (u0 * np.sin(F(np.pi) * x / F(W)).astype(F)).astype(F)
+        spec.meta["u0"] = float(u0)
+    return spec
+
+
+def _log_uniform_int(rng, lo: int, hi: int) -> int:
+    return int(round(float(np.exp(rng.uniform(np.log(lo), np.log(hi))))))
+
+
+def batched_mix(n_scenes: int = 256, seed: int = 7, n_lo: int = 4096, n_hi: int = 262144,
+                ticks: int = 300, substeps: int = 10) -> list:
+    """The batched workload: n_scenes independent dam-break tanks with particle counts
+    log-uniform in [n_lo, n_hi], aspect U(0.5, 2), fill U(0.2, 0.6) and spacing
+    U(0.005, 0.02) m (h = 2 s), all drawn from one seed (PCG64); each scene's jitter seed
+    is seed * 100003 + its index."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    out = []
+    for q in range(n_scenes):
+        n = _log_uniform_int(rng, n_lo, n_hi)
+        aspect = float(rng.uniform(0.5, 2.0))
+        fill = float(rng.uniform(0.2, 0.6))
+        s = float(rng.uniform(0.005, 0.02))
+        out.append(tank_scene("dam", n, s, aspect, fill, seed * 100003 + q, ticks, substeps, name=f"mix{q}"))
+    return out
+
+
+@dataclass
+class Request:
+    arrival_s: float
+    spec: SceneSpec
+    ticks: int
+
+
+def served_stream(n_requests: int, rate: float, seed: int = 11, n_lo: int = 8192, n_hi: int = 1048576,
+                  ticks_lo: int = 60, ticks_hi: int = 600, tick_scale: float = 1.0, substeps: int = 10) -> list:
+    """The served workload: requests arriving as a Poisson process of `rate` per second,
+    particle counts log-uniform in [n_lo, n_hi], ticks uniform in [ticks_lo, ticks_hi]
+    (times tick_scale, at least 1), a dam-break or sloshing tank (even odds) with aspect,
+    fill and spacing drawn as in batched_mix, each from its own per-request seed."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    t = 0.0
+    out = []
+    for r in range(n_requests):
+        t += float(rng.exponential(1.0 / rate))
+        n = _log_uniform_int(rng, n_lo, n_hi)
+        ticks = max(1, int(round(int(rng.integers(ticks_lo, ticks_hi + 1)) * tick_scale)))
+        kind = "dam" if rng.uniform() < 0.5 else "slosh"
+        aspect = float(rng.uniform(0.5, 2.0))
+        fill = float(rng.uniform(0.2, 0.6))
+        s = float(rng.uniform(0.005, 0.02))
+        spec = tank_scene(kind, n, s, aspect, fill, seed * 1000003 + r, ticks, substeps, name=f"req{r}")
+        out.append(Request(t, spec, ticks))
+    return out
 
 
 CONFIGS = {"dam0": dam0, "dam1": dam1, "dam10m": dam10m}

@@ -120,6 +120,9 @@ def test_served_requests_equal_alone_runs(vxl):
         st = srv.poll(i)
         assert st.state == vxl.Server.DONE and st.ticks_done == ticks[r]
         assert st.tick_p99_ms >= st.tick_p50_ms > 0
+        tt = srv.tick_times(i)
+        assert tt.shape == (ticks[r],) and np.all(tt > 0)
+        assert tt.min() <= st.tick_p50_ms <= tt.max()
         p, v = srv.read(i)
         ap, av = _alone(vxl, specs[r], ticks[r])
         _assert_same(p, ap, f"request {r} pos")
