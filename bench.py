@@ -564,13 +564,14 @@ def run_mix(args) -> None:
     clocks = ClockSampler(local)
     clocks.start()
     if args.workload == "batched":
-        m = measure_batched(local, args.steps, args.warmup)
+        m = measure_batched(local, args.steps, args.warmup, n_scenes=args.scenes, plain_loop=not args.no_plain)
         value, ms = m["value"], m["ms_per_tick"]
         cfg = {"workload": "batched", **{k: m[k] for k in ("scenes", "n_fluid", "n_boundary", "cells", "substeps")},
                "step": "one 60 Hz tick of every scene", "l2": "flushed between ticks",
                "parallelism": "scenes packed in one handle, one GPU"}
     else:
-        m = measure_served(local, n_requests=args.requests, rate=args.rate, tick_scale=args.tick_scale)
+        m = measure_served(local, n_requests=args.requests, rate=args.rate, tick_scale=args.tick_scale,
+                           plain=not args.no_plain)
         value, ms = m["value"], None
         cfg = {"workload": "served", "requests": m["requests"], "rate_per_s": m["rate_per_s"],
                "step": "one serve step = one substep of every admitted scene",
@@ -588,9 +589,19 @@ def run_ncu_case(args) -> None:
     """Smallest run of the workload for a profiler: build, `--warmup` ticks, exit."""
     import vxl_sph
     vxl_sph.load()
+    dt_tick = float(np.float32(1.0) / np.float32(60.0))
+    if args.workload == "batched":
+        from vxl_sph import scenes
+        specs = scenes.batched_mix(args.scenes)
+        batch = vxl_sph.Batch(specs)
+        for _ in range(max(args.warmup, 1)):
+            batch.step_tick(dt_tick)
+        batch.close()
+        print(json.dumps({"ncu_case": "batched", "scenes": args.scenes, "ticks": max(args.warmup, 1),
+                          "n_fluid": sum(s.n_fluid for s in specs), "n_boundary": sum(s.n_boundary for s in specs)}))
+        return
     spec = build_scene(args.workload)
     scene = vxl_sph.Scene(spec.params, spec.pos, spec.vel, spec.pmass, spec.n_fluid)
-    dt_tick = float(np.float32(1.0) / np.float32(60.0))
     for _ in range(max(args.warmup, 1)):
         scene.step_tick(dt_tick, spec.spans)
     scene.close()
@@ -609,6 +620,8 @@ def main():
     ap.add_argument("--rate", type=float, default=200.0, help="served: Poisson arrival rate (1/s)")
     ap.add_argument("--tick-scale", type=float, default=0.1, help="served: factor on the 60-600 tick counts")
     ap.add_argument("--no-mix", action="store_true", help="skip the batched/served comparison in the plain run")
+    ap.add_argument("--scenes", type=int, default=256, help="batched: number of tanks")
+    ap.add_argument("--no-plain", action="store_true", help="batched/served: skip the plain-path comparison")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ncu-case", action="store_true", help="build + warm-up ticks only (for ncu captures)")
     args = ap.parse_args()
