@@ -260,11 +260,8 @@ def run_ours(args) -> None:
     stats = scene.stats()
     cells = int(stats.cells)
 
-    t_max = total_ms
-    if dist:
-        t = torch.tensor([total_ms], device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_max = float(t.item())
+    from vxl_sph import placement
+    t_max = placement.max_over_ranks(total_ms, dist, f"cuda:{local}")
     updates = spec.n_fluid * sub * args.steps * world
     value = updates / (t_max / 1e3)
 
@@ -307,11 +304,7 @@ def run_ours(args) -> None:
         scene.write_state(pin_p, pin_v)
         scene.step_tick(dt_tick, spec.spans)
         scene.read_state(out=(pin_p, pin_v))
-    e2e_s = time.perf_counter() - t0
-    if dist:
-        t = torch.tensor([e2e_s], device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = placement.max_over_ranks(time.perf_counter() - t0, dist, f"cuda:{local}")
     e2e = {"value": updates / e2e_s, "unit": UNIT, "h2d_bytes_per_step": spec.n_total * 24,
            "d2h_bytes_per_step": spec.n_total * 24,
            "api": "vxl_sph_write_state + vxl_sph_step_tick + vxl_sph_read_state, pinned host buffers"}
@@ -356,7 +349,7 @@ def _pct(v, q):
 
 
 def measure_batched(local: int, steps: int, warmup: int, n_scenes: int = 256, seed: int = 7,
-                    plain_loop: bool = True) -> dict:
+                    plain_loop: bool = True, rank: int = 0, world: int = 1, dist=None) -> dict:
     """The batched workload (n_scenes uneven dam-break tanks in one handle, autotuned launch
     shape, one graph per tick) against looping the plain step scene by scene.
 
@@ -364,13 +357,19 @@ def measure_batched(local: int, steps: int, warmup: int, n_scenes: int = 256, se
     between ticks) and the wall time of the same ticks through the synchronous C ABI call.
     Plain loop: `steps` ticks of every scene on its own plain handle, one synchronous
     vxl_sph_step_tick after another (the reference's per-stepper call pattern), wall time.
+    On several GPUs each rank steps its share of the scenes (scene-parallel placement, no
+    collective on the data path); rates are summed over ranks and divided by the slowest
+    rank's time.
     """
     import torch
     import vxl_sph
-    from vxl_sph import scenes
+    from vxl_sph import placement, scenes
 
     t_build = time.perf_counter()
     specs = scenes.batched_mix(n_scenes, seed)
+    if world > 1:
+        mine = placement.assign_scenes([s.n_total for s in specs], world)[rank]
+        specs = [specs[q] for q in mine]
     t_build = time.perf_counter() - t_build
     nf = sum(s.n_fluid for s in specs)
     nb = sum(s.n_boundary for s in specs)
@@ -402,7 +401,7 @@ def measure_batched(local: int, steps: int, warmup: int, n_scenes: int = 256, se
             evs[k][1].record(stream)
     torch.cuda.synchronize()
     batch.sync()
-    dev_ms = sum(a.elapsed_time(b) for a, b in evs)
+    dev_ms = placement.max_over_ranks(sum(a.elapsed_time(b) for a, b in evs), dist, f"cuda:{local}")
     prof = batch.profile()
     batch.set_profile(False)
     stats = batch.stats()
@@ -416,16 +415,18 @@ def measure_batched(local: int, steps: int, warmup: int, n_scenes: int = 256, se
     t0 = time.perf_counter()
     for _ in range(steps):
         batch.step_tick(dt_tick)
-    wall_s = time.perf_counter() - t0
+    wall_s = placement.max_over_ranks(time.perf_counter() - t0, dist, f"cuda:{local}")
     batch.close()
     del batch
-    updates = nf * sub * steps
+    nf_all = int(placement.sum_over_ranks(nf, dist, f"cuda:{local}"))
+    updates = nf_all * sub * steps
     peak, _ = hbm_peak()
     sb = substep_bytes(nf, nb, cells)
     out = {
         "workload": f"{n_scenes} dam-break tanks, N log-U[4096, 262144], aspect U[0.5, 2], fill U[0.2, 0.6], "
                     f"s U[0.005, 0.02] m, h = 2 s, closed tanks, seed {seed}",
-        "scenes": n_scenes, "n_fluid": nf, "n_boundary": nb, "cells": cells, "substeps": sub, "ticks": steps,
+        "scenes": n_scenes, "scenes_this_rank": len(specs), "n_fluid": nf_all, "n_boundary_this_rank": nb,
+        "cells_this_rank": cells, "substeps": sub, "ticks": steps,
         "value": updates / (dev_ms / 1e3), "unit": UNIT, "ms_per_tick": dev_ms / steps,
         "wall_value": updates / wall_s, "wall_ms_per_tick": 1e3 * wall_s / steps,
         "tuning": tune, "autotune_s": tune_s, "build_s": t_build, "gpu_launches_per_tick": launches,
@@ -444,7 +445,7 @@ def measure_batched(local: int, steps: int, warmup: int, n_scenes: int = 256, se
         for _ in range(steps):
             for sc, s in zip(plain, specs):
                 sc.step_tick(dt_tick, s.spans)
-        plain_s = time.perf_counter() - t0
+        plain_s = placement.max_over_ranks(time.perf_counter() - t0, dist, f"cuda:{local}")
         for sc, s in zip(plain, specs):
             sc.write_state(s.pos, s.vel)
         torch.cuda.synchronize()
@@ -455,7 +456,7 @@ def measure_batched(local: int, steps: int, warmup: int, n_scenes: int = 256, se
                 sc.step_tick_async(dt_tick, s.spans)
             for sc in plain:
                 sc.sync()
-        plain_async_s = time.perf_counter() - t0
+        plain_async_s = placement.max_over_ranks(time.perf_counter() - t0, dist, f"cuda:{local}")
         for sc in plain:
             sc.close()
         out["plain_loop"] = {"value": updates / plain_s, "ms_per_tick": 1e3 * plain_s / steps,
@@ -468,22 +469,28 @@ def measure_batched(local: int, steps: int, warmup: int, n_scenes: int = 256, se
 
 
 def measure_served(local: int, n_requests: int = 48, rate: float = 200.0, tick_scale: float = 0.1,
-                   budget_bytes: int = 150 * 10**9, seed: int = 11, plain: bool = True) -> dict:
+                   budget_bytes: int = 150 * 10**9, seed: int = 11, plain: bool = True, rank: int = 0,
+                   world: int = 1, dist=None) -> dict:
     """The served workload: Poisson arrivals submitted as wall time reaches them, one
     vxl_sph_serve_step (retire, admit, one substep of every admitted scene) after another
     until every request is done. Reports aggregate fluid particle-updates/s over the
     makespan (first arrival to last completion), per-tick latency percentiles pooled over
     every tick of every request, and request latency (completion - arrival). The plain path
     runs the same requests one after another on plain handles (FIFO from their arrival
-    times: each starts when it has arrived and the previous one is done)."""
+    times: each starts when it has arrived and the previous one is done). On several GPUs
+    each rank serves its share of the stream (placement by work, no collective on the data
+    path); throughput is summed over ranks over the longest makespan."""
     import torch
     import vxl_sph
-    from vxl_sph import scenes
+    from vxl_sph import placement, scenes
 
     reqs = scenes.served_stream(n_requests, rate, seed, tick_scale=tick_scale)
+    if world > 1:
+        mine = placement.assign_scenes([r.spec.n_fluid * r.ticks for r in reqs], world)[rank]
+        reqs = [reqs[q] for q in mine]
     dt_tick = float(np.float32(1.0) / np.float32(60.0))
     sub = reqs[0].spec.params.substeps
-    updates = sum(r.spec.n_fluid * sub * r.ticks for r in reqs)
+    updates = placement.sum_over_ranks(sum(r.spec.n_fluid * sub * r.ticks for r in reqs), dist, f"cuda:{local}")
     srv = vxl_sph.Server(budget_bytes=budget_bytes, device=local)
     torch.cuda.synchronize()
     ids, py_submit = [], []
@@ -505,12 +512,14 @@ def measure_served(local: int, n_requests: int = 48, rate: float = 200.0, tick_s
                 break
             time.sleep(max(0.0, reqs[i].arrival_s - (time.perf_counter() - t0)))
     t_end = time.perf_counter() - t0
+    if dist is not None and world > 1:
+        dist.barrier()
     sts = [srv.poll(q) for q in ids]
     ticks_ms = np.concatenate([srv.tick_times(q) for q in ids])
     # server clock -> this loop's clock (both steady; offset from the submit times)
     off = float(np.median([st.submit_s - ps for st, ps in zip(sts, py_submit)]))
     done = [st.done_s - off for st in sts]
-    makespan = t_end - reqs[0].arrival_s
+    makespan = placement.max_over_ranks(t_end - reqs[0].arrival_s, dist, f"cuda:{local}")
     req_lat = [d - r.arrival_s for d, r in zip(done, reqs)]
     assert all(st.state == vxl_sph.Server.DONE for st in sts)
     srv.close()
@@ -519,7 +528,8 @@ def measure_served(local: int, n_requests: int = 48, rate: float = 200.0, tick_s
         "workload": f"{n_requests} requests, Poisson rate {rate}/s, N log-U[8192, 1048576], ticks U[60, 600] x "
                     f"{tick_scale}, dam-break or sloshing (closed tanks), budget {budget_bytes / 1e9:.0f} GB, "
                     f"seed {seed}",
-        "requests": n_requests, "rate_per_s": rate, "fluid_particles": sum(r.spec.n_fluid for r in reqs),
+        "requests": n_requests, "requests_this_rank": len(reqs), "rate_per_s": rate,
+        "fluid_particles_this_rank": sum(r.spec.n_fluid for r in reqs),
         "ticks_total": sum(r.ticks for r in reqs), "serve_steps": steps, "peak_active": peak_active,
         "value": updates / makespan, "unit": UNIT, "makespan_s": makespan,
         "tick_p50_ms": _pct(ticks_ms, 50), "tick_p99_ms": _pct(ticks_ms, 99),
@@ -543,7 +553,7 @@ def measure_served(local: int, n_requests: int = 48, rate: float = 200.0, tick_s
             start = max(r.arrival_s, free_at)
             free_at = start + run
             p_lat.append(free_at - r.arrival_s)
-        p_makespan = free_at - reqs[0].arrival_s
+        p_makespan = placement.max_over_ranks(free_at - reqs[0].arrival_s, dist, f"cuda:{local}")
         out["plain"] = {"value": updates / p_makespan, "makespan_s": p_makespan, "busy_s": busy,
                         "tick_p50_ms": _pct(p_ticks, 50), "tick_p99_ms": _pct(p_ticks, 99),
                         "request_p50_s": _pct(p_lat, 50), "request_p99_s": _pct(p_lat, 99),
@@ -560,22 +570,28 @@ def run_mix(args) -> None:
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     vxl_sph.load()
     clocks = ClockSampler(local)
     clocks.start()
     if args.workload == "batched":
-        m = measure_batched(local, args.steps, args.warmup, n_scenes=args.scenes, plain_loop=not args.no_plain)
+        m = measure_batched(local, args.steps, args.warmup, n_scenes=args.scenes, plain_loop=not args.no_plain,
+                            rank=rank, world=world, dist=dist)
         value, ms = m["value"], m["ms_per_tick"]
-        cfg = {"workload": "batched", **{k: m[k] for k in ("scenes", "n_fluid", "n_boundary", "cells", "substeps")},
+        cfg = {"workload": "batched", **{k: m[k] for k in ("scenes", "n_fluid", "substeps")},
                "step": "one 60 Hz tick of every scene", "l2": "flushed between ticks",
-               "parallelism": "scenes packed in one handle, one GPU"}
+               "parallelism": f"scenes packed in one handle per GPU, scene-parallel x{world}"}
     else:
         m = measure_served(local, n_requests=args.requests, rate=args.rate, tick_scale=args.tick_scale,
-                           plain=not args.no_plain)
+                           plain=not args.no_plain, rank=rank, world=world, dist=dist)
         value, ms = m["value"], None
         cfg = {"workload": "served", "requests": m["requests"], "rate_per_s": m["rate_per_s"],
                "step": "one serve step = one substep of every admitted scene",
-               "parallelism": "continuous batching, one GPU"}
+               "parallelism": f"continuous batching per GPU, request-parallel x{world}"}
     clk = clocks.stop()
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -583,6 +599,9 @@ def run_mix(args) -> None:
                 "vs_baseline": None, "dtype": "f32", "data": "synthetic: seeded tanks (no public dataset exists)",
                 "config": cfg, args.workload: m, "clocks": clk}
         print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
 
 
 def run_ncu_case(args) -> None:

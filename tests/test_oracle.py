@@ -11,6 +11,7 @@ These tests pin it before it is trusted as the checker of the CUDA path:
     crates/vxl-phys-fluid/tests/boundary_reaction_balance.rs).
 """
 import json
+import os
 from pathlib import Path
 
 import numpy as np
@@ -262,3 +263,51 @@ def test_fp64_twin_close(oracle_mod):
     assert np.max(np.abs(ra["dens"] - rb["dens"]) / rb["dens"]) < 1e-5
     amax = np.abs(rb["acc"]).max()
     assert np.max(np.abs(ra["acc"] - rb["acc"])) / amax < 1e-4
+
+
+def _stable_dam():
+    from vxl_sph import scenes
+    # c0 dt / h = 20 * (1/1200) / 0.04 = 0.42: acoustically stable (20 substeps per tick)
+    return scenes.small_dam(n=(10, 14, 10), spacing=0.02, tank=(0.5, 0.5, 0.3), seed=5, substeps=20)
+
+
+def test_dam_break_physics_bands(oracle_mod):
+    """Multi-tick physics of the oracle on a CFL-stable dam break: mass conserved, the column
+    collapses (centre of mass and surface height fall, kinetic energy rises from zero),
+    speeds stay below the free-fall bound, and no fluid particle leaves the tank."""
+    from vxl_sph import diagnostics
+    spec = _stable_dam()
+    tank = spec.meta["tank"]
+    box = ((-0.5 * spec.spacing,) * 3, tuple(t + 0.5 * spec.spacing for t in tank))
+    o = oracle_mod.OracleSystem.from_scene(spec, threads=4)
+    r = o.read_f32()
+    q0 = diagnostics.quantities(r["pos"], r["vel"], spec.n_fluid, spec.params.particle_mass, box)
+    h0 = float(np.max(r["pos"][:spec.n_fluid, 1]))
+    for _ in range(24):
+        o.step(float(np.float32(1.0) / np.float32(60.0)))
+    r = o.read_f32()
+    q1 = diagnostics.quantities(r["pos"], r["vel"], spec.n_fluid, spec.params.particle_mass, box)
+    o.close()
+    assert q1["mass"] == q0["mass"]
+    assert q0["kinetic_energy"] == 0.0 and q1["kinetic_energy"] > 0.0
+    assert q1["com"][1] < q0["com"][1] - 0.01
+    assert q1["com"][0] > q0["com"][0]  # the column spreads towards +x
+    assert q1["surface_height"] < q0["surface_height"]
+    assert q1["max_speed"] < 1.5 * np.sqrt(2.0 * 9.81 * h0)
+    assert q1["escaped_fraction"] == 0.0
+
+
+def test_configured_constants_are_acoustically_unstable(oracle_mod):
+    """The 16,384-particle dam at the configured 10 substeps (c0 dt / h = 0.83): within 5
+    ticks fluid leaves the open tank, which the stable run above never does."""
+    from vxl_sph import diagnostics, scenes
+    spec = scenes.dam0()
+    tank = spec.meta["tank"]
+    box = ((-0.5 * spec.spacing,) * 3, tuple(t + 0.5 * spec.spacing for t in tank))
+    o = oracle_mod.OracleSystem.from_scene(spec, threads=os.cpu_count() or 4)
+    for _ in range(5):
+        o.step(float(np.float32(1.0) / np.float32(60.0)))
+    r = o.read_f32()
+    o.close()
+    q = diagnostics.quantities(r["pos"], r["vel"], spec.n_fluid, spec.params.particle_mass, box)
+    assert q["escaped_fraction"] > 0.01
