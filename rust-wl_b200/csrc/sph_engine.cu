@@ -121,6 +121,9 @@ vxl_status Engine::create(int device, uint64_t slot_cap, uint64_t cell_cap, uint
   e->tiles_h_ = new std::vector<TileDev>();
   cudaError_t ce = cudaSetDevice(device);
   if (ce == cudaSuccess) ce = cudaStreamCreateWithFlags(&e->own_stream_, cudaStreamNonBlocking);
+  if (ce == cudaSuccess) ce = cudaStreamCreateWithFlags(&e->side_, cudaStreamNonBlocking);
+  if (ce == cudaSuccess) ce = cudaEventCreateWithFlags(&e->ev_fork_, cudaEventDisableTiming);
+  if (ce == cudaSuccess) ce = cudaEventCreateWithFlags(&e->ev_join_, cudaEventDisableTiming);
   if (ce != cudaSuccess) {
     cudaGetLastError();
     delete e;  // the destructor releases tiles_h_
@@ -200,11 +203,17 @@ void Engine::free_all() {
   prof_ev_.clear();
   if (own_stream_) cudaStreamDestroy(own_stream_);
   own_stream_ = nullptr;
+  if (side_) cudaStreamDestroy(side_);
+  side_ = nullptr;
+  if (ev_fork_) cudaEventDestroy(ev_fork_);
+  if (ev_join_) cudaEventDestroy(ev_join_);
+  ev_fork_ = ev_join_ = nullptr;
 }
 
 Engine::~Engine() {
   cudaSetDevice(device_);
   if (stream_) cudaStreamSynchronize(stream_);
+  if (side_) cudaStreamSynchronize(side_);
   free_all();
   delete tiles_h_;
 }
@@ -625,22 +634,29 @@ vxl_status Engine::stage_spans() {
 
 // ---------------------------------------------------------------- profiling
 
-void Engine::record_event(cudaEvent_t e) {
-  if (capturing_) cudaEventRecordWithFlags(e, stream_, cudaEventRecordExternal);
-  else cudaEventRecord(e, stream_);
+void Engine::record_event(cudaEvent_t e, cudaStream_t st) {
+  if (capturing_) cudaEventRecordWithFlags(e, st, cudaEventRecordExternal);
+  else cudaEventRecord(e, st);
 }
 
-int Engine::prof_begin(int kid) {
+int Engine::prof_begin(int kid, cudaStream_t st) {
   if (!prof_) return -1;
   if (2 * prof_used_ + 2 > prof_ev_.size()) return -1;  // pre-created in set_profile
   const size_t i = prof_used_++;
   prof_kid_[i] = kid;
-  record_event(prof_ev_[2 * i]);
+  record_event(prof_ev_[2 * i], st);
   return (int)i;
 }
 
-void Engine::prof_end(int i) {
-  if (i >= 0) record_event(prof_ev_[2 * i + 1]);
+void Engine::prof_end(int i, cudaStream_t st) {
+  if (i >= 0) record_event(prof_ev_[2 * i + 1], st);
+}
+
+void Engine::join_side() {
+  if (side_pending_) {
+    cudaStreamWaitEvent(stream_, ev_join_, 0);
+    side_pending_ = false;
+  }
 }
 
 void Engine::prof_collect() {
@@ -692,11 +708,19 @@ vxl_status Engine::profile_read(uint32_t k, const char** name, double* ms, uint6
   return VXL_OK;
 }
 
+#define LAUNCH_ON(kid, stream, ...)   \
+  do {                                \
+    int pe_ = prof_begin(kid, stream);\
+    __VA_ARGS__;                      \
+    prof_end(pe_, stream);            \
+    launches_counter_ += 1;           \
+  } while (0)
+
 #define LAUNCH(kid, ...)          \
   do {                            \
-    int pe_ = prof_begin(kid);    \
+    int pe_ = prof_begin(kid, stream_); \
     __VA_ARGS__;                  \
-    prof_end(pe_);                \
+    prof_end(pe_, stream_);       \
     launches_counter_ += 1;       \
   } while (0)
 
@@ -712,6 +736,9 @@ void Engine::enqueue_substep(bool with_reactions) {
   const float4* v0 = (const float4*)vel_[0];
   const float4* p1 = (const float4*)pos_[1];
   const float4* v1 = (const float4*)vel_[1];
+  // The previous substep's reaction branch reads this substep's inputs-to-be (scene grids,
+  // cell table, sorted buffer, permutation, lists, work counters): join it first.
+  join_side();
   cudaMemsetAsync(ctl_d_->work, 0, sizeof(ctl_d_->work), st);
   LAUNCH(KID_GRIDBOX, k_e_gridbox<<<blocks_for(S, 128), 128, 0, st>>>(sc_d_, S, ctl_d_));
   LAUNCH(KID_CELLOFF, k_e_celloff<<<1, 1024, 0, st>>>(sc_d_, S, ctl_d_, (uint32_t)cell_cap_));
@@ -730,35 +757,45 @@ void Engine::enqueue_substep(bool with_reactions) {
   const uint32_t gd = grid_density_ ? (uint32_t)grid_density_ : per_tile;
   const uint32_t gf = grid_force_ ? (uint32_t)grid_force_ : per_tile;
   const uint32_t gb = grid_bforce_ ? (uint32_t)grid_bforce_ : std::max<uint32_t>(nbtiles_, 1);
-  if (tuning_.block == 128) {
+  if (tuning_.block == 128)
     LAUNCH(KID_DENSITY, k_e_density<128><<<gd, 128, 0, st>>>(p1, start_, sc_d_, tiles_d_, ntiles_, ctl_d_,
-                                                                        (float2*)rc_, press_, nbr_, nbr_n_, nbr_cap_,
-                                                                        stride));
+                                                             (float2*)rc_, press_, nbr_, nbr_n_, nbr_cap_, stride));
+  else
+    LAUNCH(KID_DENSITY, k_e_density<256><<<gd, 256, 0, st>>>(p1, start_, sc_d_, tiles_d_, ntiles_, ctl_d_,
+                                                             (float2*)rc_, press_, nbr_, nbr_n_, nbr_cap_, stride));
+  // Reaction branch on the side stream: it reads only the sorted buffer, the densities and
+  // the lists, so it runs beside the force pass (which writes the other buffer).
+  const bool bforce = nb_total > 0 && ((with_reactions && nspans_ > 0) || rec);
+  const bool react = with_reactions && nspans_ > 0 && nchunks_ > 0;
+  if (bforce || react) {
+    cudaEventRecord(ev_fork_, st);
+    cudaStreamWaitEvent(side_, ev_fork_, 0);
+    if (bforce)
+      LAUNCH_ON(KID_BFORCE, side_,
+                k_e_bforce<<<gb, 128, 0, side_>>>(p1, v1, (const float2*)rc_, start_, orig_, nbr_, nbr_n_, nbr_cap_,
+                                                  stride, sc_d_, slot_of_, tiles_d_ + ntiles_, nbtiles_, ctl_d_,
+                                                  (float4*)bforce_));
+    if (react) {
+      LAUNCH_ON(KID_REACT_CHUNKS, side_,
+                k_react_chunks<<<nchunks_, kReactThreads, 0, side_>>>((const float4*)bforce_, (const float4*)bpos_,
+                                                                      spans_d_, chunks_d_, ctl_d_, react_partial_));
+      LAUNCH_ON(KID_REACT_SPANS, side_,
+                k_react_spans<<<blocks_for(nspans_, 64), 64, 0, side_>>>(react_partial_, chunk_first_d_, ctl_d_,
+                                                                         breact_d_, nspans_));
+    }
+    cudaEventRecord(ev_join_, side_);
+    side_pending_ = true;
+  }
+  if (tuning_.block == 128)
     LAUNCH(KID_FORCE, k_e_force<128><<<gf, 128, 0, st>>>(
                           p1, v1, (const float2*)rc_, start_, nbr_, nbr_n_, nbr_cap_, stride, sc_d_, tiles_d_,
                           ntiles_, ctl_d_, (float4*)pos_[0], (float4*)vel_[0], rec ? (float4*)acc_ : nullptr,
                           rec ? (float4*)xsph_ : nullptr));
-  } else {
-    LAUNCH(KID_DENSITY, k_e_density<256><<<gd, 256, 0, st>>>(p1, start_, sc_d_, tiles_d_, ntiles_, ctl_d_,
-                                                                        (float2*)rc_, press_, nbr_, nbr_n_, nbr_cap_,
-                                                                        stride));
+  else
     LAUNCH(KID_FORCE, k_e_force<256><<<gf, 256, 0, st>>>(
                           p1, v1, (const float2*)rc_, start_, nbr_, nbr_n_, nbr_cap_, stride, sc_d_, tiles_d_,
                           ntiles_, ctl_d_, (float4*)pos_[0], (float4*)vel_[0], rec ? (float4*)acc_ : nullptr,
                           rec ? (float4*)xsph_ : nullptr));
-  }
-  if (nb_total > 0 && ((with_reactions && nspans_ > 0) || rec)) {
-    LAUNCH(KID_BFORCE, k_e_bforce<<<gb, 128, 0, st>>>(p1, v1, (const float2*)rc_, start_, orig_, nbr_, nbr_n_,
-                                                      nbr_cap_, stride, sc_d_, slot_of_, tiles_d_ + ntiles_,
-                                                      nbtiles_, ctl_d_, (float4*)bforce_));
-  }
-  if (with_reactions && nspans_ > 0 && nchunks_ > 0) {
-    LAUNCH(KID_REACT_CHUNKS, k_react_chunks<<<nchunks_, kReactThreads, 0, st>>>(
-                                 (const float4*)bforce_, (const float4*)bpos_, spans_d_, chunks_d_, ctl_d_,
-                                 react_partial_));
-    LAUNCH(KID_REACT_SPANS, k_react_spans<<<blocks_for(nspans_, 64), 64, 0, st>>>(react_partial_, chunk_first_d_,
-                                                                                  ctl_d_, breact_d_, nspans_));
-  }
 }
 
 void Engine::enqueue_tick(float /*dt_tick*/) {
@@ -771,6 +808,7 @@ void Engine::enqueue_tick(float /*dt_tick*/) {
     cudaMemsetAsync(breact_d_, 0, nspans_ * 6 * sizeof(float), st);
   }
   for (uint32_t s = 0; s < sub; ++s) enqueue_substep(true);
+  join_side();
   if (nspans_ > 0) {
     if (sub > 1) {
       const float inv = 1.0f / (float)sub;  // fluid_step.rs:85
@@ -890,6 +928,7 @@ vxl_status Engine::substep(const std::vector<float>& dt) {
   prof_used_ = 0;
   launches_counter_ = 0;
   enqueue_substep(false);
+  join_side();
   cudaMemcpyAsync(ctl_h_, ctl_d_, sizeof(EngineCtl), cudaMemcpyDeviceToHost, stream_);
   prof_pending_ = prof_;
   launches_last_tick_ = launches_counter_;
@@ -958,6 +997,7 @@ vxl_status Engine::autotune(float dt_tick, uint32_t trials, Tuning* best, float*
         enqueue_substep(false);  // warm-up
         cudaEventRecord(e0, stream_);
         for (uint32_t r = 0; r < trials; ++r) enqueue_substep(false);
+        join_side();
         cudaEventRecord(e1, stream_);
         if (cudaStreamSynchronize(stream_) != cudaSuccess) {
           st = set_error(VXL_CUDA_ERROR, "autotune trial failed");

@@ -107,15 +107,22 @@ class Engine {
   void enqueue_tick(float dt_tick);
   vxl_status finish();
   void prof_collect();
-  int prof_begin(int kid);
-  void prof_end(int i);
-  void record_event(cudaEvent_t e);
+  int prof_begin(int kid, cudaStream_t st);
+  void prof_end(int i, cudaStream_t st);
+  void record_event(cudaEvent_t e, cudaStream_t st);
+  void join_side();
 
   template <class T>
   vxl_status dalloc(T** p, size_t count);
 
   int device_ = 0;
   cudaStream_t stream_ = nullptr, own_stream_ = nullptr;
+  // Reaction branch (boundary reactions + per-span sums) forked off the substep onto its
+  // own stream after the density pass and joined before the next sort overwrites its
+  // inputs (or at the end of the tick / substep call).
+  cudaStream_t side_ = nullptr;
+  cudaEvent_t ev_fork_ = nullptr, ev_join_ = nullptr;
+  bool side_pending_ = false;
   uint64_t slot_cap_ = 0, cell_cap_ = 0, used_ = 0;
   uint32_t scene_cap_ = 0, nbr_cap_ = 64;
   uint64_t device_bytes_ = 0;
