@@ -32,11 +32,11 @@ inline uint32_t blocks_for(uint64_t n, int t = kThreads) { return (uint32_t)((n 
 
 enum KernelId : int {
   KID_GRIDBOX, KID_CELLOFF, KID_KEYS, KID_SCAN_PARTIAL, KID_SCAN_TOP, KID_SCAN_FINAL, KID_PLACE, KID_CANON,
-  KID_DENSITY, KID_FORCE, KID_BFORCE, KID_REACT_CHUNKS, KID_REACT_SPANS, KID_SCALE, KID_COUNT
+  KID_DENSITY, KID_FORCE, KID_BFORCE, KID_REACT_CHUNKS, KID_REACT_SPANS, KID_SCALE, KID_HALFMASK, KID_COUNT
 };
 const char* const kKernelNames[KID_COUNT] = {
     "k_gridbox", "k_celloff", "k_keys", "k_scan_partial", "k_scan_top", "k_scan_final", "k_place", "k_canon",
-    "k_density", "k_force", "k_bforce", "k_react_chunks", "k_react_spans", "k_scale"};
+    "k_density", "k_force", "k_bforce", "k_react_chunks", "k_react_spans", "k_scale", "k_halfmask"};
 
 constexpr size_t kSceneHostBytes = offsetof(SceneDev, g);
 
@@ -88,7 +88,7 @@ namespace vxl {
 uint64_t Engine::bytes_per_slot(uint32_t nbr_cap) {
   // pos, vel (x2), orig, slot_of, cellrank, items, rc, press, acc, xsph, bforce, bpos,
   // neighbour list + count, staging
-  return 4 * 16 + 4 + 4 + 8 + 8 + 8 + 4 + 16 + 16 + 16 + 16 + (uint64_t)nbr_cap * 4 + 4 + 32;
+  return 4 * 16 + 4 + 4 + 8 + 8 + 8 + 4 + 16 + 16 + 16 + 16 + (uint64_t)nbr_cap * 4 + 4 + 32 + 1;
 }
 
 uint64_t Engine::bytes_per_cell() { return 8; }
@@ -162,6 +162,7 @@ vxl_status Engine::alloc_all() {
   A(dalloc((float4**)&bpos_, n));
   A(dalloc(&nbr_, (size_t)nbr_cap_ * n));
   A(dalloc(&nbr_n_, n));
+  A(dalloc(&halves_, 4 * (n / 32 + 2)));
   A(dalloc(&stage_, 8 * n));
   A(dalloc(&counts_, cell_cap_ + 1));
   A(dalloc(&start_, cell_cap_ + 1));
@@ -192,7 +193,7 @@ void Engine::free_all() {
   if (graph_) cudaGraphExecDestroy(graph_);
   graph_ = nullptr;
   void* d[] = {pos_[0], pos_[1], vel_[0], vel_[1], orig_, slot_of_, cellrank_, items_, rc_, press_, acc_, xsph_,
-               bforce_, bpos_, nbr_, nbr_n_, stage_, counts_, start_, partial_, sc_d_, tiles_d_, ctl_d_, spans_d_,
+               bforce_, bpos_, nbr_, nbr_n_, halves_, stage_, counts_, start_, partial_, sc_d_, tiles_d_, ctl_d_, spans_d_,
                chunks_d_, chunk_first_d_, react_partial_, breact_d_};
   for (void* p : d)
     if (p) cudaFree(p);
@@ -751,6 +752,8 @@ void Engine::enqueue_substep(bool with_reactions) {
                                                                ntiles_, ctl_d_, (uint2*)items_));
   LAUNCH(KID_CANON, k_e_canon<<<148 * 8, 256, 0, st>>>((const uint2*)items_, start_, ctl_d_, p0, v0, (float4*)pos_[1],
                                                        (float4*)vel_[1], orig_, slot_of_));
+  cudaMemsetAsync(halves_, 0, (size_t)16 * (used_ / 32 + 1), st);
+  LAUNCH(KID_HALFMASK, k_e_halfmask<<<key_blocks, kThreads, 0, st>>>(p1, sc_d_, tiles_d_, ntiles_, ctl_d_, halves_));
   const uint32_t stride = (uint32_t)slot_cap_;
   const bool rec = record_;
   const uint32_t per_tile = std::max<uint32_t>(ntiles_, 1);
@@ -758,10 +761,10 @@ void Engine::enqueue_substep(bool with_reactions) {
   const uint32_t gf = grid_force_ ? (uint32_t)grid_force_ : per_tile;
   const uint32_t gb = grid_bforce_ ? (uint32_t)grid_bforce_ : std::max<uint32_t>(nbtiles_, 1);
   if (tuning_.block == 128)
-    LAUNCH(KID_DENSITY, k_e_density<128><<<gd, 128, 0, st>>>(p1, start_, sc_d_, tiles_d_, ntiles_, ctl_d_,
+    LAUNCH(KID_DENSITY, k_e_density<128><<<gd, 128, 0, st>>>(p1, start_, sc_d_, tiles_d_, ntiles_, ctl_d_, halves_,
                                                              (float2*)rc_, press_, nbr_, nbr_n_, nbr_cap_, stride));
   else
-    LAUNCH(KID_DENSITY, k_e_density<256><<<gd, 256, 0, st>>>(p1, start_, sc_d_, tiles_d_, ntiles_, ctl_d_,
+    LAUNCH(KID_DENSITY, k_e_density<256><<<gd, 256, 0, st>>>(p1, start_, sc_d_, tiles_d_, ntiles_, ctl_d_, halves_,
                                                              (float2*)rc_, press_, nbr_, nbr_n_, nbr_cap_, stride));
   // Reaction branch on the side stream: it reads only the sorted buffer, the densities and
   // the lists, so it runs beside the force pass (which writes the other buffer).

@@ -39,6 +39,11 @@
 #define VXL_FORCE_THREADS_PER_SM 1024
 #endif
 
+// 1: the half-culled walk takes cells with every half reachable as a plain range.
+#ifndef VXL_HALF_FULL_RANGE
+#define VXL_HALF_FULL_RANGE 0
+#endif
+
 namespace vxl {
 
 constexpr uint32_t kErrCellCap = 1u << 3;  // the scenes' cells exceed the cell capacity
@@ -587,6 +592,134 @@ __device__ __forceinline__ void walk27(const GridBox& g, const uint32_t* __restr
   }
 }
 
+// Half-cell masks of the sorted slots, for the density walk: for each aligned block of 32
+// slots, halves[4 * (s >> 5) + a] has bit (s & 31) set iff slot s lies at or above the
+// midplane of its own cell along axis a (x, y, z). One thread per slot over tiles;
+// lanes that share a block and axis combine their bits before one atomicOr.
+__global__ void k_e_halfmask(const float4* __restrict__ pos, const SceneDev* __restrict__ sc,
+                             const TileDev* __restrict__ tiles, uint32_t ntiles, const EngineCtl* __restrict__ ctl,
+                             uint32_t* __restrict__ halves) {
+  if (ctl->err & kErrCellCap) return;
+  const int lane = threadIdx.x & 31;
+  for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const TileDev td = tiles[t];
+    const GridBox g = sc[td.scene].g;
+    if (g.bin < 2.0f * sc[td.scene].k.h) continue;  // the density pass walks this scene unmasked
+    const float hb = g.bin * 0.5f;
+    for (uint32_t b0 = 0; b0 < td.count; b0 += blockDim.x) {
+      const uint32_t i = b0 + threadIdx.x;
+      const bool valid = i < td.count;
+      uint32_t blk = 0xffffffffu, bit = 0, hx = 0, hy = 0, hz = 0;
+      if (valid) {
+        const uint32_t s = td.first + i;
+        const float4 p = pos[s];
+        uint32_t cx, cy, cz;
+        bin_of(g, p.x, p.y, p.z, cx, cy, cz);
+        hx = p.x >= g.minx + (float)cx * g.bin + hb;
+        hy = p.y >= g.miny + (float)cy * g.bin + hb;
+        hz = p.z >= g.minz + (float)cz * g.bin + hb;
+        blk = s >> 5;
+        bit = 1u << (s & 31);
+      }
+      const uint32_t active = __ballot_sync(0xffffffffu, valid);
+      if (valid) {
+        const uint32_t peers = __match_any_sync(active, blk);
+        const uint32_t mx = __reduce_or_sync(peers, hx ? bit : 0u);
+        const uint32_t my = __reduce_or_sync(peers, hy ? bit : 0u);
+        const uint32_t mz = __reduce_or_sync(peers, hz ? bit : 0u);
+        if (lane == __ffs(peers) - 1) {
+          if (mx) atomicOr(&halves[4 * blk], mx);
+          if (my) atomicOr(&halves[4 * blk + 1], my);
+          if (mz) atomicOr(&halves[4 * blk + 2], mz);
+        }
+      }
+    }
+  }
+}
+
+// Per axis, which halves of the three cells (d = -1, 0, +1) along it a particle at p can
+// reach: bit 2 (d + 1) for the lower half, bit 2 (d + 1) + 1 for the upper half. A half is
+// dropped only when the gap from p to its nominal interval exceeds `reach` (h plus a
+// margin far above the rounding of cell faces and midplanes).
+__device__ __forceinline__ uint32_t half_reach_bits(float p, float l, float B, float reach) {
+  const float hb = B * 0.5f;
+  const float gm_lo = fmaxf(p - (l - hb), 0.0f);
+  const float gm_hi = fmaxf(p - l, 0.0f);
+  const float g0_lo = fmaxf(fmaxf(l - p, p - (l + hb)), 0.0f);
+  const float g0_hi = fmaxf(fmaxf((l + hb) - p, p - (l + B)), 0.0f);
+  const float gp_lo = fmaxf((l + B) - p, 0.0f);
+  const float gp_hi = fmaxf((l + B + hb) - p, 0.0f);
+  return (gm_lo <= reach ? 1u : 0u) | (gm_hi <= reach ? 2u : 0u) | (g0_lo <= reach ? 4u : 0u) |
+         (g0_hi <= reach ? 8u : 0u) | (gp_lo <= reach ? 16u : 0u) | (gp_hi <= reach ? 32u : 0u);
+}
+
+// Slot mask of the particles in a block whose half along one axis is reachable.
+__device__ __forceinline__ uint32_t half_select(uint32_t two_bits, uint32_t upper) {
+  return two_bits == 3u ? 0xffffffffu : (two_bits == 2u ? upper : ~upper);
+}
+
+// walk27 with half-cell culling: the same cells in the same order, and inside each cell
+// the same slots in ascending order, except slots lying in a half-cell (along any axis)
+// farther than h from p — they cannot be accepted, so the accepted set and its order are
+// unchanged. Used when the grid's bins are at least 2h (the reference's cell budget
+// doubled them), where a particle reaches only about a quarter of the 27 cells' slots.
+template <class F>
+__device__ __forceinline__ void walk27_half(const GridBox& g, const uint32_t* __restrict__ start,
+                                            const uint32_t* __restrict__ halves, float px, float py, float pz,
+                                            uint32_t cx, uint32_t cy, uint32_t cz, float h, F&& f) {
+  const float B = g.bin;
+  const float lx = g.minx + (float)cx * B, ly = g.miny + (float)cy * B, lz = g.minz + (float)cz * B;
+  const float gxl = fmaxf(px - lx, 0.0f), gxr = fmaxf(lx + B - px, 0.0f);
+  const float gyl = fmaxf(py - ly, 0.0f), gyr = fmaxf(ly + B - py, 0.0f);
+  const float gzl = fmaxf(pz - lz, 0.0f), gzr = fmaxf(lz + B - pz, 0.0f);
+  const float reach = h + B * (1.0f / 1024.0f);
+  const float reach2 = reach * reach;
+  const uint32_t bxs = half_reach_bits(px, lx, B, reach);
+  const uint32_t bys = half_reach_bits(py, ly, B, reach);
+  const uint32_t bzs = half_reach_bits(pz, lz, B, reach);
+  for (int dz = -1; dz <= 1; ++dz) {
+    const int z = (int)cz + dz;
+    if (z < 0 || z >= (int)g.nz) continue;
+    const float gz = dz < 0 ? gzl : (dz > 0 ? gzr : 0.0f);
+    const float dz2 = gz * gz;
+    const uint32_t zsel = (bzs >> (2 * (dz + 1))) & 3u;
+    for (int dy = -1; dy <= 1; ++dy) {
+      const int y = (int)cy + dy;
+      if (y < 0 || y >= (int)g.ny) continue;
+      const float gy = dy < 0 ? gyl : (dy > 0 ? gyr : 0.0f);
+      const float dyz2 = dz2 + gy * gy;
+      const uint32_t ysel = (bys >> (2 * (dy + 1))) & 3u;
+      for (int dx = -1; dx <= 1; ++dx) {
+        const int x = (int)cx + dx;
+        if (x < 0 || x >= (int)g.nx) continue;
+        const float gx = dx < 0 ? gxl : (dx > 0 ? gxr : 0.0f);
+        if (dyz2 + gx * gx > reach2) continue;
+        const uint32_t xsel = (bxs >> (2 * (dx + 1))) & 3u;
+        if (!xsel || !ysel || !zsel) continue;
+        const uint32_t idx = ((uint32_t)x * g.ny + (uint32_t)y) * g.nz + (uint32_t)z;
+        const uint32_t j0 = start[idx], j1 = start[idx + 1];
+#if VXL_HALF_FULL_RANGE
+        if ((xsel & ysel & zsel) == 3u) {
+          for (uint32_t j = j0; j < j1; ++j) f(j);
+          continue;
+        }
+#endif
+        for (uint32_t base = j0 & ~31u; base < j1; base += 32) {
+          const uint4 hm = *reinterpret_cast<const uint4*>(halves + 4 * (base >> 5));
+          uint32_t m = half_select(xsel, hm.x) & half_select(ysel, hm.y) & half_select(zsel, hm.z);
+          if (j0 > base) m &= ~0u << (j0 - base);
+          if (j1 < base + 32) m &= (1u << (j1 - base)) - 1u;
+          while (m) {
+            const uint32_t j = base + (uint32_t)(__ffs(m) - 1);
+            m &= m - 1u;
+            f(j);
+          }
+        }
+      }
+    }
+  }
+}
+
 // Density (poly6 with self term) + Tait EOS, persistent over tiles, one thread per slot.
 // Fluid: rho = mass * (w0 + sum_fluid W) + sum_boundary pmass_j W
 // (crates/vxl-phys-fluid/src/fluid_density.rs:24-51); boundary: rho = pmass_i w0 +
@@ -598,9 +731,9 @@ __device__ __forceinline__ void walk27(const GridBox& g, const uint32_t* __restr
 template <int kBlock>
 __global__ void __launch_bounds__(kBlock, VXL_DENSITY_THREADS_PER_SM / kBlock) k_e_density(
     const float4* __restrict__ pos, const uint32_t* __restrict__ start, const SceneDev* __restrict__ sc,
-    const TileDev* __restrict__ tiles, uint32_t ntiles, EngineCtl* ctl, float2* __restrict__ rc,
-    float* __restrict__ press_out, uint32_t* __restrict__ nbr, uint32_t* __restrict__ nbr_n, uint32_t cap,
-    uint32_t stride) {
+    const TileDev* __restrict__ tiles, uint32_t ntiles, EngineCtl* ctl, const uint32_t* __restrict__ halves,
+    float2* __restrict__ rc, float* __restrict__ press_out, uint32_t* __restrict__ nbr,
+    uint32_t* __restrict__ nbr_n, uint32_t cap, uint32_t stride) {
   if (ctl->err & kErrCellCap) return;
   for (uint32_t t = first_tile(&ctl->work[kWorkDensity], ntiles); t < ntiles; t = following_tile(&ctl->work[kWorkDensity], ntiles)) {
     const TileDev td = tiles[t];
@@ -609,6 +742,7 @@ __global__ void __launch_bounds__(kBlock, VXL_DENSITY_THREADS_PER_SM / kBlock) k
     const SphConst& k = S.k;
     const uint32_t* cst = start + S.cell_off;
     const float h = k.h, h2 = k.h2, k6 = k.k6, w0 = k.w0, mass = k.mass;
+    const bool half_walk = halves != nullptr && g.bin >= 2.0f * h;  // uniform over the tile
     for (uint32_t i = threadIdx.x; i < td.count; i += kBlock) {
       const uint32_t s = td.first + i;
       const float4 pi = pos[s];
@@ -618,7 +752,7 @@ __global__ void __launch_bounds__(kBlock, VXL_DENSITY_THREADS_PER_SM / kBlock) k
       float sum = fluid_i ? w0 : 0.0f;
       float sum_b = 0.0f;
       uint32_t cnt = 0;
-      walk27(g, cst, pi.x, pi.y, pi.z, cx, cy, cz, h, [&](uint32_t j) {
+      auto visit = [&](uint32_t j) {
         if (j == s) return;
         const float4 pj = pos[j];
         const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
@@ -640,7 +774,11 @@ __global__ void __launch_bounds__(kBlock, VXL_DENSITY_THREADS_PER_SM / kBlock) k
             ++cnt;
           }
         }
-      });
+      };
+      if (half_walk)
+        walk27_half(g, cst, halves, pi.x, pi.y, pi.z, cx, cy, cz, h, visit);
+      else
+        walk27(g, cst, pi.x, pi.y, pi.z, cx, cy, cz, h, visit);
       nbr_n[s] = cnt;
       const float rho = fluid_i ? (mass * sum + sum_b) : ((-pi.w) * w0 + sum);
       const float p = tait(k, rho);

@@ -143,6 +143,7 @@ class Engine {
   void* bpos_ = nullptr;
   uint32_t* nbr_ = nullptr;
   uint32_t* nbr_n_ = nullptr;
+  uint32_t* halves_ = nullptr;  // 4 words per 32 slots: upper-half masks along x, y, z
   float* stage_ = nullptr;  // 8 floats per slot: staging for host transfers
   // cells (cell_cap_ + 1)
   uint32_t* counts_ = nullptr;

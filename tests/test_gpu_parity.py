@@ -368,3 +368,15 @@ def test_dam1_table_properties_and_determinism(vxl):
     assert np.all(items[1:][same] > items[:-1][same]), "cell contents must ascend by particle index"
     p, v = g.read_state()
     assert np.isfinite(p).all() and np.isfinite(v).all()
+
+
+def test_doubled_bins_many_per_cell(vxl, oracle_mod):
+    """A cell budget that forces bins of 4h with ~500 particles per cell: the density pass
+    culls half-cells out of reach and must still accept the same neighbours in the same
+    order (table, fields and state bit for bit over six substeps)."""
+    from vxl_sph import scenes
+    s = 0.01
+    fluid = scenes.fluid_block((0.0, 0.0, 0.0), (20, 16, 18), s)
+    b = scenes.body_particles([scenes.Body(0, (0.12, 0.01, 0.11), (0.1, -0.01, 0.09))], s, 2 * s, 1, 1000.0)
+    spec = _custom(vxl, fluid, h=2 * s, spacing=s, boundary=b, max_bins=64)
+    _run_both(vxl, oracle_mod, spec, substeps=6)
