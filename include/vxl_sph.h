@@ -276,6 +276,31 @@ vxl_status vxl_sph_get_tuning(vxl_sph_handle* h, vxl_sph_tuning* t);
  * Results are identical for every shape; only the time differs. */
 vxl_status vxl_sph_autotune(vxl_sph_handle* h, float dt_tick, uint32_t trials, vxl_sph_tuning* best);
 
+/* ------------------------------------------------------------------ moving bodies on the device
+ * The reference rebuilds the boundary segment on the host every tick from the bodies'
+ * poses (set_boundary_particles, crates/vxl-phys-fluid/src/fluid_step.rs:13-53) and the GPU
+ * tier uploads it (crates/vxl-phys-gpu/src/pipeline/coupling.rs:20-50). With the body-frame
+ * lattice resident on the device, a tick needs only the poses: each boundary particle k of
+ * body b becomes p = pos_b + rotate(rot_b, L_k), v = linvel_b + angvel_b x (p - pos_b), with
+ * the reference's f32 operation order, bit for bit what vxl_sph_upload_boundary would be
+ * given. pmass (the lattice volume) is unchanged. */
+typedef struct vxl_sph_body_pose {
+  uint32_t body;       /* body id (informational) */
+  float pos[3];        /* body origin (the lattice's frame) */
+  float rot[4];        /* unit quaternion x, y, z, w */
+  float linvel[3];
+  float angvel[3];
+} vxl_sph_body_pose;
+
+/* local_xyz[3 k..3 k+3): boundary particle k's lattice point in its body's frame;
+ * body_index[k] < nbodies: its body's position in the pose array. nb must equal the
+ * scene's boundary count. Plain handles use scene 0. */
+vxl_status vxl_sph_set_body_lattice(vxl_sph_handle* h, uint32_t scene, const float* local_xyz,
+                                    const uint32_t* body_index, uint64_t nb, uint32_t nbodies);
+/* Rebuild the scene's boundary segment from `nbodies` poses (same count as the lattice). */
+vxl_status vxl_sph_set_body_poses(vxl_sph_handle* h, uint32_t scene, const vxl_sph_body_pose* poses,
+                                  uint32_t nbodies);
+
 /* ------------------------------------------------------------------ served form
  * A request loop (the served workload): scene-step requests are submitted at any time,
  * admitted while their device footprint fits an HBM budget, stepped together with

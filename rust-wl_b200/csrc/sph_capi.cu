@@ -163,6 +163,26 @@ vxl_status vxl_sph_upload_boundary_scene(vxl_sph_handle* h, uint32_t scene, cons
   return h->e->upload_boundary(scene, pos_xyz, vel_xyz, nb);
 }
 
+vxl_status vxl_sph_set_body_lattice(vxl_sph_handle* h, uint32_t scene, const float* local_xyz,
+                                    const uint32_t* body_index, uint64_t nb, uint32_t nbodies) {
+  HANDLE_OR_FAIL(h);
+  try {
+    return h->e->set_body_lattice(scene, local_xyz, body_index, nb, nbodies);
+  } catch (...) {
+    return set_error(VXL_PANIC_CAUGHT, "exception in vxl_sph_set_body_lattice");
+  }
+}
+
+vxl_status vxl_sph_set_body_poses(vxl_sph_handle* h, uint32_t scene, const vxl_sph_body_pose* poses,
+                                  uint32_t nbodies) {
+  HANDLE_OR_FAIL(h);
+  try {
+    return h->e->set_body_poses(scene, poses, nbodies);
+  } catch (...) {
+    return set_error(VXL_PANIC_CAUGHT, "exception in vxl_sph_set_body_poses");
+  }
+}
+
 vxl_status vxl_sph_set_spans_scene(vxl_sph_handle* h, uint32_t scene, const vxl_sph_span* spans, uint32_t nspans) {
   HANDLE_OR_FAIL(h);
   return h->e->set_spans(scene, spans, nspans);

@@ -200,6 +200,10 @@ void Engine::free_all() {
   void* hp[] = {sc_h_, ctl_h_, spans_h_, chunks_h_, chunk_first_h_, breact_h_};
   for (void* p : hp)
     if (p) cudaFreeHost(p);
+  if (blocal_) cudaFree(blocal_);
+  if (poses_d_) cudaFree(poses_d_);
+  blocal_ = nullptr;
+  poses_d_ = nullptr;
   for (cudaEvent_t e : prof_ev_) cudaEventDestroy(e);
   prof_ev_.clear();
   if (own_stream_) cudaStreamDestroy(own_stream_);
@@ -361,6 +365,7 @@ vxl_status Engine::add_scene(const vxl_sph_params& p, uint64_t nf, uint64_t nb, 
   if (s == VXL_OK) s = recompute_scene_boxes(q);
   if (s == VXL_OK) s = rebuild_tiles();
   spans_local_.resize(scenes_.size());
+  scene_bodies_.resize(scenes_.size(), 0);
   spans_dirty_ = true;
   if (out_index) *out_index = q;
   return s;
@@ -376,6 +381,7 @@ vxl_status Engine::remove_scenes(const std::vector<uint32_t>& indices) {
     if (i < scenes_.size()) drop[i] = true;
   std::vector<SceneInfo> keep;
   std::vector<std::vector<vxl_sph_span>> keep_spans;
+  std::vector<uint32_t> keep_bodies;
   std::vector<uint4> moves;
   uint32_t next = 0;
   for (uint32_t q = 0; q < scenes_.size(); ++q) {
@@ -387,6 +393,7 @@ vxl_status Engine::remove_scenes(const std::vector<uint32_t>& indices) {
     next += n;
     keep.push_back(si);
     keep_spans.push_back(q < spans_local_.size() ? spans_local_[q] : std::vector<vxl_sph_span>());
+    keep_bodies.push_back(q < scene_bodies_.size() ? scene_bodies_[q] : 0u);
   }
   // copy every kept scene into the second buffer set at its new base, then back
   if (!moves.empty() && next > 0) {
@@ -405,11 +412,18 @@ vxl_status Engine::remove_scenes(const std::vector<uint32_t>& indices) {
     CU(cudaMemcpyAsync(vel_[0], vel_[1], (size_t)next * 16, cudaMemcpyDeviceToDevice, stream_));
     CU(cudaMemcpyAsync(orig_, orig_tmp, (size_t)next * 4, cudaMemcpyDeviceToDevice, stream_));
     CU(cudaMemcpyAsync(bpos_, bpos_tmp, (size_t)next * 16, cudaMemcpyDeviceToDevice, stream_));
+    if (blocal_) {  // body lattices move with their scenes (reference order, like bpos)
+      float4* tmp = (float4*)xsph_;
+      for (auto& m : moves)
+        if (m.z) CU(cudaMemcpyAsync(tmp + m.y, blocal_ + m.x, (size_t)m.z * 16, cudaMemcpyDeviceToDevice, stream_));
+      CU(cudaMemcpyAsync(blocal_, tmp, (size_t)next * 16, cudaMemcpyDeviceToDevice, stream_));
+    }
     k_e_slot_of<<<blocks_for(next), kThreads, 0, stream_>>>(orig_, slot_of_, next);
     CU(cudaGetLastError());
   }
   scenes_.swap(keep);
   spans_local_.swap(keep_spans);
+  scene_bodies_.swap(keep_bodies);
   used_ = next;
   spans_dirty_ = true;
   vxl_status s = push_scene_records({});
@@ -434,6 +448,70 @@ vxl_status Engine::upload_boundary(uint32_t q, const float* pos, const float* ve
                                                                  sc_d_[q].bbox, si.base, si.nf, si.nb);
   CU(cudaGetLastError());
   CU(cudaStreamSynchronize(stream_));  // the caller's arrays are borrowed for this call only
+  return VXL_OK;
+}
+
+vxl_status Engine::set_body_lattice(uint32_t q, const float* local_xyz, const uint32_t* body_index, uint64_t nb,
+                                    uint32_t nbodies) {
+  if (q >= scenes_.size()) return set_error(VXL_INVALID_ARGUMENT, "scene index out of range");
+  const SceneInfo& si = scenes_[q];
+  if (nb != si.nb) return set_error(VXL_SIZE_MISMATCH, "lattice length differs from the boundary segment");
+  if (nb == 0) return VXL_OK;
+  if (!local_xyz || !body_index) return set_error(VXL_NULL_POINTER, "lattice arrays are NULL");
+  if (nbodies == 0) return set_error(VXL_INVALID_ARGUMENT, "nbodies must be > 0");
+  for (uint64_t k = 0; k < nb; ++k)
+    if (body_index[k] >= nbodies) return set_error(VXL_INVALID_ARGUMENT, "body index past nbodies");
+  CU(cudaSetDevice(device_));
+  if (!blocal_) {
+    vxl_status st = dalloc(&blocal_, slot_cap_);
+    if (st != VXL_OK) return st;
+  }
+  std::vector<float4> h(nb);
+  for (uint64_t k = 0; k < nb; ++k) {
+    uint32_t b = body_index[k];
+    float w;
+    std::memcpy(&w, &b, 4);
+    h[k] = make_float4(local_xyz[3 * k], local_xyz[3 * k + 1], local_xyz[3 * k + 2], w);
+  }
+  CU(cudaMemcpyAsync(blocal_ + si.base + si.nf, h.data(), nb * sizeof(float4), cudaMemcpyHostToDevice, stream_));
+  CU(cudaStreamSynchronize(stream_));
+  if (scene_bodies_.size() < scenes_.size()) scene_bodies_.resize(scenes_.size(), 0);
+  scene_bodies_[q] = nbodies;
+  return VXL_OK;
+}
+
+vxl_status Engine::set_body_poses(uint32_t q, const vxl_sph_body_pose* poses, uint32_t nbodies) {
+  if (q >= scenes_.size()) return set_error(VXL_INVALID_ARGUMENT, "scene index out of range");
+  if (q >= scene_bodies_.size() || scene_bodies_[q] == 0)
+    return set_error(VXL_NOT_READY, "no body lattice set for this scene");
+  if (nbodies != scene_bodies_[q]) return set_error(VXL_SIZE_MISMATCH, "pose count differs from the lattice's bodies");
+  if (!poses) return set_error(VXL_NULL_POINTER, "poses is NULL");
+  const SceneInfo& si = scenes_[q];
+  CU(cudaSetDevice(device_));
+  prof_collect();
+  CU(cudaStreamSynchronize(stream_));
+  if (nbodies > poses_cap_) {
+    if (poses_d_) cudaFree(poses_d_);
+    poses_d_ = nullptr;
+    poses_cap_ = 0;
+    vxl_status st = dalloc(&poses_d_, nbodies);
+    if (st != VXL_OK) return st;
+    poses_cap_ = nbodies;
+  }
+  std::vector<BodyPoseDev> h(nbodies);
+  for (uint32_t b = 0; b < nbodies; ++b) {
+    const vxl_sph_body_pose& p = poses[b];
+    h[b] = BodyPoseDev{p.pos[0], p.pos[1], p.pos[2], p.rot[0], p.rot[1], p.rot[2], p.rot[3],
+                       p.linvel[0], p.linvel[1], p.linvel[2], p.angvel[0], p.angvel[1], p.angvel[2]};
+  }
+  static const uint32_t init[6] = {0xffffffffu, 0xffffffffu, 0xffffffffu, 0u, 0u, 0u};
+  CU(cudaMemcpyAsync(poses_d_, h.data(), nbodies * sizeof(BodyPoseDev), cudaMemcpyHostToDevice, stream_));
+  CU(cudaMemcpyAsync(sc_d_[q].bbox, init, sizeof(init), cudaMemcpyHostToDevice, stream_));
+  k_e_body_rebuild<<<blocks_for(si.nb), kThreads, 0, stream_>>>(blocal_, poses_d_, (float4*)pos_[0],
+                                                                 (float4*)vel_[0], slot_of_, (float4*)bpos_,
+                                                                 sc_d_[q].bbox, si.base, si.nf, si.nb);
+  CU(cudaGetLastError());
+  CU(cudaStreamSynchronize(stream_));  // the caller's poses are borrowed for this call only
   return VXL_OK;
 }
 

@@ -63,6 +63,14 @@ struct SceneDev {
   uint32_t bbox[6];     // boundary AABB (fixed within a tick)
 };
 
+// Per-body pose of the device-side boundary rebuild.
+struct BodyPoseDev {
+  float px, py, pz;
+  float qx, qy, qz, qw;
+  float vx, vy, vz;
+  float wx, wy, wz;
+};
+
 struct TileDev {
   uint32_t scene, first, count, pad;
 };
@@ -257,6 +265,58 @@ __global__ void k_e_bbox(const float4* __restrict__ pos, uint32_t base, uint32_t
 // Move whole scenes to new bases (the served form's repack): slot ranges are copied into
 // the second buffer set, reference indices shifted by the move. from_base/to_base/count
 // per moved scene; one block row per scene (blockIdx.y).
+
+// set_boundary_particles on the device (crates/vxl-phys-fluid/src/fluid_step.rs:13-53): for
+// boundary particle k of a scene (reference order), with body-frame lattice point L and
+// its body's pose, world position p = body.pos + rotate(q, L) (Quat::rotate_vec3:
+// t = 2 (q.xyz x L); L + q.xyz x t + w t) and velocity v = linvel + angvel x (p - body.pos),
+// in f32 in the reference's operation order. Written at the particle's current slot and in
+// reference order (bpos); the boundary AABB is re-accumulated. The class/mass word is kept.
+__device__ __forceinline__ void cross3(float ax, float ay, float az, float bx, float by, float bz, float& cx,
+                                       float& cy, float& cz) {
+  cx = ay * bz - az * by;
+  cy = az * bx - ax * bz;
+  cz = ax * by - ay * bx;
+}
+
+__global__ void k_e_body_rebuild(const float4* __restrict__ blocal, const BodyPoseDev* __restrict__ poses,
+                                 float4* __restrict__ pos, float4* __restrict__ vel,
+                                 const uint32_t* __restrict__ slot_of, float4* __restrict__ bpos,
+                                 uint32_t* __restrict__ bbox_acc, uint32_t base, uint32_t nf, uint32_t nb) {
+  const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool valid = q < nb;
+  float x = 0, y = 0, z = 0;
+  if (valid) {
+    const uint32_t g = base + nf + q;
+    const float4 L = blocal[g];
+    const BodyPoseDev P = poses[__float_as_uint(L.w)];
+    float tx, ty, tz;
+    cross3(P.qx, P.qy, P.qz, L.x, L.y, L.z, tx, ty, tz);
+    tx = tx * 2.0f;
+    ty = ty * 2.0f;
+    tz = tz * 2.0f;
+    float ux, uy, uz;
+    cross3(P.qx, P.qy, P.qz, tx, ty, tz, ux, uy, uz);
+    const float rx = (L.x + ux) + tx * P.qw;
+    const float ry = (L.y + uy) + ty * P.qw;
+    const float rz = (L.z + uz) + tz * P.qw;
+    x = P.px + rx;
+    y = P.py + ry;
+    z = P.pz + rz;
+    float ax, ay, az;
+    cross3(P.wx, P.wy, P.wz, x - P.px, y - P.py, z - P.pz, ax, ay, az);
+    const uint32_t s = slot_of[g];
+    float4 p = pos[s];
+    p.x = x;
+    p.y = y;
+    p.z = z;
+    pos[s] = p;
+    vel[s] = make_float4(P.vx + ax, P.vy + ay, P.vz + az, 0.0f);
+    bpos[g] = make_float4(x, y, z, 0.0f);
+  }
+  block_bbox_accumulate(bbox_acc, x, y, z, valid);
+}
+
 __global__ void k_e_move(const float4* __restrict__ pos_in, const float4* __restrict__ vel_in,
                          const uint32_t* __restrict__ orig_in, const float4* __restrict__ bpos_in,
                          float4* __restrict__ pos_out, float4* __restrict__ vel_out, uint32_t* __restrict__ orig_out,

@@ -21,6 +21,7 @@ struct TileDev;
 struct EngineCtl;
 struct SpanDev;
 struct SpanChunk;
+struct BodyPoseDev;
 
 // Launch shape of the particle passes (chosen by the autotuner for batches).
 struct Tuning {
@@ -65,6 +66,11 @@ class Engine {
   vxl_status remove_scenes(const std::vector<uint32_t>& indices);
 
   vxl_status upload_boundary(uint32_t scene, const float* pos, const float* vel, uint64_t nb);
+  // Device-side boundary rebuild: the body-frame lattice point and body index of every
+  // boundary particle (reference order), then per tick only the bodies' poses.
+  vxl_status set_body_lattice(uint32_t scene, const float* local_xyz, const uint32_t* body_index, uint64_t nb,
+                              uint32_t nbodies);
+  vxl_status set_body_poses(uint32_t scene, const vxl_sph_body_pose* poses, uint32_t nbodies);
   vxl_status write_state(uint32_t scene, const float* pos, const float* vel);
   vxl_status read_state(uint32_t scene, float* pos, float* vel);
   vxl_status read_fields(uint32_t scene, float* dens, float* press, float* acc, float* xsph, float* bforce);
@@ -127,6 +133,7 @@ class Engine {
   uint32_t scene_cap_ = 0, nbr_cap_ = 64;
   uint64_t device_bytes_ = 0;
   std::vector<SceneInfo> scenes_;
+  std::vector<uint32_t> scene_bodies_;  // bodies of each scene's lattice (0: none set)
 
   // pool (slot_cap_)
   void* pos_[2] = {nullptr, nullptr};
@@ -143,7 +150,10 @@ class Engine {
   void* bpos_ = nullptr;
   uint32_t* nbr_ = nullptr;
   uint32_t* nbr_n_ = nullptr;
-  uint32_t* halves_ = nullptr;  // 4 words per 32 slots: upper-half masks along x, y, z
+  uint32_t* halves_ = nullptr;
+  float4* blocal_ = nullptr;         // body-frame lattice per boundary slot (reference order), lazily
+  BodyPoseDev* poses_d_ = nullptr;   // poses of one scene's bodies (staged per call)
+  uint32_t poses_cap_ = 0;  // 4 words per 32 slots: upper-half masks along x, y, z
   float* stage_ = nullptr;  // 8 floats per slot: staging for host transfers
   // cells (cell_cap_ + 1)
   uint32_t* counts_ = nullptr;

@@ -118,6 +118,25 @@ class ServeReport(C.Structure):
                 ("retired", C.c_uint32), ("particles", C.c_uint64), ("device_bytes_in_use", C.c_uint64)]
 
 
+class BodyPose(C.Structure):
+    _fields_ = [("body", C.c_uint32), ("pos", C.c_float * 3), ("rot", C.c_float * 4), ("linvel", C.c_float * 3),
+                ("angvel", C.c_float * 3)]
+
+
+def poses_array(bodies):
+    """BodyPose array from objects with id, pos, rot, linvel, angvel (e.g. scenes.Body)."""
+    arr = (BodyPose * max(len(bodies), 1))()
+    for q, b in enumerate(bodies):
+        arr[q].body = b.id
+        for a in range(3):
+            arr[q].pos[a] = b.pos[a]
+            arr[q].linvel[a] = b.linvel[a]
+            arr[q].angvel[a] = b.angvel[a]
+        for a in range(4):
+            arr[q].rot[a] = b.rot[a]
+    return arr, len(bodies)
+
+
 def header(struct_type) -> BlockHeader:
     return BlockHeader(C.sizeof(struct_type), ABI_VERSION)
 
@@ -166,6 +185,8 @@ SIGNATURES = {
     "vxl_sph_set_tuning": (C.c_int, [_H, C.POINTER(Tuning)]),
     "vxl_sph_get_tuning": (C.c_int, [_H, C.POINTER(Tuning)]),
     "vxl_sph_autotune": (C.c_int, [_H, C.c_float, C.c_uint32, C.POINTER(Tuning)]),
+    "vxl_sph_set_body_lattice": (C.c_int, [_H, C.c_uint32, _FP, C.POINTER(C.c_uint32), C.c_uint64, C.c_uint32]),
+    "vxl_sph_set_body_poses": (C.c_int, [_H, C.c_uint32, C.POINTER(BodyPose), C.c_uint32]),
     "vxl_sph_serve_create": (C.c_int, [C.c_int32, C.c_uint64, C.c_uint32, C.POINTER(C.c_void_p)]),
     "vxl_sph_serve_destroy": (C.c_int, [C.c_void_p]),
     "vxl_sph_serve_submit": (C.c_int, [C.c_void_p, C.POINTER(Desc), C.c_uint32, C.POINTER(C.c_uint64)]),
@@ -346,6 +367,17 @@ class Scene:
         pos = np.ascontiguousarray(pos, dtype=np.float32).reshape(-1, 3)
         vel = np.ascontiguousarray(vel, dtype=np.float32).reshape(-1, 3)
         _check(self.lib.vxl_sph_upload_boundary(self._h, self.n_fluid, _fptr(pos), _fptr(vel), pos.shape[0]))
+
+    def set_body_lattice(self, local_xyz: np.ndarray, body_index: np.ndarray, nbodies: int, scene: int = 0) -> None:
+        """Body-frame lattice of the boundary segment (see scenes.body_lattice)."""
+        lx = np.ascontiguousarray(local_xyz, dtype=np.float32).reshape(-1, 3)
+        bi = np.ascontiguousarray(body_index, dtype=np.uint32).reshape(-1)
+        _check(self.lib.vxl_sph_set_body_lattice(self._h, scene, _fptr(lx), _u32ptr(bi), lx.shape[0], nbodies))
+
+    def set_body_poses(self, bodies, scene: int = 0) -> None:
+        """Rebuild the boundary segment on the device from the bodies' poses."""
+        arr, n = poses_array(bodies)
+        _check(self.lib.vxl_sph_set_body_poses(self._h, scene, arr, n))
 
     def read_state(self, out=None) -> tuple[np.ndarray, np.ndarray]:
         """Positions and velocities in reference order; `out=(pos, vel)` reuses caller

@@ -120,6 +120,26 @@ def body_particles(bodies, spacing: float, h: float, layers: int, rest_density: 
     return np.concatenate(ps), np.concatenate(vs), np.concatenate(ms), spans
 
 
+def body_lattice(bodies, spacing: float, h: float, layers: int, cache=None):
+    """The body-frame side of body_particles: (local points, body index into `bodies`) of
+    the boundary segment in the same body-major order, for the device-side rebuild
+    (vxl_sph_set_body_lattice + vxl_sph_set_body_poses)."""
+    cache = {} if cache is None else cache
+    pts, idx = [], []
+    for q, b in enumerate(bodies):
+        key = tuple(np.asarray(b.half, F).tolist())
+        if key not in cache:
+            cache[key] = boundary_lattice(0, key, 0.0, spacing, h, layers)
+        lat, _ = cache[key]
+        if lat.shape[0] == 0:
+            continue
+        pts.append(lat)
+        idx.append(np.full(lat.shape[0], q, np.uint32))
+    if not pts:
+        return np.zeros((0, 3), F), np.zeros(0, np.uint32)
+    return np.concatenate(pts).astype(F), np.concatenate(idx)
+
+
 def tank_bodies(inner, t: float, first_id: int = 0) -> list:
     """Floor + four walls (static boxes) around the open box [0, inner]; thickness t
     (the reference's --tank pattern, gpu_tick_probe.rs:20-63, with the tank's own size)."""

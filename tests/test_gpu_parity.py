@@ -380,3 +380,52 @@ def test_doubled_bins_many_per_cell(vxl, oracle_mod):
     b = scenes.body_particles([scenes.Body(0, (0.12, 0.01, 0.11), (0.1, -0.01, 0.09))], s, 2 * s, 1, 1000.0)
     spec = _custom(vxl, fluid, h=2 * s, spacing=s, boundary=b, max_bins=64)
     _run_both(vxl, oracle_mod, spec, substeps=6)
+
+
+def test_device_body_rebuild_equals_host_upload(vxl, oracle_mod):
+    """Moving and rotating bodies: rebuilding the boundary segment on the device from the
+    poses (vxl_sph_set_body_poses) gives, tick after tick, exactly the state and reactions
+    of uploading the host-built segment (vxl_sph_upload_boundary) and of the oracle's
+    set_boundary_particles."""
+    from vxl_sph import scenes
+    s = 0.02
+    h = 2 * s
+    tank = (0.6, 0.5, 0.4)
+    walls = scenes.tank_bodies(tank, 2 * s)
+    paddle = scenes.Body(9, (0.02, 0.12, 0.08), (0.42, 0.16, 0.2), rot=(0.0, 0.0, 0.0, 1.0),
+                         linvel=(-0.3, 0.0, 0.05), angvel=(0.0, 1.5, 0.4))
+    bodies = walls + [paddle]
+    params = scenes.baseline_params(s, substeps=4)
+    fluid = scenes.jitter(scenes.fluid_block((0.0, 0.0, 0.0), (10, 12, 10), s), s, 17)
+    spec = scenes.assemble("paddle", params, fluid, bodies, s, 4)
+    a = vxl.Scene(spec.params, spec.pos, spec.vel, spec.pmass, spec.n_fluid)
+    b = vxl.Scene(spec.params, spec.pos, spec.vel, spec.pmass, spec.n_fluid)
+    o = oracle_mod.OracleSystem.from_scene(spec, threads=4)
+    local, idx = scenes.body_lattice(bodies, s, h, params.boundary_layers)
+    b.set_body_lattice(local, idx, len(bodies))
+    dt = float(np.float32(1.0) / np.float32(60.0))
+    for t in range(4):
+        # advance the paddle's pose on the host (the caller's rigid integrator)
+        p = np.asarray(paddle.pos, F32) + np.asarray(paddle.linvel, F32) * F32(dt)
+        ang = F32(0.05 * (t + 1))
+        q = (0.0, float(np.sin(ang)), 0.0, float(np.cos(ang)))
+        paddle = scenes.Body(9, paddle.half, tuple(float(x) for x in p), rot=q, linvel=paddle.linvel,
+                             angvel=paddle.angvel)
+        bodies = walls + [paddle]
+        bpos, bvel, _, bsp = scenes.body_particles(bodies, s, h, params.boundary_layers, params.rest_density)
+        spans = [(bb, org, st + spec.n_fluid, en + spec.n_fluid) for bb, org, st, en in bsp]
+        a.upload_boundary(bpos, bvel)
+        b.set_body_poses(bodies)
+        o.set_bodies(bodies)
+        ra = a.step_tick(dt, spans)
+        rb = b.step_tick(dt, spans)
+        o.step(dt)
+        for (b1, f1, t1), (b2, f2, t2) in zip(ra, rb):
+            assert b1 == b2 and f1.tobytes() == f2.tobytes() and t1.tobytes() == t2.tobytes()
+        pa, va = a.read_state()
+        pb, vb = b.read_state()
+        assert_bits(pb, pa, f"tick {t} pos (device rebuild vs upload)")
+        assert_bits(vb, va, f"tick {t} vel (device rebuild vs upload)")
+        r = o.read_f32()
+        assert_bits(pb, r["pos"], f"tick {t} pos vs oracle")
+    o.close()

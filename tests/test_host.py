@@ -42,13 +42,13 @@ def test_struct_sizes_match_header(vxl, tmp_path):
         '#include <stdio.h>\n#include "vxl_sph.h"\nint main(void){printf("%zu %zu %zu %zu %zu %zu %zu\\n",'
         "sizeof(vxl_sph_params),sizeof(vxl_sph_desc),sizeof(vxl_sph_span),sizeof(vxl_sph_reaction),"
         "sizeof(vxl_sph_grid_info),sizeof(vxl_sph_stats),sizeof(vxl_block_header));"
-        'printf("%zu %zu %zu\\n",sizeof(vxl_sph_tuning),sizeof(vxl_sph_request_status),sizeof(vxl_sph_serve_report));'
+        'printf("%zu %zu %zu %zu\\n",sizeof(vxl_sph_tuning),sizeof(vxl_sph_request_status),sizeof(vxl_sph_serve_report),sizeof(vxl_sph_body_pose));'
         "return 0;}\n")
     exe = tmp_path / "sizes"
     subprocess.run(["gcc", "-std=c99", "-I", str(ROOT / "include"), str(src), "-o", str(exe)], check=True)
     got = [int(x) for x in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
     want = [C.sizeof(t) for t in (vxl.Params, vxl.Desc, vxl.Span, vxl.Reaction, vxl.GridInfo, vxl.Stats,
-                                  vxl.BlockHeader, vxl.Tuning, vxl.RequestStatus, vxl.ServeReport)]
+                                  vxl.BlockHeader, vxl.Tuning, vxl.RequestStatus, vxl.ServeReport, vxl.BodyPose)]
     assert got == want
 
 
@@ -173,3 +173,24 @@ def test_scene_sizes(vxl):
     dj = np.abs(s0.pos[:s0.n_fluid] - lat)
     assert dj.max() <= 0.01 * 0.02 * 1.0001 and dj.max() > 0
     assert scenes.dam0().pos.tobytes() == s0.pos.tobytes()
+
+
+def test_body_lattice_matches_body_particles(vxl):
+    """scenes.body_lattice + the pose transform restate body_particles exactly (the inputs
+    of the device-side rebuild describe the same boundary segment)."""
+    from vxl_sph import scenes
+    bodies = [scenes.Body(3, (0.05, 0.07, 0.04), (0.2, 0.3, 0.1), rot=(0.0, 0.38268343, 0.0, 0.9238795),
+                          linvel=(0.5, -0.2, 0.1), angvel=(0.3, 1.2, -0.7)),
+              scenes.Body(7, (0.03, 0.03, 0.06), (-0.1, 0.2, 0.05), rot=(0.1, 0.2, 0.3, 0.9273618))]
+    pos, vel, _, _ = scenes.body_particles(bodies, 0.01, 0.02, 1, 1000.0)
+    local, idx = scenes.body_lattice(bodies, 0.01, 0.02, 1)
+    assert local.shape == pos.shape and idx.shape == (pos.shape[0],)
+    F = np.float32
+    for q, b in enumerate(bodies):
+        sel = idx == q
+        bp = np.asarray(b.pos, F)
+        wp = (bp + scenes.rotate(b.rot, local[sel])).astype(F)
+        assert wp.tobytes() == pos[sel].tobytes()
+        r = (wp - bp).astype(F)
+        wv = (np.asarray(b.linvel, F) + scenes._cross(np.broadcast_to(np.asarray(b.angvel, F), r.shape), r)).astype(F)
+        assert wv.tobytes() == vel[sel].tobytes()
