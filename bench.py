@@ -291,11 +291,15 @@ def run_ours(args) -> None:
     pin_p = torch.empty((spec.n_total, 3), dtype=torch.float32, pin_memory=True).numpy()
     pin_v = torch.empty((spec.n_total, 3), dtype=torch.float32, pin_memory=True).numpy()
     scene.set_profile(False)
-    scene.read_state(out=(pin_p, pin_v))
+    pin_p[:] = spec.pos
+    pin_v[:] = spec.vel
     for _ in range(2):
         scene.write_state(pin_p, pin_v)
         scene.step_tick(dt_tick, spec.spans)
         scene.read_state(out=(pin_p, pin_v))
+    # the timed steps start from the initial state too (the device-timed ticks' states)
+    pin_p[:] = spec.pos
+    pin_v[:] = spec.vel
     torch.cuda.synchronize()
     if dist:
         dist.barrier()

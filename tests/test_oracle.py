@@ -311,3 +311,37 @@ def test_configured_constants_are_acoustically_unstable(oracle_mod):
     o.close()
     q = diagnostics.quantities(r["pos"], r["vel"], spec.n_fluid, spec.params.particle_mass, box)
     assert q["escaped_fraction"] > 0.01
+
+
+def test_f32_error_against_fp64_single_step_from_flowing_state(oracle_mod):
+    """Error of the f32 path (the reference's arithmetic, which the CUDA path matches bit for
+    bit) against the FP64 twin, one substep from an identical, flowing state (30 substeps
+    into a dam break): density ~3e-7 relative; pressure and acceleration ~7e-6 of their
+    maxima (the Tait EOS amplifies density rounding ~7x near rest density); XSPH ~2e-7."""
+    from vxl_sph import scenes
+    spec = scenes.small_dam(n=(12, 14, 10), spacing=0.02, tank=(0.5, 0.5, 0.3), substeps=10)
+    o32 = oracle_mod.OracleSystem.from_scene(spec, threads=4)
+    o64 = oracle_mod.OracleSystem.from_scene(spec, threads=4, fp64=True)
+    dt = float(np.float32(np.float32(1) / np.float32(60)) / np.float32(spec.params.substeps))
+    for _ in range(30):
+        o32.substep(dt)
+    r = o32.read_f32()
+    o64.set_state(r["pos"], r["vel"])
+    o32.substep(dt)
+    o64.substep(dt)
+    a, b = o32.read(), o64.read()
+    o32.close()
+    o64.close()
+    nf = spec.n_fluid
+
+    def err(k, fluid_only=False):
+        x = np.asarray(a[k], np.float64)
+        y = np.asarray(b[k], np.float64)
+        if fluid_only:
+            x, y = x[:nf], y[:nf]
+        return np.max(np.abs(x - y)) / np.max(np.abs(y))
+
+    assert np.max(np.abs(np.asarray(a["dens"], np.float64) - b["dens"]) / b["dens"]) < 1e-6
+    assert err("press") < 3e-5
+    assert err("acc", True) < 3e-5
+    assert err("xsph", True) < 1e-6
