@@ -174,6 +174,8 @@ def run_reference(args) -> None:
     spec = build_scene(args.workload)
     from oracle import oracle as orc
     cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+    if args.cpu_threads:
+        cores = args.cpu_threads
     o = orc.OracleSystem.from_scene(spec, threads=cores)
     dt_sub = float(np.float32(np.float32(1.0) / np.float32(60.0)) / np.float32(spec.params.substeps))
     # one step = one substep of the workload (a bounded sample of the tick the GPU arm
@@ -228,37 +230,47 @@ def run_ours(args) -> None:
         scene.sync()
 
     l2_flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
-    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    scene.set_profile(True)
-    scene.step_tick_async(dt_tick, spec.spans)  # capture the profiled graph outside the timed region
-    scene.sync()
-    # the timed ticks start from the workload's initial state (the states the CPU arm times)
-    scene.write_state(spec.pos, spec.vel)
-    scene.set_profile(True)  # reset accumulators
 
+    def timed_ticks(profiled: bool) -> list:
+        """`args.steps` ticks from the workload's initial state (the states the CPU arm
+        times), L2 flushed before each, one CUDA-event pair per tick on the scene's stream."""
+        scene.write_state(spec.pos, spec.vel)
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+               for _ in range(args.steps)]
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        for k in range(args.steps):
+            if profiled:
+                scene.profile()  # collect the previous tick's kernel timers before enqueueing more
+            with torch.cuda.stream(stream):
+                l2_flush.zero_()
+                evs[k][0].record(stream)
+            scene.step_tick_async(dt_tick, spec.spans)
+            with torch.cuda.stream(stream):
+                evs[k][1].record(stream)
+        torch.cuda.synchronize()
+        scene.sync()
+        if dist:
+            dist.barrier()
+        return [a.elapsed_time(b) for a, b in evs]
+
+    # headline pass: the tick graph without per-kernel events
     clocks = ClockSampler(local)
-    torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
     clocks.start()
-    for k in range(args.steps):
-        scene.profile()  # collect the previous tick's kernel timers before enqueueing more
-        with torch.cuda.stream(stream):
-            l2_flush.zero_()
-            evs[k][0].record(stream)
-        scene.step_tick_async(dt_tick, spec.spans)
-        with torch.cuda.stream(stream):
-            evs[k][1].record(stream)
-    torch.cuda.synchronize()
-    scene.sync()
-    if dist:
-        dist.barrier()
+    step_ms = timed_ticks(False)
     clk = clocks.stop()
-    step_ms = [a.elapsed_time(b) for a, b in evs]
     total_ms = sum(step_ms)
-    prof = scene.profile()
     stats = scene.stats()
     cells = int(stats.cells)
+    launches_per_tick = int(stats.launches_last_tick)
+    # roofline pass: the same ticks with a CUDA-event pair around every kernel launch
+    scene.set_profile(True)
+    scene.step_tick_async(dt_tick, spec.spans)  # capture the profiled graph outside the timed ticks
+    scene.sync()
+    scene.set_profile(True)  # reset accumulators
+    prof_step_ms = timed_ticks(True)
+    prof = scene.profile()
 
     from vxl_sph import placement
     t_max = placement.max_over_ranks(total_ms, dist, f"cuda:{local}")
@@ -282,6 +294,10 @@ def run_ours(args) -> None:
                 "algorithmic_bytes_per_launch": bytes_launch,
                 "substep": {"bytes": substep_bytes(spec.n_fluid, spec.n_boundary, cells),
                             "ms": total_ms / (args.steps * sub)},
+                "profiled_ms_per_tick": sum(prof_step_ms) / args.steps,
+                "timing": "kernel times from a second pass over the same ticks with an event pair around "
+                          "every launch (k_bforce and k_react_* run on a second stream beside k_force, so "
+                          "their spans include waiting for SMs); value from the pass without them",
                 "kernels_ms_per_substep": {k: v[0] / max(args.steps * sub, 1) for k, v in sorted(prof.items())}}
     sb = roofline["substep"]
     sb["achieved_gbs"] = sb["bytes"] / (sb["ms"] / 1e3) / 1e9
@@ -337,7 +353,7 @@ def run_ours(args) -> None:
             "roofline": roofline,
             "cpu_baseline": cpu,
             "e2e": e2e,
-            "gpu_launches": int(stats.launches_last_tick) * args.steps,
+            "gpu_launches": launches_per_tick * args.steps,
             "clocks": clk,
             "step_ms": step_ms,
             **mix,
@@ -388,29 +404,35 @@ def measure_batched(local: int, steps: int, warmup: int, n_scenes: int = 256, se
     for _ in range(max(warmup, 3)):
         batch.step_tick(dt_tick)
     l2_flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
-    batch.set_profile(True)
-    batch.step_tick(dt_tick)
-    for q, sp in enumerate(specs):  # timed ticks start from the initial state
-        batch.write_state(q, sp.pos, sp.vel)
-    batch.set_profile(True)
-    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
-    torch.cuda.synchronize()
-    for k in range(steps):
-        batch.profile()
-        with torch.cuda.stream(stream):
-            l2_flush.zero_()
-            evs[k][0].record(stream)
-        batch.step_tick_async(dt_tick)
-        with torch.cuda.stream(stream):
-            evs[k][1].record(stream)
-    torch.cuda.synchronize()
-    batch.sync()
-    dev_ms = placement.max_over_ranks(sum(a.elapsed_time(b) for a, b in evs), dist, f"cuda:{local}")
-    prof = batch.profile()
-    batch.set_profile(False)
+
+    def timed_ticks(profiled: bool) -> float:
+        for q, sp in enumerate(specs):  # timed ticks start from the initial state
+            batch.write_state(q, sp.pos, sp.vel)
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        torch.cuda.synchronize()
+        for k in range(steps):
+            if profiled:
+                batch.profile()
+            with torch.cuda.stream(stream):
+                l2_flush.zero_()
+                evs[k][0].record(stream)
+            batch.step_tick_async(dt_tick)
+            with torch.cuda.stream(stream):
+                evs[k][1].record(stream)
+        torch.cuda.synchronize()
+        batch.sync()
+        return sum(a.elapsed_time(b) for a, b in evs)
+
+    dev_ms = placement.max_over_ranks(timed_ticks(False), dist, f"cuda:{local}")
     stats = batch.stats()
     cells = int(stats.cells)
     launches = int(stats.launches_last_tick)
+    batch.set_profile(True)
+    batch.step_tick(dt_tick)  # capture the profiled graph outside the timed ticks
+    batch.set_profile(True)
+    timed_ticks(True)
+    prof = batch.profile()
+    batch.set_profile(False)
     batch.step_tick(dt_tick)  # re-capture the tick graph without profiling events
     for q, sp in enumerate(specs):
         batch.write_state(q, sp.pos, sp.vel)
@@ -646,6 +668,7 @@ def main():
     ap.add_argument("--scenes", type=int, default=256, help="batched: number of tanks")
     ap.add_argument("--no-plain", action="store_true", help="batched/served: skip the plain-path comparison")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-threads", type=int, default=0, help="reference arm: host threads (default: all)")
     ap.add_argument("--ncu-case", action="store_true", help="build + warm-up ticks only (for ncu captures)")
     args = ap.parse_args()
     if args.ncu_case:
