@@ -276,6 +276,17 @@ vxl_status vxl_sph_get_tuning(vxl_sph_handle* h, vxl_sph_tuning* t);
  * Results are identical for every shape; only the time differs. */
 vxl_status vxl_sph_autotune(vxl_sph_handle* h, float dt_tick, uint32_t trials, vxl_sph_tuning* best);
 
+/* ------------------------------------------------------------------ deferred state readback
+ * The GPU tier's pipelined readback (Packet::run_deferred + take_deferred_state,
+ * crates/vxl-phys-gpu/src/pipeline.rs:603-609, pipeline/readback.rs:229-262): request enqueues,
+ * after whatever is already enqueued on the handle's stream (e.g. vxl_sph_step_tick_async),
+ * a copy of every particle's position (reference order; for a batch, scene after scene) into
+ * a pinned buffer the handle owns and returns without waiting; take waits for that copy and
+ * writes it out. The host's wait overlaps the tick: renderers draw the previous tick. */
+vxl_status vxl_sph_request_state(vxl_sph_handle* h);
+/* n: every particle of the handle (the sum over its scenes), as at the request. */
+vxl_status vxl_sph_take_state(vxl_sph_handle* h, float* pos_xyz, uint64_t n);
+
 /* ------------------------------------------------------------------ moving bodies on the device
  * The reference rebuilds the boundary segment on the host every tick from the bodies'
  * poses (set_boundary_particles, crates/vxl-phys-fluid/src/fluid_step.rs:13-53) and the GPU

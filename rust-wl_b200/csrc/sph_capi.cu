@@ -163,6 +163,24 @@ vxl_status vxl_sph_upload_boundary_scene(vxl_sph_handle* h, uint32_t scene, cons
   return h->e->upload_boundary(scene, pos_xyz, vel_xyz, nb);
 }
 
+vxl_status vxl_sph_request_state(vxl_sph_handle* h) {
+  HANDLE_OR_FAIL(h);
+  try {
+    return h->e->request_state();
+  } catch (...) {
+    return set_error(VXL_PANIC_CAUGHT, "exception in vxl_sph_request_state");
+  }
+}
+
+vxl_status vxl_sph_take_state(vxl_sph_handle* h, float* pos_xyz, uint64_t n) {
+  HANDLE_OR_FAIL(h);
+  try {
+    return h->e->take_state(pos_xyz, n);
+  } catch (...) {
+    return set_error(VXL_PANIC_CAUGHT, "exception in vxl_sph_take_state");
+  }
+}
+
 vxl_status vxl_sph_set_body_lattice(vxl_sph_handle* h, uint32_t scene, const float* local_xyz,
                                     const uint32_t* body_index, uint64_t nb, uint32_t nbodies) {
   HANDLE_OR_FAIL(h);

@@ -8,6 +8,7 @@
 #include <cstring>
 #include <new>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "sph_engine.cuh"
@@ -200,6 +201,10 @@ void Engine::free_all() {
   void* hp[] = {sc_h_, ctl_h_, spans_h_, chunks_h_, chunk_first_h_, breact_h_};
   for (void* p : hp)
     if (p) cudaFreeHost(p);
+  if (snap_h_) cudaFreeHost(snap_h_);
+  snap_h_ = nullptr;
+  if (ev_snap_) cudaEventDestroy(ev_snap_);
+  ev_snap_ = nullptr;
   if (blocal_) cudaFree(blocal_);
   if (poses_d_) cudaFree(poses_d_);
   blocal_ = nullptr;
@@ -545,6 +550,53 @@ vxl_status Engine::read_state(uint32_t q, float* pos, float* vel) {
   if (pos) CU(cudaMemcpyAsync(pos, dp, (size_t)n * 12, cudaMemcpyDeviceToHost, stream_));
   if (vel) CU(cudaMemcpyAsync(vel, dv, (size_t)n * 12, cudaMemcpyDeviceToHost, stream_));
   CU(cudaStreamSynchronize(stream_));
+  return VXL_OK;
+}
+
+vxl_status Engine::request_state() {
+  CU(cudaSetDevice(device_));
+  const uint64_t n = used_;
+  if (n > snap_cap_) {
+    if (snap_pending_) {
+      cudaEventSynchronize(ev_snap_);
+      snap_pending_ = false;
+    }
+    if (snap_h_) cudaFreeHost(snap_h_);
+    snap_h_ = nullptr;
+    snap_cap_ = 0;
+    CU(cudaMallocHost((void**)&snap_h_, n * 12));
+    snap_cap_ = n;
+  }
+  if (!ev_snap_) CU(cudaEventCreateWithFlags(&ev_snap_, cudaEventDisableTiming));
+  if (n) {
+    k_e_read_scene<<<blocks_for(n), kThreads, 0, stream_>>>((const float4*)pos_[0], nullptr, orig_, stage_,
+                                                             nullptr, 0u, (uint32_t)n);
+    CU(cudaGetLastError());
+    CU(cudaMemcpyAsync(snap_h_, stage_, n * 12, cudaMemcpyDeviceToHost, stream_));
+  }
+  CU(cudaEventRecord(ev_snap_, stream_));
+  snap_n_ = n;
+  snap_pending_ = true;
+  return VXL_OK;
+}
+
+vxl_status Engine::take_state(float* pos, uint64_t n) {
+  if (!snap_pending_) return set_error(VXL_NOT_READY, "no state requested");
+  if (n != snap_n_) return set_error(VXL_SIZE_MISMATCH, "n differs from the particles of the requested state");
+  if (n && !pos) return set_error(VXL_NULL_POINTER, "pos is NULL");
+  CU(cudaSetDevice(device_));
+  CU(cudaEventSynchronize(ev_snap_));
+  // copy out in parallel chunks for large states (one thread moves ~10 GB/s)
+  const size_t bytes = n * 12;
+  const size_t nthr = bytes >= (64u << 20) ? std::min<size_t>(8, std::max<unsigned>(1, std::thread::hardware_concurrency())) : 1;
+  const size_t chunk = ((bytes / nthr) + 63) & ~size_t(63);
+  std::vector<std::thread> th;
+  for (size_t t = 1; t < nthr && t * chunk < bytes; ++t)
+    th.emplace_back([=] {
+      std::memcpy((char*)pos + t * chunk, (const char*)snap_h_ + t * chunk, std::min(chunk, bytes - t * chunk));
+    });
+  std::memcpy(pos, snap_h_, std::min(chunk, bytes));
+  for (auto& x : th) x.join();
   return VXL_OK;
 }
 

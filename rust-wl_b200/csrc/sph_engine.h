@@ -73,6 +73,10 @@ class Engine {
   vxl_status set_body_poses(uint32_t scene, const vxl_sph_body_pose* poses, uint32_t nbodies);
   vxl_status write_state(uint32_t scene, const float* pos, const float* vel);
   vxl_status read_state(uint32_t scene, float* pos, float* vel);
+  // Deferred readback of every slot's position (reference order, scene after scene):
+  // request enqueues the copy into a pinned buffer and returns; take waits and copies out.
+  vxl_status request_state();
+  vxl_status take_state(float* pos, uint64_t n);
   vxl_status read_fields(uint32_t scene, float* dens, float* press, float* acc, float* xsph, float* bforce);
   vxl_status export_grid(uint32_t scene, uint32_t* items, uint32_t* start, uint64_t start_cap, uint32_t* bins,
                          vxl_sph_grid_info* info);
@@ -153,7 +157,11 @@ class Engine {
   uint32_t* halves_ = nullptr;
   float4* blocal_ = nullptr;         // body-frame lattice per boundary slot (reference order), lazily
   BodyPoseDev* poses_d_ = nullptr;   // poses of one scene's bodies (staged per call)
-  uint32_t poses_cap_ = 0;  // 4 words per 32 slots: upper-half masks along x, y, z
+  uint32_t poses_cap_ = 0;
+  float* snap_h_ = nullptr;  // pinned, 3 floats per slot
+  uint64_t snap_cap_ = 0, snap_n_ = 0;
+  cudaEvent_t ev_snap_ = nullptr;
+  bool snap_pending_ = false;  // 4 words per 32 slots: upper-half masks along x, y, z
   float* stage_ = nullptr;  // 8 floats per slot: staging for host transfers
   // cells (cell_cap_ + 1)
   uint32_t* counts_ = nullptr;

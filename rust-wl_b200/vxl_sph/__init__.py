@@ -185,6 +185,8 @@ SIGNATURES = {
     "vxl_sph_set_tuning": (C.c_int, [_H, C.POINTER(Tuning)]),
     "vxl_sph_get_tuning": (C.c_int, [_H, C.POINTER(Tuning)]),
     "vxl_sph_autotune": (C.c_int, [_H, C.c_float, C.c_uint32, C.POINTER(Tuning)]),
+    "vxl_sph_request_state": (C.c_int, [_H]),
+    "vxl_sph_take_state": (C.c_int, [_H, _FP, C.c_uint64]),
     "vxl_sph_set_body_lattice": (C.c_int, [_H, C.c_uint32, _FP, C.POINTER(C.c_uint32), C.c_uint64, C.c_uint32]),
     "vxl_sph_set_body_poses": (C.c_int, [_H, C.c_uint32, C.POINTER(BodyPose), C.c_uint32]),
     "vxl_sph_serve_create": (C.c_int, [C.c_int32, C.c_uint64, C.c_uint32, C.POINTER(C.c_void_p)]),
@@ -368,6 +370,16 @@ class Scene:
         vel = np.ascontiguousarray(vel, dtype=np.float32).reshape(-1, 3)
         _check(self.lib.vxl_sph_upload_boundary(self._h, self.n_fluid, _fptr(pos), _fptr(vel), pos.shape[0]))
 
+    def request_state(self) -> None:
+        """Enqueue a copy of every position after the work already enqueued; returns at once."""
+        _check(self.lib.vxl_sph_request_state(self._h))
+
+    def take_state(self, out: np.ndarray | None = None) -> np.ndarray:
+        """Wait for the requested copy; positions (N, 3) in reference order."""
+        p = np.empty((self.n_total, 3), np.float32) if out is None else out
+        _check(self.lib.vxl_sph_take_state(self._h, _fptr(p), p.shape[0]))
+        return p
+
     def set_body_lattice(self, local_xyz: np.ndarray, body_index: np.ndarray, nbodies: int, scene: int = 0) -> None:
         """Body-frame lattice of the boundary segment (see scenes.body_lattice)."""
         lx = np.ascontiguousarray(local_xyz, dtype=np.float32).reshape(-1, 3)
@@ -492,6 +504,7 @@ class Batch:
         self._h = h
         self.lib = lib
         self.specs = list(specs)
+        self.n_total = sum(sp.n_total for sp in specs)
         for q, sp in enumerate(specs):
             if sp.spans:
                 a, n = spans_array(sp.spans)  # scene-local particle indices
@@ -582,6 +595,8 @@ class Batch:
         _check(self.lib.vxl_sph_set_profile(self._h, 1 if on else 0))
 
     profile = Scene.profile
+    request_state = Scene.request_state
+    take_state = Scene.take_state
 
     def stats(self) -> Stats:
         s = Stats()

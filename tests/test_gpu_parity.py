@@ -429,3 +429,31 @@ def test_device_body_rebuild_equals_host_upload(vxl, oracle_mod):
         r = o.read_f32()
         assert_bits(pb, r["pos"], f"tick {t} pos vs oracle")
     o.close()
+
+
+def test_deferred_readback_and_vxld_dump(vxl, oracle_mod, tmp_path):
+    """vxl_sph_request_state / vxl_sph_take_state return the state that vxl_sph_read_state
+    returns, and a VXLD dump's frames are the oracle's fluid positions at those ticks."""
+    from vxl_sph import export, scenes
+    spec = scenes.small_dam(n=(8, 10, 8), spacing=0.05, tank=(0.8, 0.7, 0.6), seed=4)
+    g = vxl.Scene(spec.params, spec.pos, spec.vel, spec.pmass, spec.n_fluid)
+    dt = float(F32(1.0) / F32(60.0))
+    g.step_tick(dt, spec.spans)
+    g.request_state()
+    p1 = g.take_state()
+    p2, _ = g.read_state()
+    assert_bits(p1, p2, "take_state vs read_state")
+    g.close()
+    g = vxl.Scene(spec.params, spec.pos, spec.vel, spec.pmass, spec.n_fluid)
+    path = str(tmp_path / "dam.bin")
+    info = export.dump_run(g, path, ticks=6, dt_tick=dt, spans=spec.spans)
+    assert info["frames"] == 3
+    r = export.read_vxld(path)
+    o = oracle_mod.OracleSystem.from_scene(spec, threads=4)
+    for t in range(1, 7):
+        o.step(dt)
+        if t % 2 == 0:
+            fr = r["frames"][t // 2 - 1]
+            assert fr["tick"] == t
+            assert_bits(fr["systems"][0], o.read_f32()["pos"][:spec.n_fluid], f"frame at tick {t}")
+    o.close()

@@ -194,3 +194,22 @@ def test_body_lattice_matches_body_particles(vxl):
         r = (wp - bp).astype(F)
         wv = (np.asarray(b.linvel, F) + scenes._cross(np.broadcast_to(np.asarray(b.angvel, F), r.shape), r)).astype(F)
         assert wv.tobytes() == vel[sel].tobytes()
+
+
+def test_vxld_round_trip(tmp_path):
+    """VXLD v3 writer/reader round trip (the layout of the reference's demo dumps)."""
+    from vxl_sph import export
+    rng = np.random.Generator(np.random.PCG64(1))
+    frames = [rng.standard_normal((17, 3)).astype(np.float32) for _ in range(3)]
+    path = tmp_path / "run.bin"
+    with open(path, "wb") as f:
+        export.write_header(f, 6, 2, 1.0 / 60.0, 1)
+        for k, p in enumerate(frames):
+            export.write_frame(f, 2 * (k + 1), 1.5, [p])
+    r = export.read_vxld(str(path))
+    assert r["version"] == 3 and r["ticks"] == 6 and r["ticks_per_frame"] == 2
+    assert [fr["tick"] for fr in r["frames"]] == [2, 4, 6]
+    for fr, p in zip(r["frames"], frames):
+        assert fr["systems"][0].tobytes() == p.tobytes()
+    # header size: magic + 4 words + voxel block (28 B) + 3 counts
+    assert path.stat().st_size == 4 + 16 + 28 + 12 + 3 * (12 + 1 + 4 + 17 * 12)
