@@ -1019,8 +1019,15 @@ vxl_status Engine::finish() {
   if (ctl_h_->err & kErrCellCap) {
     ctl_h_->err = 0;
     cudaMemsetAsync(&ctl_d_->err, 0, 4, stream_);
+    // the skipped substeps left the state as it was but emptied the fluid AABB
+    // accumulators (reset by the grid-box pass): rebuild them from the state
+    for (uint32_t q = 0; q < scenes_.size(); ++q) {
+      vxl_status s = recompute_scene_boxes(q);
+      if (s != VXL_OK) return s;
+    }
     cudaStreamSynchronize(stream_);
-    return set_error(VXL_DEVICE_FAULT_FLAG, "the scenes' cells exceed the engine's cell capacity; the substep was skipped");
+    return set_error(VXL_DEVICE_FAULT_FLAG,
+                     "the scenes' cells exceed the engine's cell capacity; the tick was skipped, state unchanged");
   }
   return VXL_OK;
 }

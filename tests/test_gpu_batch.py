@@ -150,3 +150,32 @@ def test_served_budget_queues_then_admits(vxl):
         p, _ = srv.read(i)
         ap, _ = _alone(vxl, s, 2)
         _assert_same(p, ap, "queued request")
+
+
+def test_cell_capacity_overflow_is_reported_and_harmless(vxl):
+    """A batch whose scenes need more cells than its cell capacity: the device flags it, every
+    kernel of the tick returns without touching memory, the call reports
+    VXL_DEVICE_FAULT_FLAG and the state is exactly the state before — repeatedly (no GPU
+    fault involved; the flag is an ordinary word the host reads)."""
+    specs = _specs()
+    b = vxl.Batch(specs, cell_capacity=64)
+    before = [b.read_state(q) for q in range(len(specs))]
+    for _ in range(2):
+        with pytest.raises(vxl.VxlError) as e:
+            b.step_tick(DT_TICK)
+        assert e.value.status == vxl.DEVICE_FAULT_FLAG and "cell capacity" in str(e.value)
+        for q in range(len(specs)):
+            p, v = b.read_state(q)
+            _assert_same(p, before[q][0], f"scene {q} pos")
+            _assert_same(v, before[q][1], f"scene {q} vel")
+
+
+def test_served_request_that_never_fits_is_rejected(vxl):
+    from vxl_sph import scenes
+    srv = vxl.Server(budget_bytes=64 << 20)
+    big = scenes.small_dam(n=(40, 40, 40), spacing=0.01, tank=(0.6, 0.6, 0.6), seed=1)
+    with pytest.raises(vxl.VxlError) as e:
+        srv.submit(big, 2)
+    assert e.value.status == vxl.OUT_OF_MEMORY
+    rep = srv.step(DT_TICK)
+    assert rep.active == 0 and rep.queued == 0
