@@ -179,3 +179,32 @@ def test_served_request_that_never_fits_is_rejected(vxl):
     assert e.value.status == vxl.OUT_OF_MEMORY
     rep = srv.step(DT_TICK)
     assert rep.active == 0 and rep.queued == 0
+
+
+def test_batch_with_boundary_only_and_single_particle_scenes(vxl):
+    """Degenerate scenes inside a batch: a boundary-only scene stays exactly where it is
+    (the reference does not drive a system without fluid, fluid_step.rs:93-95) and a
+    one-particle scene falls like its own plain handle; the ordinary scenes around them are
+    unaffected."""
+    from vxl_sph import scenes
+    specs = _specs()[:2]
+    b_pos, b_vel, b_pm, b_spans = scenes.body_particles([scenes.Body(0, (0.1, 0.02, 0.1), (0.2, 0.1, 0.2))],
+                                                        0.05, 0.1, 1, 1000.0)
+    p = scenes.baseline_params(0.05, substeps=4)
+    walls_only = scenes.SceneSpec("walls", p, b_pos, b_vel, b_pm, 0, [], 0.05, 1)
+    one = scenes.SceneSpec("one", scenes.baseline_params(0.05, substeps=4), np.array([[0.3, 0.4, 0.2]], F32),
+                           np.zeros((1, 3), F32), np.full(1, F32(p.particle_mass), F32), 1, [], 0.05, 1)
+    mix = [specs[0], walls_only, one, specs[1]]
+    batch = vxl.Batch(mix)
+    plain = [vxl.Scene(s.params, s.pos, s.vel, s.pmass, s.n_fluid) for s in mix]
+    for _ in range(3):
+        batch.step_tick(DT_TICK)
+        for q, (pl, s) in enumerate(zip(plain, mix)):
+            pl.step_tick(DT_TICK, s.spans if q != 1 else ())
+    for q, pl in enumerate(plain):
+        bp, bv = batch.read_state(q)
+        pp, pv = pl.read_state()
+        _assert_same(bp, pp, f"scene {q} pos")
+        _assert_same(bv, pv, f"scene {q} vel")
+    wp, _ = batch.read_state(1)
+    _assert_same(wp, b_pos, "boundary-only scene moved")
