@@ -14,7 +14,6 @@ namespace vxl {
 
 constexpr uint32_t kGridDimMax = 1u << 14;   // crates/vxl-phys-core/src/grid.rs:8
 constexpr uint32_t kErrGridLoop = 1u << 0;    // grid-box doubling loop did not settle
-constexpr uint32_t kErrNeighbourCap = 1u << 1;  // a boundary gather used its slow path (info)
 constexpr uint32_t kErrCanonLarge = 1u << 2;  // a cell above the shared-memory sort size (info)
 
 // Grid box of one substep: crates/vxl-phys-core/src/grid.rs:34-50 (min, bin, dims)
@@ -27,16 +26,6 @@ struct GridBox {
   uint32_t pad[3];
 };
 
-// Device control block of one scene.
-struct Ctl {
-  uint32_t fbox[6];  // fluid AABB accumulator, ordered-uint: min xyz, max xyz
-  uint32_t bbox[6];  // boundary AABB (fixed within a tick)
-  GridBox grid;
-  uint32_t err;
-  uint32_t slow_gathers;
-  uint32_t pad[2];
-};
-
 // Constants of one scene, computed on the host exactly as FluidSystem::new does
 // (crates/vxl-phys-fluid/src/fluid_access.rs:8-13).
 struct SphConst {
@@ -45,11 +34,6 @@ struct SphConst {
   float gx, gy, gz;
   uint32_t clamp_p, gamma7;
   uint32_t n_fluid, n_total, max_bins;
-};
-
-// Per-substep values (fluid_step.rs:112-123).
-struct StepConst {
-  float dt, vmax, vmax2;
 };
 
 // Ordered-uint encoding of floats: monotone, so atomicMin/atomicMax on the code give

@@ -677,7 +677,7 @@ class PhysGpuBackend:
         return bool(load().vxl_sph_backend_available())
 
     def submit(self, tag: str) -> bool:
-        # The reference's fluid path never calls submit (SURVEY: marker trait); the
+        # The reference's fluid path never calls submit (for it the trait is a marker); the
         # fluid entry points are the stepper's.
         return False
 

@@ -23,7 +23,7 @@ pytestmark = pytest.mark.gpu
 
 GOLDEN = json.loads((Path(__file__).parent / "golden" / "grid_hashes.json").read_text())
 REACTION_RTOL = 1e-5   # |F_gpu - F_cpu| <= REACTION_RTOL * sum_k |f_k| (per span, per axis)
-DENS_RTOL = 1e-5       # north-star per-step tolerance (f32), used where bitwise is not claimed
+DENS_RTOL = 1e-5       # per-step tolerance of the f32 fluid step, used where bitwise is not claimed
 F32 = np.float32
 
 
