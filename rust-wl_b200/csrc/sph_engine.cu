@@ -32,11 +32,11 @@ constexpr uint32_t kBoundaryTile = 128;  // boundary particles per tile of the r
 inline uint32_t blocks_for(uint64_t n, int t = kThreads) { return (uint32_t)((n + t - 1) / t); }
 
 enum KernelId : int {
-  KID_GRIDBOX, KID_CELLOFF, KID_KEYS, KID_SCAN_PARTIAL, KID_SCAN_TOP, KID_SCAN_FINAL, KID_PLACE, KID_CANON,
+  KID_CELLOFF, KID_KEYS, KID_SCAN_PARTIAL, KID_SCAN_TOP, KID_SCAN_FINAL, KID_PLACE, KID_CANON,
   KID_DENSITY, KID_FORCE, KID_BFORCE, KID_REACT_CHUNKS, KID_REACT_SPANS, KID_SCALE, KID_HALFMASK, KID_COUNT
 };
 const char* const kKernelNames[KID_COUNT] = {
-    "k_gridbox", "k_celloff", "k_keys", "k_scan_partial", "k_scan_top", "k_scan_final", "k_place", "k_canon",
+    "k_celloff", "k_keys", "k_scan_partial", "k_scan_top", "k_scan_final", "k_place", "k_canon",
     "k_density", "k_force", "k_bforce", "k_react_chunks", "k_react_spans", "k_scale", "k_halfmask"};
 
 constexpr size_t kSceneHostBytes = offsetof(SceneDev, g);
@@ -870,8 +870,6 @@ void Engine::enqueue_substep(bool with_reactions) {
   // The previous substep's reaction branch reads this substep's inputs-to-be (scene grids,
   // cell table, sorted buffer, permutation, lists, work counters): join it first.
   join_side();
-  cudaMemsetAsync(ctl_d_->work, 0, sizeof(ctl_d_->work), st);
-  LAUNCH(KID_GRIDBOX, k_e_gridbox<<<blocks_for(S, 128), 128, 0, st>>>(sc_d_, S, ctl_d_));
   LAUNCH(KID_CELLOFF, k_e_celloff<<<1, 1024, 0, st>>>(sc_d_, S, ctl_d_, (uint32_t)cell_cap_));
   LAUNCH(KID_KEYS, k_e_keys<<<key_blocks, kThreads, 0, st>>>(p0, sc_d_, tiles_d_, ntiles_, ctl_d_, counts_,
                                                              (uint2*)cellrank_));

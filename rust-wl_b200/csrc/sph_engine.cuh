@@ -95,7 +95,7 @@ struct EngineCtl {
   uint32_t cells;  // sum of the scenes' cells this substep
   uint32_t err;
   uint32_t slow_gathers;
-  uint32_t pad;
+  uint32_t doubled;  // some scene's bins are at least 2h this substep (half-cell masks needed)
   uint32_t work[kWorkSlots];
 };
 
@@ -337,39 +337,46 @@ __global__ void k_e_slot_of(const uint32_t* __restrict__ orig, uint32_t* __restr
 
 // ---------------------------------------------------------------- substep kernels
 
-// Per scene: grid box of this substep from the AABB of all its particles
-// (crates/vxl-phys-fluid/src/grid.rs:37-44 -> crates/vxl-phys-core/src/grid.rs:34-50),
-// then reset the fluid accumulator for the force kernel's epilogue.
-__global__ void k_e_gridbox(SceneDev* __restrict__ sc, uint32_t nscenes, EngineCtl* ctl) {
-  const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= nscenes) return;
-  SceneDev& s = sc[q];
-  float lo[3], hi[3];
-  for (int a = 0; a < 3; ++a) {
-    lo[a] = fminf(o2f(s.fbox[a]), o2f(s.bbox[a]));
-    hi[a] = fmaxf(o2f(s.fbox[3 + a]), o2f(s.bbox[3 + a]));
-  }
-  GridBox g;
-  if (!grid_box(lo[0], lo[1], lo[2], hi[0], hi[1], hi[2], s.k.h, s.k.max_bins, g)) atomicOr(&ctl->err, kErrGridLoop);
-  s.g = g;
-  s.cells = g.total;
-  for (int a = 0; a < 3; ++a) {
-    s.fbox[a] = 0xffffffffu;
-    s.fbox[3 + a] = 0u;
-  }
-}
-
-// Cell offsets: exclusive scan of the scenes' cell counts (one block, any scene count);
+// Grid boxes and cell offsets (one block, any scene count): each scene's grid for this
+// substep (crates/vxl-phys-fluid/src/grid.rs:37-44 -> crates/vxl-phys-core/src/grid.rs:34-50)
+// from its AABB accumulators, which are then reset for the force pass's epilogue; then an
+// exclusive scan of the scenes' cell counts;
 // flags the substep when the total exceeds the cell capacity (every later kernel then
 // returns without touching memory).
 __global__ void k_e_celloff(SceneDev* __restrict__ sc, uint32_t nscenes, EngineCtl* ctl, uint32_t cell_cap) {
   __shared__ uint32_t sh[1024];
   __shared__ unsigned long long carry;
-  if (threadIdx.x == 0) carry = 0;
+  __shared__ uint32_t doubled;
+  if (threadIdx.x == 0) {
+    carry = 0;
+    doubled = 0;
+  }
+  if (threadIdx.x < kWorkSlots) ctl->work[threadIdx.x] = 0;  // persistent-pass counters of this substep
   __syncthreads();
   for (uint32_t b0 = 0; b0 < nscenes; b0 += 1024) {
     const uint32_t q = b0 + threadIdx.x;
-    const uint32_t v = q < nscenes ? sc[q].cells : 0u;
+    uint32_t v = 0;
+    if (q < nscenes) {
+      // this substep's grid from the AABB accumulators (the reference's rule on all of the
+      // scene's particles, crates/vxl-phys-core/src/grid.rs:34-50); reset the fluid one
+      SceneDev& s = sc[q];
+      float lo[3], hi[3];
+      for (int a = 0; a < 3; ++a) {
+        lo[a] = fminf(o2f(s.fbox[a]), o2f(s.bbox[a]));
+        hi[a] = fmaxf(o2f(s.fbox[3 + a]), o2f(s.bbox[3 + a]));
+      }
+      GridBox g;
+      if (!grid_box(lo[0], lo[1], lo[2], hi[0], hi[1], hi[2], s.k.h, s.k.max_bins, g))
+        atomicOr(&ctl->err, kErrGridLoop);
+      s.g = g;
+      s.cells = g.total;
+      for (int a = 0; a < 3; ++a) {
+        s.fbox[a] = 0xffffffffu;
+        s.fbox[3 + a] = 0u;
+      }
+      if (g.bin >= 2.0f * s.k.h) doubled = 1;
+      v = g.total;
+    }
     sh[threadIdx.x] = v;
     __syncthreads();
     for (uint32_t off = 1; off < 1024; off <<= 1) {
@@ -385,6 +392,7 @@ __global__ void k_e_celloff(SceneDev* __restrict__ sc, uint32_t nscenes, EngineC
     __syncthreads();
   }
   if (threadIdx.x == 0) {
+    ctl->doubled = doubled;
     if (carry > (unsigned long long)cell_cap) {
       atomicOr(&ctl->err, kErrCellCap);
       ctl->cells = 0;
@@ -659,7 +667,7 @@ __device__ __forceinline__ void walk27(const GridBox& g, const uint32_t* __restr
 __global__ void k_e_halfmask(const float4* __restrict__ pos, const SceneDev* __restrict__ sc,
                              const TileDev* __restrict__ tiles, uint32_t ntiles, const EngineCtl* __restrict__ ctl,
                              uint32_t* __restrict__ halves) {
-  if (ctl->err & kErrCellCap) return;
+  if ((ctl->err & kErrCellCap) || !ctl->doubled) return;
   const int lane = threadIdx.x & 31;
   for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
     const TileDev td = tiles[t];
