@@ -32,11 +32,11 @@ constexpr uint32_t kBoundaryTile = 128;  // boundary particles per tile of the r
 inline uint32_t blocks_for(uint64_t n, int t = kThreads) { return (uint32_t)((n + t - 1) / t); }
 
 enum KernelId : int {
-  KID_CELLOFF, KID_KEYS, KID_SCAN_PARTIAL, KID_SCAN_TOP, KID_SCAN_FINAL, KID_PLACE, KID_CANON,
+  KID_CELLOFF, KID_KEYS, KID_SCAN_PARTIAL, KID_SCAN_FINAL, KID_PLACE, KID_CANON,
   KID_DENSITY, KID_FORCE, KID_BFORCE, KID_REACT_CHUNKS, KID_REACT_SPANS, KID_SCALE, KID_HALFMASK, KID_COUNT
 };
 const char* const kKernelNames[KID_COUNT] = {
-    "k_celloff", "k_keys", "k_scan_partial", "k_scan_top", "k_scan_final", "k_place", "k_canon",
+    "k_celloff", "k_keys", "k_scan_partial", "k_scan_final", "k_place", "k_canon",
     "k_density", "k_force", "k_bforce", "k_react_chunks", "k_react_spans", "k_scale", "k_halfmask"};
 
 constexpr size_t kSceneHostBytes = offsetof(SceneDev, g);
@@ -872,15 +872,14 @@ void Engine::enqueue_substep(bool with_reactions) {
   join_side();
   LAUNCH(KID_CELLOFF, k_e_celloff<<<1, 1024, 0, st>>>(sc_d_, S, ctl_d_, (uint32_t)cell_cap_));
   LAUNCH(KID_KEYS, k_e_keys<<<key_blocks, kThreads, 0, st>>>(p0, sc_d_, tiles_d_, ntiles_, ctl_d_, counts_,
-                                                             (uint2*)cellrank_));
-  LAUNCH(KID_SCAN_PARTIAL, k_e_scan_partial<<<148 * 4, kScanThreads, 0, st>>>(counts_, ctl_d_, partial_));
-  LAUNCH(KID_SCAN_TOP, k_e_scan_top<<<1, 1024, 0, st>>>(partial_, ctl_d_, start_));
+                                                             (uint2*)cellrank_, halves_,
+                                                             (uint32_t)(4 * (used_ / 32 + 1))));
+  LAUNCH(KID_SCAN_PARTIAL, k_e_scan_partial<<<148 * 4, kScanThreads, 0, st>>>(counts_, ctl_d_, partial_, start_));
   LAUNCH(KID_SCAN_FINAL, k_e_scan_final<<<148 * 4, kScanThreads, 0, st>>>(counts_, ctl_d_, partial_, start_));
   LAUNCH(KID_PLACE, k_e_place<<<key_blocks, kThreads, 0, st>>>((const uint2*)cellrank_, start_, orig_, tiles_d_,
                                                                ntiles_, ctl_d_, (uint2*)items_));
   LAUNCH(KID_CANON, k_e_canon<<<148 * 8, 256, 0, st>>>((const uint2*)items_, start_, ctl_d_, p0, v0, (float4*)pos_[1],
                                                        (float4*)vel_[1], orig_, slot_of_));
-  cudaMemsetAsync(halves_, 0, (size_t)16 * (used_ / 32 + 1), st);
   LAUNCH(KID_HALFMASK, k_e_halfmask<<<key_blocks, kThreads, 0, st>>>(p1, sc_d_, tiles_d_, ntiles_, ctl_d_, halves_));
   const uint32_t stride = (uint32_t)slot_cap_;
   const bool rec = record_;

@@ -100,7 +100,7 @@ struct EngineCtl {
 };
 
 // Work counter indices.
-enum WorkId : int { kWorkDensity = 0, kWorkForce = 1, kWorkBforce = 2 };
+enum WorkId : int { kWorkDensity = 0, kWorkForce = 1, kWorkBforce = 2, kWorkScan = 3 };
 
 namespace {
 
@@ -407,8 +407,12 @@ __global__ void k_e_celloff(SceneDev* __restrict__ sc, uint32_t nscenes, EngineC
 // makes the final order deterministic.
 __global__ void k_e_keys(const float4* __restrict__ pos, const SceneDev* __restrict__ sc,
                          const TileDev* __restrict__ tiles, uint32_t ntiles, const EngineCtl* __restrict__ ctl,
-                         uint32_t* __restrict__ counts, uint2* __restrict__ cellrank) {
+                         uint32_t* __restrict__ counts, uint2* __restrict__ cellrank, uint32_t* __restrict__ halves,
+                         uint32_t half_words) {
   if (ctl->err & kErrCellCap) return;
+  if (ctl->doubled)  // clear the half-cell masks that k_e_halfmask fills after the sort
+    for (uint32_t w = blockIdx.x * blockDim.x + threadIdx.x; w < half_words; w += gridDim.x * blockDim.x)
+      halves[w] = 0u;
   for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
     const TileDev td = tiles[t];
     const GridBox g = sc[td.scene].g;
@@ -435,17 +439,20 @@ __global__ void k_e_keys(const float4* __restrict__ pos, const SceneDev* __restr
   }
 }
 
-// Exclusive scan of the global cell counts -> start (phase 1: tile sums).
-__global__ void k_e_scan_partial(const uint32_t* __restrict__ counts, const EngineCtl* __restrict__ ctl,
-                                 uint32_t* __restrict__ partial) {
+// Phases 1-2 of the scan: per-tile sums of the counts (tiles of kScanTile cells,
+// grid-stride), then, in whichever block finishes last (an atomic count of finished blocks;
+// nothing waits), the exclusive scan of the tile sums in place and the total into
+// start[cells].
+__global__ void k_e_scan_partial(const uint32_t* __restrict__ counts, EngineCtl* ctl,
+                                 uint32_t* __restrict__ partial, uint32_t* __restrict__ start) {
   if (ctl->err & kErrCellCap) return;
   const uint32_t total = ctl->cells;
+  __shared__ uint32_t ws[kScanThreads / 32];
   for (uint32_t tile = blockIdx.x; (size_t)tile * kScanTile < total; tile += gridDim.x) {
     const uint32_t base = tile * kScanTile;
     uint32_t sum = 0;
     for (uint32_t i = base + threadIdx.x; i < min(base + kScanTile, total); i += kScanThreads) sum += counts[i];
     for (int off = 16; off > 0; off >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, off);
-    __shared__ uint32_t ws[kScanThreads / 32];
     if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = sum;
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -455,24 +462,25 @@ __global__ void k_e_scan_partial(const uint32_t* __restrict__ counts, const Engi
     }
     __syncthreads();
   }
-}
-
-// Phase 2: one block scans the tile sums (any count, 1024 at a time with a carry).
-__global__ void k_e_scan_top(uint32_t* __restrict__ partial, const EngineCtl* __restrict__ ctl,
-                             uint32_t* __restrict__ start) {
-  if (ctl->err & kErrCellCap) return;
-  const uint32_t total = ctl->cells;
+  __shared__ uint32_t last;
+  if (threadIdx.x == 0) {
+    __threadfence();  // this block's tile sums are visible before it counts itself done
+    last = atomicAdd(&ctl->work[kWorkScan], 1u) == gridDim.x - 1 ? 1u : 0u;
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
   const uint32_t ntiles = (total + kScanTile - 1) / kScanTile;
-  __shared__ uint32_t sh[1024];
+  __shared__ uint32_t sh[kScanThreads];
   __shared__ uint32_t carry;
   if (threadIdx.x == 0) carry = 0;
   __syncthreads();
-  for (uint32_t b0 = 0; b0 < ntiles; b0 += 1024) {
+  for (uint32_t b0 = 0; b0 < ntiles; b0 += kScanThreads) {
     const uint32_t t = b0 + threadIdx.x;
-    const uint32_t v = t < ntiles ? partial[t] : 0u;
+    const uint32_t v = t < ntiles ? __ldcg(partial + t) : 0u;  // written by other blocks: skip L1
     sh[threadIdx.x] = v;
     __syncthreads();
-    for (uint32_t off = 1; off < 1024; off <<= 1) {
+    for (uint32_t off = 1; off < kScanThreads; off <<= 1) {
       const uint32_t add = threadIdx.x >= off ? sh[threadIdx.x - off] : 0u;
       __syncthreads();
       sh[threadIdx.x] += add;
@@ -480,12 +488,11 @@ __global__ void k_e_scan_top(uint32_t* __restrict__ partial, const EngineCtl* __
     }
     if (t < ntiles) partial[t] = carry + sh[threadIdx.x] - v;
     __syncthreads();
-    if (threadIdx.x == 1023) carry += sh[1023];
+    if (threadIdx.x == kScanThreads - 1) carry += sh[kScanThreads - 1];
     __syncthreads();
   }
   if (threadIdx.x == 0) start[total] = carry;
 }
-
 // Phase 3: per-tile exclusive scan + tile offset -> start; zero counts for the next substep.
 __global__ void k_e_scan_final(uint32_t* __restrict__ counts, const EngineCtl* __restrict__ ctl,
                                const uint32_t* __restrict__ partial, uint32_t* __restrict__ start) {
