@@ -171,11 +171,14 @@ def run_reference(args) -> None:
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    spec = build_scene(args.workload)
     from oracle import oracle as orc
     cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
     if args.cpu_threads:
         cores = args.cpu_threads
+    if args.workload in ("batched", "served"):
+        run_reference_mix(args, orc, cores)
+        return
+    spec = build_scene(args.workload)
     o = orc.OracleSystem.from_scene(spec, threads=cores)
     dt_sub = float(np.float32(np.float32(1.0) / np.float32(60.0)) / np.float32(spec.params.substeps))
     # one step = one substep of the workload (a bounded sample of the tick the GPU arm
@@ -198,6 +201,46 @@ def run_reference(args) -> None:
                    "step": "one substep on the host cores (reference CPU path restated in C++; Rust not buildable here)"},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
                          "sample": f"{args.steps} substeps of {spec.name} after {args.warmup} warm-up substeps"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_reference_mix(args, orc, cores: int) -> None:
+    """The reference CPU path scene by scene on the batched or served workload: each step is
+    one substep of every scene of a bounded sample (the first `--scenes` tanks of the mix,
+    at most 16, or the first 8 requests), the scenes stepped one after another as a host
+    running one FluidSystem per scene would."""
+    from vxl_sph import scenes
+    if args.workload == "batched":
+        specs = scenes.batched_mix(min(args.scenes, 16))
+        sample = f"the first {len(specs)} of the 256 tanks"
+    else:
+        specs = [r.spec for r in scenes.served_stream(8, args.rate, tick_scale=args.tick_scale)]
+        sample = f"the first {len(specs)} requests of the stream"
+    systems = [orc.OracleSystem.from_scene(sp, threads=cores) for sp in specs]
+    dts = [float(np.float32(np.float32(1.0) / np.float32(60.0)) / np.float32(sp.params.substeps)) for sp in specs]
+    for _ in range(args.warmup):
+        for o, dt in zip(systems, dts):
+            o.substep(dt)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        for o, dt in zip(systems, dts):
+            o.substep(dt)
+    total = time.perf_counter() - t0
+    for o in systems:
+        o.close()
+    nf = sum(sp.n_fluid for sp in specs)
+    value = nf * args.steps / total
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded tanks)",
+        "config": {"workload": args.workload, "scenes": len(specs), "n_fluid": nf,
+                   "step": "one substep of every sampled scene, scene by scene, on the host cores"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": f"{args.steps} substeps of {sample} after {args.warmup} warm-up substeps"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)

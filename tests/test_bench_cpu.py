@@ -33,3 +33,11 @@ def test_reference_arm_other_ranks_exit_quietly():
              "--warmup", "0")
     assert r.returncode == 0, r.stderr
     assert r.stdout.strip() == ""
+
+
+def test_reference_arm_on_the_batched_sample():
+    r = _run({}, "--workload", "batched", "--scenes", "2", "--steps", "1", "--warmup", "0")
+    assert r.returncode == 0, r.stderr
+    line = json.loads(r.stdout.strip().splitlines()[-1])
+    assert line["impl"] == "reference" and line["value"] > 0
+    assert line["config"]["workload"] == "batched" and line["config"]["scenes"] == 2
