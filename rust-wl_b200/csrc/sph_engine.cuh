@@ -36,7 +36,7 @@
 #define VXL_DENSITY_THREADS_PER_SM 2048
 #endif
 #ifndef VXL_FORCE_THREADS_PER_SM
-#define VXL_FORCE_THREADS_PER_SM 1024
+#define VXL_FORCE_THREADS_PER_SM 1280
 #endif
 
 // 1: the half-culled walk takes cells with every half reachable as a plain range.
