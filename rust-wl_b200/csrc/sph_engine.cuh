@@ -107,6 +107,7 @@ namespace {
 constexpr int kScanTile = 2048;
 constexpr int kScanThreads = 256;
 constexpr int kCanonSmem = 1024;
+constexpr int kCanonWindow = kCanonSmem / 2;  // window path: keys + segment table in one warp's buffer
 constexpr int kBGatherCap = 64;
 
 // Block-level ordered-uint min/max of (x, y, z), one atomic per component into acc.
@@ -615,6 +616,39 @@ __global__ void k_e_canon(const uint2* __restrict__ items, const uint32_t* __res
     if (c < total) {
       b = start[c];
       n = start[c + 1] - b;
+    }
+    // Window path: the entries of these 32 cells are contiguous; when they are few and every
+    // cell is small, rank and gather them 32 at a time across cell boundaries, with the
+    // keys and a per-entry (cell start, cell size) table in shared memory.
+    const uint32_t wb = __shfl_sync(0xffffffffu, b, 0);
+    uint32_t we = c < total ? b + n : 0u;
+    uint32_t maxn = n;
+    for (int off = 16; off > 0; off >>= 1) {
+      we = max(we, __shfl_xor_sync(0xffffffffu, we, off));
+      maxn = max(maxn, __shfl_xor_sync(0xffffffffu, maxn, off));
+    }
+    if (maxn <= 32 && we - wb <= (uint32_t)kCanonWindow) {
+      uint32_t* wkeys = skeys[wib];
+      uint32_t* wseg = skeys[wib] + kCanonWindow;
+      const uint32_t rel = b - wb;
+      for (uint32_t q = 0; q < n; ++q) wseg[rel + q] = (rel << 6) | n;  // n <= 32 < 64
+      const uint32_t T = we - wb;
+      for (uint32_t e = lane; e < T; e += 32) wkeys[e] = items[wb + e].x;
+      __syncwarp();
+      for (uint32_t e = lane; e < T; e += 32) {
+        const uint2 it = items[wb + e];
+        const uint32_t seg = wseg[e];
+        const uint32_t s0 = seg >> 6, sn = seg & 63u;
+        uint32_t rank = 0;
+        for (uint32_t j = 0; j < sn; ++j) rank += (wkeys[s0 + j] < it.x) ? 1u : 0u;
+        const uint32_t dst = wb + s0 + rank;
+        pos_out[dst] = pos_in[it.y];
+        vel_out[dst] = vel_in[it.y];
+        orig[dst] = it.x;
+        slot_of[it.x] = dst;
+      }
+      __syncwarp();
+      continue;
     }
     uint32_t mask = __ballot_sync(0xffffffffu, n > 0);
     while (mask) {
