@@ -1063,7 +1063,9 @@ __global__ void __launch_bounds__(128) k_e_bforce(
       const float mj = -pj.w;
       uint32_t cx, cy, cz;
       bin_of(g, pj.x, pj.y, pj.z, cx, cy, cz);
-      uint32_t key[kBGatherCap] = {};
+      // insertion-sort buffer: only entries [0, n) are ever read (not zero-filled: that
+      // cost 64 local stores per particle)
+      uint32_t key[kBGatherCap];
       uint32_t slot[kBGatherCap];
       int n = 0;
       bool overflow = false;
@@ -1071,10 +1073,11 @@ __global__ void __launch_bounds__(128) k_e_bforce(
         if (n < kBGatherCap) {
           const uint32_t o = orig[ii];
           int q = n++;
-          while (q > 0 && key[q - 1] > o) {
-            key[q] = key[q - 1];
+          for (; q > 0; --q) {
+            const uint32_t kq = key[q - 1];
+            if (kq <= o) break;
+            key[q] = kq;
             slot[q] = slot[q - 1];
-            --q;
           }
           key[q] = o;
           slot[q] = ii;
