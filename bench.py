@@ -346,31 +346,41 @@ def run_ours(args) -> None:
     sb["achieved_gbs"] = sb["bytes"] / (sb["ms"] / 1e3) / 1e9
     sb["frac"] = sb["achieved_gbs"] / peak
 
-    # e2e: through the C ABI with pinned host buffers: H2D state, one tick, D2H state
+    # e2e: the drop-in call pattern of FluidStepper::step through the C ABI, pinned host
+    # buffers. The backend owns the fluid state, so a step uploads the boundary segment
+    # (the reference's per-tick upload, crates/vxl-phys-gpu/src/pipeline/coupling.rs:20-50),
+    # steps one tick (the per-body reactions come back) and reads every position back (what
+    # a renderer or the host-side copy takes).
+    nf, nb = spec.n_fluid, spec.n_boundary
+    pin_bp = torch.empty((max(nb, 1), 3), dtype=torch.float32, pin_memory=True).numpy()[:nb]
+    pin_bv = torch.empty((max(nb, 1), 3), dtype=torch.float32, pin_memory=True).numpy()[:nb]
     pin_p = torch.empty((spec.n_total, 3), dtype=torch.float32, pin_memory=True).numpy()
-    pin_v = torch.empty((spec.n_total, 3), dtype=torch.float32, pin_memory=True).numpy()
+    pin_bp[:] = spec.pos[nf:]
+    pin_bv[:] = spec.vel[nf:]
     scene.set_profile(False)
-    pin_p[:] = spec.pos
-    pin_v[:] = spec.vel
-    for _ in range(2):
-        scene.write_state(pin_p, pin_v)
+
+    def e2e_step():
+        if nb:
+            scene.upload_boundary(pin_bp, pin_bv)
         scene.step_tick(dt_tick, spec.spans)
-        scene.read_state(out=(pin_p, pin_v))
-    # the timed steps start from the initial state too (the device-timed ticks' states)
-    pin_p[:] = spec.pos
-    pin_v[:] = spec.vel
+        vxl_sph._check(scene.lib.vxl_sph_read_state(scene._h, vxl_sph._fptr(pin_p), None))
+
+    scene.write_state(spec.pos, spec.vel)
+    for _ in range(2):
+        e2e_step()
+    scene.write_state(spec.pos, spec.vel)  # the timed steps start from the initial state too
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        scene.write_state(pin_p, pin_v)
-        scene.step_tick(dt_tick, spec.spans)
-        scene.read_state(out=(pin_p, pin_v))
+        e2e_step()
     e2e_s = placement.max_over_ranks(time.perf_counter() - t0, dist, f"cuda:{local}")
-    e2e = {"value": updates / e2e_s, "unit": UNIT, "h2d_bytes_per_step": spec.n_total * 24,
-           "d2h_bytes_per_step": spec.n_total * 24,
-           "api": "vxl_sph_write_state + vxl_sph_step_tick + vxl_sph_read_state, pinned host buffers"}
+    nspans = len(spec.spans)
+    e2e = {"value": updates / e2e_s, "unit": UNIT, "h2d_bytes_per_step": nb * 24 + nspans * 24,
+           "d2h_bytes_per_step": spec.n_total * 12 + nspans * 28,
+           "api": "vxl_sph_upload_boundary (boundary segment) + vxl_sph_step_tick (spans in, reactions out) + "
+                  "vxl_sph_read_state (positions), pinned host buffers: the FluidStepper::step pattern"}
 
     mix = {}
     if world == 1 and not args.no_mix:
