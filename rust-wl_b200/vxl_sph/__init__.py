@@ -722,3 +722,9 @@ class GpuFluidStepper:
     def gather_walls(self, h: float, providers) -> None:
         # Provider walls are not part of this path (the configs use Akinci walls).
         return None
+
+
+# launch shape and autotuner on the plain handle too (same C entry points as the batch's)
+Scene.set_tuning = Batch.set_tuning
+Scene.tuning = Batch.tuning
+Scene.autotune = Batch.autotune
