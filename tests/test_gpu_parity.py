@@ -457,3 +457,16 @@ def test_deferred_readback_and_vxld_dump(vxl, oracle_mod, tmp_path):
             assert fr["tick"] == t
             assert_bits(fr["systems"][0], o.read_f32()["pos"][:spec.n_fluid], f"frame at tick {t}")
     o.close()
+
+
+def test_canon_window_at_its_limit(vxl, oracle_mod):
+    """Sixteen particles per cell (two interleaved lattices at spacing h/2): 32 consecutive
+    cells hold exactly 512 entries, the limit of the sort's window path, and cells at the
+    block's edges fall back to the per-cell path; the table, fields and state stay bit-exact."""
+    from vxl_sph import scenes
+    s = 0.025
+    a = scenes.fluid_block((0.0, 0.0, 0.0), (12, 10, 32), s)
+    b = (a + F32(0.3 * s)).astype(F32)
+    fluid = np.concatenate([a, b]).astype(F32)
+    spec = _custom(vxl, fluid, h=2 * s, spacing=s)
+    _run_both(vxl, oracle_mod, spec, substeps=2)
