@@ -723,7 +723,8 @@ vxl_status Engine::stage_spans() {
       sp.push_back(SpanDev{s.body, s.origin[0], s.origin[1], s.origin[2], gs, ge});
       span_scene_.push_back(q);
       first.push_back((uint32_t)ch.size());
-      for (uint32_t b = gs; b < ge; b += kReactChunk) ch.push_back(SpanChunk{idx, b, std::min(ge, b + kReactChunk), 0u});
+      if (ge - gs > kReactExactSpan)  // larger spans take the two-level reduction
+        for (uint32_t b = gs; b < ge; b += kReactChunk) ch.push_back(SpanChunk{idx, b, std::min(ge, b + kReactChunk), 0u});
     }
   first.push_back((uint32_t)ch.size());
   const uint32_t ns = (uint32_t)sp.size(), nc = (uint32_t)ch.size();
@@ -896,7 +897,7 @@ void Engine::enqueue_substep(bool with_reactions) {
   // Reaction branch on the side stream: it reads only the sorted buffer, the densities and
   // the lists, so it runs beside the force pass (which writes the other buffer).
   const bool bforce = nb_total > 0 && ((with_reactions && nspans_ > 0) || rec);
-  const bool react = with_reactions && nspans_ > 0 && nchunks_ > 0;
+  const bool react = with_reactions && nspans_ > 0;
   if (bforce || react) {
     cudaEventRecord(ev_fork_, st);
     cudaStreamWaitEvent(side_, ev_fork_, 0);
@@ -906,11 +907,14 @@ void Engine::enqueue_substep(bool with_reactions) {
                                                   stride, sc_d_, slot_of_, tiles_d_ + ntiles_, nbtiles_, ctl_d_,
                                                   (float4*)bforce_));
     if (react) {
-      LAUNCH_ON(KID_REACT_CHUNKS, side_,
+      if (nchunks_)
+        LAUNCH_ON(KID_REACT_CHUNKS, side_,
                 k_react_chunks<<<nchunks_, kReactThreads, 0, side_>>>((const float4*)bforce_, (const float4*)bpos_,
                                                                       spans_d_, chunks_d_, ctl_d_, react_partial_));
       LAUNCH_ON(KID_REACT_SPANS, side_,
-                k_react_spans<<<blocks_for(nspans_, 64), 64, 0, side_>>>(react_partial_, chunk_first_d_, ctl_d_,
+                k_react_spans<<<blocks_for(nspans_, 64), 64, 0, side_>>>(react_partial_, chunk_first_d_,
+                                                                         (const float4*)bforce_, (const float4*)bpos_,
+                                                                         spans_d_, ctl_d_,
                                                                          breact_d_, nspans_));
     }
     cudaEventRecord(ev_join_, side_);

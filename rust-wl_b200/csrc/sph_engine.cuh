@@ -87,6 +87,9 @@ struct SpanChunk {
 };
 
 constexpr uint32_t kReactChunk = 4096;
+// Spans of at most this many particles (bodies, as opposed to tank walls) are summed by one
+// thread in index order: the reference's sum, bit for bit.
+constexpr uint32_t kReactExactSpan = 8192;
 constexpr int kReactThreads = 256;
 
 // Engine-wide control block.
@@ -1141,10 +1144,12 @@ __global__ void __launch_bounds__(128) k_e_bforce(
 }
 
 // Per-span force and torque about the body origin (fluid_boundary.rs:10-28), added to
-// the tick accumulator. Fixed-shape two-level reduction, deterministic run to run:
-// level 1, one block per chunk of <= kReactChunk consecutive particles of a span (thread
-// t sums t, t + blockDim, ... in order, then a fixed tree); level 2, one thread per span
-// adds its chunk partials in chunk order. Span ranges are global reference indices.
+// the tick accumulator. A span of at most kReactExactSpan particles is summed by one thread
+// in index order (the reference's sum, bit for bit). Larger spans (tank walls) take a
+// fixed-shape two-level reduction, deterministic run to run: level 1, one block per chunk of
+// <= kReactChunk consecutive particles (thread t sums t, t + blockDim, ... in order, then a
+// fixed tree); level 2, the span's thread adds its chunk partials in chunk order. Span
+// ranges are global reference indices.
 
 __global__ void __launch_bounds__(kReactThreads) k_react_chunks(const float4* __restrict__ bforce,
                                                                 const float4* __restrict__ bpos,
@@ -1178,15 +1183,33 @@ __global__ void __launch_bounds__(kReactThreads) k_react_chunks(const float4* __
   if (threadIdx.x < 6) partial[6 * blockIdx.x + threadIdx.x] = sh[threadIdx.x][0];
 }
 
-// chunk_first[q] .. chunk_first[q + 1]: the chunks of span q (in order).
+// chunk_first[q] .. chunk_first[q + 1]: the chunks of span q (in order; none for a span
+// summed exactly).
 __global__ void k_react_spans(const float* __restrict__ partial, const uint32_t* __restrict__ chunk_first,
-                              const EngineCtl* __restrict__ ctl, float* __restrict__ breact, uint32_t nspans) {
+                              const float4* __restrict__ bforce, const float4* __restrict__ bpos,
+                              const SpanDev* __restrict__ spans, const EngineCtl* __restrict__ ctl,
+                              float* __restrict__ breact, uint32_t nspans) {
   if (ctl->err & kErrCellCap) return;
   const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= nspans) return;
   float f[6] = {0, 0, 0, 0, 0, 0};
-  for (uint32_t c = chunk_first[q]; c < chunk_first[q + 1]; ++c)
-    for (int a = 0; a < 6; ++a) f[a] = f[a] + partial[6 * c + a];
+  const SpanDev sp = spans[q];
+  if (sp.end - sp.start <= kReactExactSpan) {
+    for (uint32_t kk = sp.start; kk < sp.end; ++kk) {
+      const float4 fk = bforce[kk];
+      const float4 p = bpos[kk];
+      const float rx = p.x - sp.ox, ry = p.y - sp.oy, rz = p.z - sp.oz;
+      f[0] = f[0] + fk.x;
+      f[1] = f[1] + fk.y;
+      f[2] = f[2] + fk.z;
+      f[3] = f[3] + (ry * fk.z - rz * fk.y);
+      f[4] = f[4] + (rz * fk.x - rx * fk.z);
+      f[5] = f[5] + (rx * fk.y - ry * fk.x);
+    }
+  } else {
+    for (uint32_t c = chunk_first[q]; c < chunk_first[q + 1]; ++c)
+      for (int a = 0; a < 6; ++a) f[a] = f[a] + partial[6 * c + a];
+  }
   for (int a = 0; a < 6; ++a) breact[6 * q + a] = breact[6 * q + a] + f[a];
 }
 
