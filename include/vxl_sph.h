@@ -312,6 +312,34 @@ vxl_status vxl_sph_set_body_lattice(vxl_sph_handle* h, uint32_t scene, const flo
 vxl_status vxl_sph_set_body_poses(vxl_sph_handle* h, uint32_t scene, const vxl_sph_body_pose* poses,
                                   uint32_t nbodies);
 
+/* ------------------------------------------------------------------ coupling loop on the device
+ * The facade's fluid coupling (crates/vxl-phys/src/world_step.rs) without its rigid contact
+ * solver: the scene's lattice bodies (vxl_sph_set_body_lattice) become rigid bodies that stay
+ * on the device. Each vxl_sph_step_coupled runs `rigid_substeps` rigid substeps per body in the
+ * reference's order — the gravity field adds m g, the fluid reaction pass adds the previous
+ * tick's tick-averaged reaction of the body's span, Integrator::integrate_velocities (speed
+ * clamps) and integrate_positions (crates/vxl-phys-integrate/src/lib.rs:18-60) — then rebuilds
+ * the boundary segment from the new poses and steps one fluid tick, whose reactions drive the
+ * next call. Spans (vxl_sph_set_spans_scene) are matched to bodies by body id and take the
+ * body's position as the torque origin. Bodies are not kept out of walls or each other: that
+ * is the contact solver's work, which this library does not do. */
+typedef struct vxl_sph_rigid_body {
+  vxl_sph_body_pose pose;       /* position (= lattice origin), rotation, velocities */
+  float inv_mass;               /* 1 / mass (mass.rs: box m = rho * 8 hx hy hz) */
+  float local_inv_inertia[3];   /* body-frame inverse inertia diagonal */
+  uint32_t dynamic;             /* 0: static (never moves), 1: dynamic */
+} vxl_sph_rigid_body;
+
+/* One rigid body per lattice body, in lattice body order. */
+vxl_status vxl_sph_set_rigid_bodies(vxl_sph_handle* h, uint32_t scene, const vxl_sph_rigid_body* bodies,
+                                    uint32_t n);
+/* One coupled tick of every scene with rigid bodies (synchronous; reactions as for
+ * vxl_sph_step_tick, nspans of them in span order). */
+vxl_status vxl_sph_step_coupled(vxl_sph_handle* h, float dt_tick, uint32_t rigid_substeps, const float gravity[3],
+                                float max_linear, float max_angular, vxl_sph_reaction* out_reactions,
+                                uint32_t nspans);
+vxl_status vxl_sph_read_rigid_bodies(vxl_sph_handle* h, uint32_t scene, vxl_sph_rigid_body* out, uint32_t n);
+
 /* ------------------------------------------------------------------ served form
  * A request loop (the served workload): scene-step requests are submitted at any time,
  * admitted while their device footprint fits an HBM budget, stepped together with

@@ -97,6 +97,8 @@ def load() -> C.CDLL:
                                      _FP, C.POINTER(C.c_uint64)]),
         "orc_boundary_self_sum": (C.c_float, [_FP, C.c_uint64, C.c_float]),
         "orc_grid_probe_hash": (C.c_uint64, [C.c_uint64, C.c_uint64, C.c_uint32]),
+        "orc_rigid_step": (None, [_FP, C.c_uint32, _FP, _FP, C.c_float, C.c_uint32, C.c_float, C.c_float]),
+        "orc_box_mass_props": (None, [_FP, C.c_float, _FP, _FP]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -349,3 +351,25 @@ def table_hash(start, items, np_count: int) -> int:
         for v in seq:
             h = ((h ^ int(v)) * prime) & mask
     return h
+
+
+def rigid_step(states: np.ndarray, reactions: np.ndarray, gravity, dt: float, substeps: int, max_linear: float,
+               max_angular: float) -> None:
+    """Rigid substeps of the coupling loop (no contacts) on (n, 18) float32 states in place:
+    pos, rot xyzw, linvel, angvel, inv_mass, local inverse inertia, dynamic; reactions (n, 6)."""
+    lib = load()
+    st = np.ascontiguousarray(states, np.float32)
+    rx = np.ascontiguousarray(reactions, np.float32)
+    g = np.ascontiguousarray(gravity, np.float32)
+    lib.orc_rigid_step(_f(st), st.shape[0], _f(rx), _f(g), float(dt), int(substeps), float(max_linear),
+                       float(max_angular))
+    states[...] = st
+
+
+def box_mass_props(half, density: float):
+    lib = load()
+    h = np.ascontiguousarray(half, np.float32)
+    im = C.c_float()
+    ii = np.zeros(3, np.float32)
+    lib.orc_box_mass_props(_f(h), float(density), C.byref(im), _f(ii))
+    return np.float32(im.value), ii

@@ -395,4 +395,39 @@ uint64_t orc_grid_probe_hash(uint64_t n, uint64_t max_bins, uint32_t threads) {
   return table_hash(g.start, g.items, total, np);
 }
 
+// Rigid bodies of the coupling loop (no contacts), float32: `substeps` rigid substeps of
+// dt each, every body receiving its reaction (force, torque; 6 floats per body) each
+// substep. bodies: pos[3], rot[4], linvel[3], angvel[3], inv_mass, local_inv_inertia[3],
+// dynamic (as a float 0/1) — 18 floats per body, updated in place.
+void orc_rigid_step(float* bodies, uint32_t n, const float* reactions, const float g[3], float dt, uint32_t substeps,
+                    float max_linear, float max_angular) {
+  for (uint32_t i = 0; i < n; ++i) {
+    float* b = bodies + 18 * i;
+    RigidBody<float> rb;
+    rb.pos = V3<float>(b[0], b[1], b[2]);
+    rb.rot = Quat<float>(b[3], b[4], b[5], b[6]);
+    rb.linvel = V3<float>(b[7], b[8], b[9]);
+    rb.angvel = V3<float>(b[10], b[11], b[12]);
+    rb.inv_mass = b[13];
+    rb.local_inv_inertia = V3<float>(b[14], b[15], b[16]);
+    rb.dynamic = b[17] != 0.0f;
+    const float* r = reactions + 6 * i;
+    for (uint32_t k = 0; k < substeps; ++k)
+      rigid_substep(rb, V3<float>(g[0], g[1], g[2]), V3<float>(r[0], r[1], r[2]), V3<float>(r[3], r[4], r[5]), dt,
+                    max_linear, max_angular);
+    const float out[17] = {rb.pos.x, rb.pos.y, rb.pos.z, rb.rot.x, rb.rot.y, rb.rot.z, rb.rot.w,
+                           rb.linvel.x, rb.linvel.y, rb.linvel.z, rb.angvel.x, rb.angvel.y, rb.angvel.z,
+                           rb.inv_mass, rb.local_inv_inertia.x, rb.local_inv_inertia.y, rb.local_inv_inertia.z};
+    for (int k = 0; k < 17; ++k) b[k] = out[k];
+  }
+}
+
+void orc_box_mass_props(const float half[3], float density, float* inv_mass, float local_inv_inertia[3]) {
+  V3<float> d;
+  box_mass_props(V3<float>(half[0], half[1], half[2]), density, *inv_mass, d);
+  local_inv_inertia[0] = d.x;
+  local_inv_inertia[1] = d.y;
+  local_inv_inertia[2] = d.z;
+}
+
 }  // extern "C"

@@ -67,6 +67,95 @@ struct Quat {
   }
 };
 
+// ---------------------------------------------------------------- rigid bodies (coupling loop)
+// A dynamic body of the facade's coupling loop without contacts: pose, velocities and mass
+// properties (crates/vxl-phys-core/src/body.rs).
+template <class R>
+struct RigidBody {
+  V3<R> pos;
+  Quat<R> rot;
+  V3<R> linvel, angvel;
+  R inv_mass;
+  V3<R> local_inv_inertia;
+  bool dynamic;
+};
+
+// crates/vxl-phys-core/src/mass.rs:35-48 (Shape::Box): m = rho ex ey ez, I = m/12 (..).
+template <class R>
+inline void box_mass_props(const V3<R>& half, R density, R& inv_mass, V3<R>& local_inv_inertia) {
+  if (!(density > R(0))) density = R(1);
+  R ex = R(2) * half.x, ey = R(2) * half.y, ez = R(2) * half.z;
+  R m = density * ex * ey * ez;
+  R ix = m / R(12) * (ey * ey + ez * ez);
+  R iy = m / R(12) * (ex * ex + ez * ez);
+  R iz = m / R(12) * (ex * ex + ey * ey);
+  inv_mass = R(1) / m;
+  local_inv_inertia = V3<R>(R(1) / ix, R(1) / iy, R(1) / iz);
+}
+
+// crates/vxl-phys-core/src/math.rs:241-252 (Hamilton product a * b).
+template <class R>
+inline Quat<R> qmul(const Quat<R>& a, const Quat<R>& b) {
+  return Quat<R>(a.w * b.x + a.x * b.w + a.y * b.z - a.z * b.y, a.w * b.y - a.x * b.z + a.y * b.w + a.z * b.x,
+                 a.w * b.z + a.x * b.y - a.y * b.x + a.z * b.w, a.w * b.w - a.x * b.x - a.y * b.y - a.z * b.z);
+}
+
+// crates/vxl-phys-core/src/math.rs:216-238 (normalize; integrate_angular with world w).
+template <class R>
+inline Quat<R> integrate_angular(const Quat<R>& q, const V3<R>& w, R dt) {
+  Quat<R> dq = qmul(Quat<R>(w.x, w.y, w.z, R(0)), q);
+  R hd = R(0.5) * dt;
+  Quat<R> r(q.x + dq.x * hd, q.y + dq.y * hd, q.z + dq.z * hd, q.w + dq.w * hd);
+  R len2 = r.x * r.x + r.y * r.y + r.z * r.z + r.w * r.w;
+  if (len2 > R(1e-16)) {
+    R inv = R(1) / std::sqrt(len2);
+    return Quat<R>(r.x * inv, r.y * inv, r.z * inv, r.w * inv);
+  }
+  return Quat<R>();
+}
+
+// crates/vxl-phys-core/src/body.rs:172-176 with Mat3::from_quat / transpose_mul_vec3 /
+// mul_vec3 (math.rs:275-311): R diag(d) R^T l.
+template <class R>
+inline V3<R> world_inv_inertia(const Quat<R>& q, const V3<R>& d, const V3<R>& l) {
+  R xx = q.x * q.x, yy = q.y * q.y, zz = q.z * q.z;
+  R xy = q.x * q.y, xz = q.x * q.z, yz = q.y * q.z;
+  R wx = q.w * q.x, wy = q.w * q.y, wz = q.w * q.z;
+  R m[3][3] = {{R(1) - R(2) * (yy + zz), R(2) * (xy - wz), R(2) * (xz + wy)},
+               {R(2) * (xy + wz), R(1) - R(2) * (xx + zz), R(2) * (yz - wx)},
+               {R(2) * (xz - wy), R(2) * (yz + wx), R(1) - R(2) * (xx + yy)}};
+  V3<R> lt(m[0][0] * l.x + m[1][0] * l.y + m[2][0] * l.z, m[0][1] * l.x + m[1][1] * l.y + m[2][1] * l.z,
+           m[0][2] * l.x + m[1][2] * l.y + m[2][2] * l.z);
+  V3<R> v(lt.x * d.x, lt.y * d.y, lt.z * d.z);
+  return V3<R>(m[0][0] * v.x + m[0][1] * v.y + m[0][2] * v.z, m[1][0] * v.x + m[1][1] * v.y + m[1][2] * v.z,
+               m[2][0] * v.x + m[2][1] * v.y + m[2][2] * v.z);
+}
+
+// One rigid substep of a dynamic, awake body with no contacts, as the facade runs it
+// (crates/vxl-phys/src/world_step.rs:240-330): the gravity field adds g * (1 / inv_mass)
+// (crates/vxl-phys-field/src/lib.rs:22-31), the fluid reaction pass adds the tick-averaged
+// reaction (world_step.rs:235-255, coupling.rs:52-57), Integrator::integrate_velocities with
+// gravity ZERO and its clamps, then integrate_positions (crates/vxl-phys-integrate/src/lib.rs:18-60).
+template <class R>
+inline void rigid_substep(RigidBody<R>& b, const V3<R>& g, const V3<R>& rf, const V3<R>& rt, R dt, R max_linear,
+                          R max_angular) {
+  if (!b.dynamic) return;
+  V3<R> force = V3<R>() + g * (R(1) / b.inv_mass);
+  V3<R> torque;
+  force += rf;
+  torque += rt;
+  V3<R> accel = V3<R>() + force * b.inv_mass;
+  b.linvel += accel * dt;
+  V3<R> ang = world_inv_inertia(b.rot, b.local_inv_inertia, torque);
+  b.angvel = b.angvel + ang * dt;
+  R sp = b.linvel.length();
+  if (sp > max_linear) b.linvel = b.linvel * (max_linear / sp);
+  R ws = b.angvel.length();
+  if (ws > max_angular) b.angvel = b.angvel * (max_angular / ws);
+  b.pos = b.pos + b.linvel * dt;
+  b.rot = integrate_angular(b.rot, b.angvel, dt);
+}
+
 // Rust `f32::powi` lowers to repeated squaring (LLVM ExpandPowI / compiler-rt
 // __powisf2); both give r = a^(bits) multiplied in this order.
 template <class R>

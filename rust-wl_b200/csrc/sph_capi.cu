@@ -181,6 +181,43 @@ vxl_status vxl_sph_take_state(vxl_sph_handle* h, float* pos_xyz, uint64_t n) {
   }
 }
 
+vxl_status vxl_sph_set_rigid_bodies(vxl_sph_handle* h, uint32_t scene, const vxl_sph_rigid_body* bodies,
+                                    uint32_t n) {
+  HANDLE_OR_FAIL(h);
+  try {
+    return h->e->set_rigid_bodies(scene, bodies, n);
+  } catch (...) {
+    return set_error(VXL_PANIC_CAUGHT, "exception in vxl_sph_set_rigid_bodies");
+  }
+}
+
+vxl_status vxl_sph_step_coupled(vxl_sph_handle* h, float dt_tick, uint32_t rigid_substeps, const float gravity[3],
+                                float max_linear, float max_angular, vxl_sph_reaction* out_reactions,
+                                uint32_t nspans) {
+  HANDLE_OR_FAIL(h);
+  if (nspans > 0 && !out_reactions) return set_error(VXL_NULL_POINTER, "out_reactions is NULL with nspans > 0");
+  try {
+    vxl_status s = h->e->step_coupled_async(dt_tick, rigid_substeps, gravity, max_linear, max_angular);
+    if (s != VXL_OK) return s;
+    s = h->e->sync(&h->last);
+    if (s != VXL_OK) return s;
+    if (nspans > h->last.size()) return set_error(VXL_SIZE_MISMATCH, "more reactions requested than spans stepped");
+    for (uint32_t q = 0; q < nspans; ++q) out_reactions[q] = h->last[q];
+    return VXL_OK;
+  } catch (...) {
+    return set_error(VXL_PANIC_CAUGHT, "exception in vxl_sph_step_coupled");
+  }
+}
+
+vxl_status vxl_sph_read_rigid_bodies(vxl_sph_handle* h, uint32_t scene, vxl_sph_rigid_body* out, uint32_t n) {
+  HANDLE_OR_FAIL(h);
+  try {
+    return h->e->read_rigid_bodies(scene, out, n);
+  } catch (...) {
+    return set_error(VXL_PANIC_CAUGHT, "exception in vxl_sph_read_rigid_bodies");
+  }
+}
+
 vxl_status vxl_sph_set_body_lattice(vxl_sph_handle* h, uint32_t scene, const float* local_xyz,
                                     const uint32_t* body_index, uint64_t nb, uint32_t nbodies) {
   HANDLE_OR_FAIL(h);

@@ -205,6 +205,8 @@ void Engine::free_all() {
   snap_h_ = nullptr;
   if (ev_snap_) cudaEventDestroy(ev_snap_);
   ev_snap_ = nullptr;
+  if (rb_d_) cudaFree(rb_d_);
+  rb_d_ = nullptr;
   if (blocal_) cudaFree(blocal_);
   if (poses_d_) cudaFree(poses_d_);
   blocal_ = nullptr;
@@ -381,6 +383,10 @@ vxl_status Engine::remove_scenes(const std::vector<uint32_t>& indices) {
   CU(cudaSetDevice(device_));
   prof_collect();
   CU(cudaStreamSynchronize(stream_));
+  {
+    vxl_status pst = rb_pull();  // coupled bodies' evolved states, in the old layout
+    if (pst != VXL_OK) return pst;
+  }
   std::vector<bool> drop(scenes_.size(), false);
   for (uint32_t i : indices)
     if (i < scenes_.size()) drop[i] = true;
@@ -429,6 +435,14 @@ vxl_status Engine::remove_scenes(const std::vector<uint32_t>& indices) {
   scenes_.swap(keep);
   spans_local_.swap(keep_spans);
   scene_bodies_.swap(keep_bodies);
+  if (!rigid_.empty()) {  // coupled bodies follow their scenes
+    std::vector<std::vector<vxl_sph_rigid_body>> keep_rigid;
+    for (uint32_t q = 0; q < drop.size(); ++q)
+      if (!drop[q]) keep_rigid.push_back(q < rigid_.size() ? rigid_[q] : std::vector<vxl_sph_rigid_body>());
+    rigid_.swap(keep_rigid);
+    rb_dirty_ = true;
+    rb_have_reaction_ = false;
+  }
   used_ = next;
   spans_dirty_ = true;
   vxl_status s = push_scene_records({});
@@ -482,6 +496,151 @@ vxl_status Engine::set_body_lattice(uint32_t q, const float* local_xyz, const ui
   CU(cudaStreamSynchronize(stream_));
   if (scene_bodies_.size() < scenes_.size()) scene_bodies_.resize(scenes_.size(), 0);
   scene_bodies_[q] = nbodies;
+  return VXL_OK;
+}
+
+// ---------------------------------------------------------------- coupled rigid bodies
+
+static RigidBodyDev to_dev(const vxl_sph_rigid_body& b) {
+  const vxl_sph_body_pose& p = b.pose;
+  return RigidBodyDev{p.pos[0], p.pos[1], p.pos[2], p.rot[0], p.rot[1], p.rot[2], p.rot[3],
+                      p.linvel[0], p.linvel[1], p.linvel[2], p.angvel[0], p.angvel[1], p.angvel[2],
+                      b.inv_mass, b.local_inv_inertia[0], b.local_inv_inertia[1], b.local_inv_inertia[2],
+                      b.dynamic ? 1u : 0u, ~0u};
+}
+
+static void from_dev(const RigidBodyDev& d, vxl_sph_rigid_body& b) {
+  vxl_sph_body_pose& p = b.pose;
+  p.pos[0] = d.px; p.pos[1] = d.py; p.pos[2] = d.pz;
+  p.rot[0] = d.qx; p.rot[1] = d.qy; p.rot[2] = d.qz; p.rot[3] = d.qw;
+  p.linvel[0] = d.vx; p.linvel[1] = d.vy; p.linvel[2] = d.vz;
+  p.angvel[0] = d.wx; p.angvel[1] = d.wy; p.angvel[2] = d.wz;
+}
+
+// Bring the device's evolved bodies back into the host copies (before the device array
+// is rebuilt from them).
+vxl_status Engine::rb_pull() {
+  if (!rb_live_ || !rb_d_ || rb_n_ == 0) return VXL_OK;
+  std::vector<RigidBodyDev> h(rb_n_);
+  CU(cudaMemcpyAsync(h.data(), rb_d_, rb_n_ * sizeof(RigidBodyDev), cudaMemcpyDeviceToHost, stream_));
+  CU(cudaStreamSynchronize(stream_));
+  for (uint32_t q = 0; q < rigid_.size() && q < rb_off_.size(); ++q)
+    for (uint32_t b = 0; b < rigid_[q].size(); ++b) from_dev(h[rb_off_[q] + b], rigid_[q][b]);
+  rb_live_ = false;
+  return VXL_OK;
+}
+
+void Engine::rb_layout() {
+  rb_off_.assign(scenes_.size(), 0);
+  uint32_t n = 0;
+  for (uint32_t q = 0; q < scenes_.size(); ++q) {
+    rb_off_[q] = n;
+    if (q < rigid_.size()) n += (uint32_t)rigid_[q].size();
+  }
+  rb_n_ = n;
+}
+
+vxl_status Engine::set_rigid_bodies(uint32_t q, const vxl_sph_rigid_body* bodies, uint32_t n) {
+  if (q >= scenes_.size()) return set_error(VXL_INVALID_ARGUMENT, "scene index out of range");
+  if (n && !bodies) return set_error(VXL_NULL_POINTER, "bodies is NULL");
+  if (q >= scene_bodies_.size() || scene_bodies_[q] == 0)
+    return set_error(VXL_NOT_READY, "set the body lattice (vxl_sph_set_body_lattice) first");
+  if (n != scene_bodies_[q]) return set_error(VXL_SIZE_MISMATCH, "one rigid body per lattice body");
+  for (uint32_t b = 0; b < n; ++b)
+    if (bodies[b].dynamic && !(bodies[b].inv_mass > 0.0f))
+      return set_error(VXL_INVALID_ARGUMENT, "a dynamic body needs inv_mass > 0");
+  CU(cudaSetDevice(device_));
+  prof_collect();
+  vxl_status st = rb_pull();  // keep the other scenes' evolved bodies
+  if (st != VXL_OK) return st;
+  if (rigid_.size() < scenes_.size()) rigid_.resize(scenes_.size());
+  rigid_[q].assign(bodies, bodies + n);
+  rb_dirty_ = true;
+  rb_have_reaction_ = false;
+  spans_dirty_ = true;  // spans map to the bodies by id
+  return VXL_OK;
+}
+
+vxl_status Engine::step_coupled_async(float dt_tick, uint32_t rigid_substeps, const float g[3], float max_linear,
+                                      float max_angular) {
+  if (!(dt_tick > 0.0f) || !std::isfinite(dt_tick)) return set_error(VXL_INVALID_ARGUMENT, "dt_tick must be > 0");
+  if (rigid_substeps == 0) return set_error(VXL_INVALID_ARGUMENT, "rigid_substeps must be > 0");
+  if (!g) return set_error(VXL_NULL_POINTER, "gravity is NULL");
+  CU(cudaSetDevice(device_));
+  bool any = false;
+  for (auto& v : rigid_) any = any || !v.empty();
+  if (!any) return set_error(VXL_NOT_READY, "no rigid bodies set (vxl_sph_set_rigid_bodies)");
+  prof_collect();
+  if (spans_dirty_ || rb_dirty_) {
+    vxl_status st = rb_pull();
+    if (st != VXL_OK) return st;
+    rb_layout();
+    st = stage_spans();  // maps spans to rigid bodies (needs rb_off_)
+    if (st != VXL_OK) return st;
+    std::vector<RigidBodyDev> h(rb_n_);
+    for (uint32_t q = 0; q < rigid_.size(); ++q)
+      for (uint32_t b = 0; b < rigid_[q].size(); ++b) h[rb_off_[q] + b] = to_dev(rigid_[q][b]);
+    for (uint32_t k = 0; k < nspans_; ++k)
+      if (spans_h_[k].rigid != ~0u) h[spans_h_[k].rigid].span = k;
+    if (rb_n_ > rb_cap_) {
+      if (rb_d_) cudaFree(rb_d_);
+      rb_d_ = nullptr;
+      rb_cap_ = 0;
+      vxl_status s2 = dalloc(&rb_d_, rb_n_);
+      if (s2 != VXL_OK) return s2;
+      rb_cap_ = rb_n_;
+      if (graph_) {  // the reaction kernels read the body array
+        cudaGraphExecDestroy(graph_);
+        graph_ = nullptr;
+      }
+    }
+    CU(cudaMemcpyAsync(rb_d_, h.data(), rb_n_ * sizeof(RigidBodyDev), cudaMemcpyHostToDevice, stream_));
+    CU(cudaStreamSynchronize(stream_));
+    rb_live_ = true;
+    rb_dirty_ = false;
+  }
+  // 1. rigid substeps from the previous coupled tick's reactions
+  const float dt = dt_tick / (float)rigid_substeps;
+  k_rigid_step<<<blocks_for(rb_n_, 64), 64, 0, stream_>>>(rb_d_, rb_n_, breact_d_,
+                                                           (rb_have_reaction_ && breact_d_) ? 1 : 0, g[0], g[1], g[2],
+                                                           dt, rigid_substeps, max_linear, max_angular);
+  CU(cudaGetLastError());
+  // 2. boundary segments from the new poses
+  static const uint32_t init[6] = {0xffffffffu, 0xffffffffu, 0xffffffffu, 0u, 0u, 0u};
+  for (uint32_t q = 0; q < scenes_.size(); ++q) {
+    if (q >= rigid_.size() || rigid_[q].empty() || scenes_[q].nb == 0) continue;
+    const SceneInfo& si = scenes_[q];
+    CU(cudaMemcpyAsync(sc_d_[q].bbox, init, sizeof(init), cudaMemcpyHostToDevice, stream_));
+    k_e_body_rebuild<<<blocks_for(si.nb), kThreads, 0, stream_>>>(blocal_, rb_d_ + rb_off_[q], (float4*)pos_[0],
+                                                                   (float4*)vel_[0], slot_of_, (float4*)bpos_,
+                                                                   sc_d_[q].bbox, si.base, si.nf, si.nb);
+    CU(cudaGetLastError());
+  }
+  // 3. the fluid tick; its tick-averaged reactions drive the next call's rigid substeps
+  vxl_status st = step_tick_async(dt_tick);
+  if (st != VXL_OK) return st;
+  rb_have_reaction_ = nspans_ > 0;
+  return VXL_OK;
+}
+
+vxl_status Engine::read_rigid_bodies(uint32_t q, vxl_sph_rigid_body* out, uint32_t n) {
+  if (q >= scenes_.size()) return set_error(VXL_INVALID_ARGUMENT, "scene index out of range");
+  if (q >= rigid_.size() || rigid_[q].empty()) return set_error(VXL_NOT_READY, "no rigid bodies in this scene");
+  if (n != rigid_[q].size()) return set_error(VXL_SIZE_MISMATCH, "n differs from the scene's rigid bodies");
+  if (!out) return set_error(VXL_NULL_POINTER, "out is NULL");
+  CU(cudaSetDevice(device_));
+  prof_collect();
+  if (rb_live_ && rb_d_) {
+    std::vector<RigidBodyDev> h(n);
+    CU(cudaMemcpyAsync(h.data(), rb_d_ + rb_off_[q], n * sizeof(RigidBodyDev), cudaMemcpyDeviceToHost, stream_));
+    CU(cudaStreamSynchronize(stream_));
+    for (uint32_t b = 0; b < n; ++b) {
+      out[b] = rigid_[q][b];
+      from_dev(h[b], out[b]);
+    }
+  } else {
+    for (uint32_t b = 0; b < n; ++b) out[b] = rigid_[q][b];
+  }
   return VXL_OK;
 }
 
@@ -720,7 +879,14 @@ vxl_status Engine::stage_spans() {
     for (const vxl_sph_span& s : spans_local_[q]) {
       const uint32_t gs = scenes_[q].base + s.start, ge = scenes_[q].base + s.end;
       const uint32_t idx = (uint32_t)sp.size();
-      sp.push_back(SpanDev{s.body, s.origin[0], s.origin[1], s.origin[2], gs, ge});
+      uint32_t rigid = ~0u;  // coupled rigid body of this span (same body id in the same scene)
+      if (q < rigid_.size() && q < rb_off_.size())
+        for (uint32_t b = 0; b < rigid_[q].size(); ++b)
+          if (rigid_[q][b].pose.body == s.body) {
+            rigid = rb_off_[q] + b;
+            break;
+          }
+      sp.push_back(SpanDev{s.body, s.origin[0], s.origin[1], s.origin[2], gs, ge, rigid});
       span_scene_.push_back(q);
       first.push_back((uint32_t)ch.size());
       if (ge - gs > kReactExactSpan)  // larger spans take the two-level reduction
@@ -757,6 +923,8 @@ vxl_status Engine::stage_spans() {
   nspans_ = ns;
   nchunks_ = nc;
   spans_dirty_ = false;
+  rb_dirty_ = true;              // the bodies' span indices follow the staging
+  rb_have_reaction_ = false;     // reactions are indexed by the old staging
   if (graph_) {
     cudaGraphExecDestroy(graph_);
     graph_ = nullptr;
@@ -910,11 +1078,12 @@ void Engine::enqueue_substep(bool with_reactions) {
       if (nchunks_)
         LAUNCH_ON(KID_REACT_CHUNKS, side_,
                 k_react_chunks<<<nchunks_, kReactThreads, 0, side_>>>((const float4*)bforce_, (const float4*)bpos_,
-                                                                      spans_d_, chunks_d_, ctl_d_, react_partial_));
+                                                                      spans_d_, chunks_d_, rb_d_, ctl_d_,
+                                                                      react_partial_));
       LAUNCH_ON(KID_REACT_SPANS, side_,
                 k_react_spans<<<blocks_for(nspans_, 64), 64, 0, side_>>>(react_partial_, chunk_first_d_,
                                                                          (const float4*)bforce_, (const float4*)bpos_,
-                                                                         spans_d_, ctl_d_,
+                                                                         spans_d_, rb_d_, ctl_d_,
                                                                          breact_d_, nspans_));
     }
     cudaEventRecord(ev_join_, side_);

@@ -71,6 +71,18 @@ struct BodyPoseDev {
   float wx, wy, wz;
 };
 
+// A rigid body of the device-side coupling loop: pose and velocities (the BodyPoseDev
+// fields, same names), mass properties, and the global index of the span whose reaction
+// drives it (~0u: none).
+struct RigidBodyDev {
+  float px, py, pz;
+  float qx, qy, qz, qw;
+  float vx, vy, vz;
+  float wx, wy, wz;
+  float inv_mass, iix, iiy, iiz;
+  uint32_t dynamic, span;
+};
+
 struct TileDev {
   uint32_t scene, first, count, pad;
 };
@@ -80,6 +92,7 @@ struct SpanDev {
   uint32_t body;
   float ox, oy, oz;
   uint32_t start, end;
+  uint32_t rigid;  // coupled rigid body whose position is the torque origin (~0u: use ox, oy, oz)
 };
 
 struct SpanChunk {
@@ -283,7 +296,8 @@ __device__ __forceinline__ void cross3(float ax, float ay, float az, float bx, f
   cz = ax * by - ay * bx;
 }
 
-__global__ void k_e_body_rebuild(const float4* __restrict__ blocal, const BodyPoseDev* __restrict__ poses,
+template <class Pose>
+__global__ void k_e_body_rebuild(const float4* __restrict__ blocal, const Pose* __restrict__ poses,
                                  float4* __restrict__ pos, float4* __restrict__ vel,
                                  const uint32_t* __restrict__ slot_of, float4* __restrict__ bpos,
                                  uint32_t* __restrict__ bbox_acc, uint32_t base, uint32_t nf, uint32_t nb) {
@@ -293,7 +307,7 @@ __global__ void k_e_body_rebuild(const float4* __restrict__ blocal, const BodyPo
   if (valid) {
     const uint32_t g = base + nf + q;
     const float4 L = blocal[g];
-    const BodyPoseDev P = poses[__float_as_uint(L.w)];
+    const Pose P = poses[__float_as_uint(L.w)];
     float tx, ty, tz;
     cross3(P.qx, P.qy, P.qz, L.x, L.y, L.z, tx, ty, tz);
     tx = tx * 2.0f;
@@ -1151,15 +1165,31 @@ __global__ void __launch_bounds__(128) k_e_bforce(
 // fixed tree); level 2, the span's thread adds its chunk partials in chunk order. Span
 // ranges are global reference indices.
 
+// Torque origin of a span: its coupled rigid body's position, or the origin it was given.
+__device__ __forceinline__ void span_origin(const SpanDev& sp, const RigidBodyDev* __restrict__ rb, float& ox,
+                                            float& oy, float& oz) {
+  if (sp.rigid != ~0u && rb) {
+    ox = rb[sp.rigid].px;
+    oy = rb[sp.rigid].py;
+    oz = rb[sp.rigid].pz;
+  } else {
+    ox = sp.ox;
+    oy = sp.oy;
+    oz = sp.oz;
+  }
+}
+
 __global__ void __launch_bounds__(kReactThreads) k_react_chunks(const float4* __restrict__ bforce,
                                                                 const float4* __restrict__ bpos,
                                                                 const SpanDev* __restrict__ spans,
                                                                 const SpanChunk* __restrict__ chunks,
+                                                                const RigidBodyDev* __restrict__ rb,
                                                                 const EngineCtl* __restrict__ ctl,
                                                                 float* __restrict__ partial) {
   if (ctl->err & kErrCellCap) return;
   const SpanChunk ch = chunks[blockIdx.x];
-  const SpanDev sp = spans[ch.span];
+  SpanDev sp = spans[ch.span];
+  span_origin(sp, rb, sp.ox, sp.oy, sp.oz);
   float f[6] = {0, 0, 0, 0, 0, 0};
   for (uint32_t kk = ch.begin + threadIdx.x; kk < ch.end; kk += kReactThreads) {
     const float4 fk = bforce[kk];
@@ -1187,13 +1217,14 @@ __global__ void __launch_bounds__(kReactThreads) k_react_chunks(const float4* __
 // summed exactly).
 __global__ void k_react_spans(const float* __restrict__ partial, const uint32_t* __restrict__ chunk_first,
                               const float4* __restrict__ bforce, const float4* __restrict__ bpos,
-                              const SpanDev* __restrict__ spans, const EngineCtl* __restrict__ ctl,
-                              float* __restrict__ breact, uint32_t nspans) {
+                              const SpanDev* __restrict__ spans, const RigidBodyDev* __restrict__ rb,
+                              const EngineCtl* __restrict__ ctl, float* __restrict__ breact, uint32_t nspans) {
   if (ctl->err & kErrCellCap) return;
   const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= nspans) return;
   float f[6] = {0, 0, 0, 0, 0, 0};
-  const SpanDev sp = spans[q];
+  SpanDev sp = spans[q];
+  span_origin(sp, rb, sp.ox, sp.oy, sp.oz);
   if (sp.end - sp.start <= kReactExactSpan) {
     for (uint32_t kk = sp.start; kk < sp.end; ++kk) {
       const float4 fk = bforce[kk];
@@ -1211,6 +1242,98 @@ __global__ void k_react_spans(const float* __restrict__ partial, const uint32_t*
       for (int a = 0; a < 6; ++a) f[a] = f[a] + partial[6 * c + a];
   }
   for (int a = 0; a < 6; ++a) breact[6 * q + a] = breact[6 * q + a] + f[a];
+}
+
+// Rigid substeps of the coupling loop without contacts, one thread per body, f32 in the
+// reference's order: per substep the gravity field adds g * (1 / inv_mass)
+// (crates/vxl-phys-field/src/lib.rs:22-31) and the fluid reaction pass adds the tick-averaged
+// reaction of the body's span (crates/vxl-phys/src/world_step.rs:235-255); then
+// Integrator::integrate_velocities with gravity ZERO (v += (0 + F inv_m) dt; w += I_world^-1 tau
+// dt with I_world^-1 = R diag(I^-1) R^T, crates/vxl-phys-core/src/body.rs:172-176; whole-vector
+// speed clamps) and integrate_positions (x += v dt; q = normalize(q + dt/2 (0, w) q),
+// crates/vxl-phys-core/src/math.rs:216-252), crates/vxl-phys-integrate/src/lib.rs:18-60.
+// `with_reaction` is 0 before the first fluid tick of the loop (no reaction yet).
+__device__ __forceinline__ void rigid_world_inv_inertia(const RigidBodyDev& b, float lx, float ly, float lz,
+                                                        float& ox, float& oy, float& oz) {
+  const float xx = b.qx * b.qx, yy = b.qy * b.qy, zz = b.qz * b.qz;
+  const float xy = b.qx * b.qy, xz = b.qx * b.qz, yz = b.qy * b.qz;
+  const float wx = b.qw * b.qx, wy = b.qw * b.qy, wz = b.qw * b.qz;
+  const float m00 = 1.0f - 2.0f * (yy + zz), m01 = 2.0f * (xy - wz), m02 = 2.0f * (xz + wy);
+  const float m10 = 2.0f * (xy + wz), m11 = 1.0f - 2.0f * (xx + zz), m12 = 2.0f * (yz - wx);
+  const float m20 = 2.0f * (xz - wy), m21 = 2.0f * (yz + wx), m22 = 1.0f - 2.0f * (xx + yy);
+  const float tx = m00 * lx + m10 * ly + m20 * lz;
+  const float ty = m01 * lx + m11 * ly + m21 * lz;
+  const float tz = m02 * lx + m12 * ly + m22 * lz;
+  const float vx = tx * b.iix, vy = ty * b.iiy, vz = tz * b.iiz;
+  ox = m00 * vx + m01 * vy + m02 * vz;
+  oy = m10 * vx + m11 * vy + m12 * vz;
+  oz = m20 * vx + m21 * vy + m22 * vz;
+}
+
+__global__ void k_rigid_step(RigidBodyDev* __restrict__ bodies, uint32_t n, const float* __restrict__ breact,
+                             int with_reaction, float gx, float gy, float gz, float dt, uint32_t substeps,
+                             float max_linear, float max_angular) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  RigidBodyDev b = bodies[i];
+  if (!b.dynamic) return;
+  float rf[6] = {0, 0, 0, 0, 0, 0};
+  if (with_reaction && b.span != ~0u)
+    for (int a = 0; a < 6; ++a) rf[a] = breact[6 * b.span + a];
+  const float hd = 0.5f * dt;
+  for (uint32_t k = 0; k < substeps; ++k) {
+    const float mass = 1.0f / b.inv_mass;
+    float fx = 0.0f + gx * mass, fy = 0.0f + gy * mass, fz = 0.0f + gz * mass;
+    fx = fx + rf[0];
+    fy = fy + rf[1];
+    fz = fz + rf[2];
+    const float tqx = 0.0f + rf[3], tqy = 0.0f + rf[4], tqz = 0.0f + rf[5];
+    b.vx = b.vx + (0.0f + fx * b.inv_mass) * dt;
+    b.vy = b.vy + (0.0f + fy * b.inv_mass) * dt;
+    b.vz = b.vz + (0.0f + fz * b.inv_mass) * dt;
+    float ax, ay, az;
+    rigid_world_inv_inertia(b, tqx, tqy, tqz, ax, ay, az);
+    b.wx = b.wx + ax * dt;
+    b.wy = b.wy + ay * dt;
+    b.wz = b.wz + az * dt;
+    const float sp = sqrtf(b.vx * b.vx + b.vy * b.vy + b.vz * b.vz);
+    if (sp > max_linear) {
+      const float s = max_linear / sp;
+      b.vx = b.vx * s;
+      b.vy = b.vy * s;
+      b.vz = b.vz * s;
+    }
+    const float ws = sqrtf(b.wx * b.wx + b.wy * b.wy + b.wz * b.wz);
+    if (ws > max_angular) {
+      const float s = max_angular / ws;
+      b.wx = b.wx * s;
+      b.wy = b.wy * s;
+      b.wz = b.wz * s;
+    }
+    b.px = b.px + b.vx * dt;
+    b.py = b.py + b.vy * dt;
+    b.pz = b.pz + b.vz * dt;
+    // dq = (w, 0) * q (Hamilton), then q + dq dt/2, normalized
+    const float dqx = 0.0f * b.qx + b.wx * b.qw + b.wy * b.qz - b.wz * b.qy;
+    const float dqy = 0.0f * b.qy - b.wx * b.qz + b.wy * b.qw + b.wz * b.qx;
+    const float dqz = 0.0f * b.qz + b.wx * b.qy - b.wy * b.qx + b.wz * b.qw;
+    const float dqw = 0.0f * b.qw - b.wx * b.qx - b.wy * b.qy - b.wz * b.qz;
+    const float nx = b.qx + dqx * hd, ny = b.qy + dqy * hd, nz = b.qz + dqz * hd, nw = b.qw + dqw * hd;
+    const float len2 = nx * nx + ny * ny + nz * nz + nw * nw;
+    if (len2 > 1e-16f) {
+      const float inv = 1.0f / sqrtf(len2);
+      b.qx = nx * inv;
+      b.qy = ny * inv;
+      b.qz = nz * inv;
+      b.qw = nw * inv;
+    } else {
+      b.qx = 0.0f;
+      b.qy = 0.0f;
+      b.qz = 0.0f;
+      b.qw = 1.0f;
+    }
+  }
+  bodies[i] = b;
 }
 
 // Tick average (fluid_step.rs:84-88): e *= 1 / substeps.

@@ -22,6 +22,7 @@ struct EngineCtl;
 struct SpanDev;
 struct SpanChunk;
 struct BodyPoseDev;
+struct RigidBodyDev;
 
 // Launch shape of the particle passes (chosen by the autotuner for batches).
 struct Tuning {
@@ -71,6 +72,13 @@ class Engine {
   vxl_status set_body_lattice(uint32_t scene, const float* local_xyz, const uint32_t* body_index, uint64_t nb,
                               uint32_t nbodies);
   vxl_status set_body_poses(uint32_t scene, const vxl_sph_body_pose* poses, uint32_t nbodies);
+  // Device-side coupling loop without contacts: the scene's bodies (one per lattice body,
+  // same order) as rigid bodies; each coupled tick integrates them from the previous tick's
+  // reactions, rebuilds the boundary segment from their poses and steps the fluid tick.
+  vxl_status set_rigid_bodies(uint32_t scene, const vxl_sph_rigid_body* bodies, uint32_t n);
+  vxl_status step_coupled_async(float dt_tick, uint32_t rigid_substeps, const float gravity[3], float max_linear,
+                                float max_angular);
+  vxl_status read_rigid_bodies(uint32_t scene, vxl_sph_rigid_body* out, uint32_t n);
   vxl_status write_state(uint32_t scene, const float* pos, const float* vel);
   vxl_status read_state(uint32_t scene, float* pos, float* vel);
   // Deferred readback of every slot's position (reference order, scene after scene):
@@ -158,6 +166,15 @@ class Engine {
   float4* blocal_ = nullptr;         // body-frame lattice per boundary slot (reference order), lazily
   BodyPoseDev* poses_d_ = nullptr;   // poses of one scene's bodies (staged per call)
   uint32_t poses_cap_ = 0;
+  std::vector<std::vector<vxl_sph_rigid_body>> rigid_;  // per scene (empty: not coupled)
+  RigidBodyDev* rb_d_ = nullptr;  // all scenes' rigid bodies, scene after scene
+  uint32_t rb_cap_ = 0, rb_n_ = 0;
+  std::vector<uint32_t> rb_off_;  // first rigid body of each scene
+  bool rb_dirty_ = false;         // host bodies changed: upload before the next coupled tick
+  bool rb_have_reaction_ = false;  // breact holds the previous coupled tick's reactions
+  bool rb_live_ = false;           // rb_d_ holds the bodies' current (evolved) states
+  vxl_status rb_pull();
+  void rb_layout();
   float* snap_h_ = nullptr;  // pinned, 3 floats per slot
   uint64_t snap_cap_ = 0, snap_n_ = 0;
   cudaEvent_t ev_snap_ = nullptr;

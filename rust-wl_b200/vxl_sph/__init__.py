@@ -123,6 +123,11 @@ class BodyPose(C.Structure):
                 ("angvel", C.c_float * 3)]
 
 
+class RigidBody(C.Structure):
+    _fields_ = [("pose", BodyPose), ("inv_mass", C.c_float), ("local_inv_inertia", C.c_float * 3),
+                ("dynamic", C.c_uint32)]
+
+
 def poses_array(bodies):
     """BodyPose array from objects with id, pos, rot, linvel, angvel (e.g. scenes.Body)."""
     arr = (BodyPose * max(len(bodies), 1))()
@@ -187,6 +192,10 @@ SIGNATURES = {
     "vxl_sph_autotune": (C.c_int, [_H, C.c_float, C.c_uint32, C.POINTER(Tuning)]),
     "vxl_sph_request_state": (C.c_int, [_H]),
     "vxl_sph_take_state": (C.c_int, [_H, _FP, C.c_uint64]),
+    "vxl_sph_set_rigid_bodies": (C.c_int, [_H, C.c_uint32, C.POINTER(RigidBody), C.c_uint32]),
+    "vxl_sph_step_coupled": (C.c_int, [_H, C.c_float, C.c_uint32, _FP, C.c_float, C.c_float, C.POINTER(Reaction),
+                                       C.c_uint32]),
+    "vxl_sph_read_rigid_bodies": (C.c_int, [_H, C.c_uint32, C.POINTER(RigidBody), C.c_uint32]),
     "vxl_sph_set_body_lattice": (C.c_int, [_H, C.c_uint32, _FP, C.POINTER(C.c_uint32), C.c_uint64, C.c_uint32]),
     "vxl_sph_set_body_poses": (C.c_int, [_H, C.c_uint32, C.POINTER(BodyPose), C.c_uint32]),
     "vxl_sph_serve_create": (C.c_int, [C.c_int32, C.c_uint64, C.c_uint32, C.POINTER(C.c_void_p)]),
@@ -390,6 +399,46 @@ class Scene:
         """Rebuild the boundary segment on the device from the bodies' poses."""
         arr, n = poses_array(bodies)
         _check(self.lib.vxl_sph_set_body_poses(self._h, scene, arr, n))
+
+    def set_spans(self, spans, scene: int = 0) -> None:
+        """Spans for ticks that take none (vxl_sph_step_coupled)."""
+        arr, n = spans_array(spans)
+        _check(self.lib.vxl_sph_set_spans_scene(self._h, scene, arr, n))
+
+    def set_rigid_bodies(self, bodies, inv_mass, local_inv_inertia, dynamic, scene: int = 0) -> None:
+        """The lattice bodies as rigid bodies: poses from `bodies` (id, pos, rot, linvel,
+        angvel), mass properties and dynamic flags per body."""
+        arr = (RigidBody * max(len(bodies), 1))()
+        poses, _ = poses_array(bodies)
+        for q in range(len(bodies)):
+            arr[q].pose = poses[q]
+            arr[q].inv_mass = float(inv_mass[q])
+            for a in range(3):
+                arr[q].local_inv_inertia[a] = float(local_inv_inertia[q][a])
+            arr[q].dynamic = 1 if dynamic[q] else 0
+        _check(self.lib.vxl_sph_set_rigid_bodies(self._h, scene, arr, len(bodies)))
+        self._rigid_n = getattr(self, "_rigid_n", {})
+        self._rigid_n[scene] = len(bodies)
+
+    def step_coupled(self, dt_tick: float, rigid_substeps: int = 2, gravity=(0.0, -9.81, 0.0),
+                     max_linear: float = 100.0, max_angular: float = 50.0, nspans: int = 0):
+        g = np.ascontiguousarray(gravity, dtype=np.float32)
+        out = (Reaction * max(nspans, 1))()
+        _check(self.lib.vxl_sph_step_coupled(self._h, dt_tick, rigid_substeps, _fptr(g), max_linear, max_angular,
+                                             out, nspans))
+        return [(out[q].body, np.array(out[q].force[:], np.float32), np.array(out[q].torque[:], np.float32))
+                for q in range(nspans)]
+
+    def read_rigid_bodies(self, scene: int = 0) -> np.ndarray:
+        """(n, 13) float32: pos xyz, rot xyzw, linvel xyz, angvel xyz."""
+        n = self._rigid_n[scene]
+        arr = (RigidBody * max(n, 1))()
+        _check(self.lib.vxl_sph_read_rigid_bodies(self._h, scene, arr, n))
+        out = np.empty((n, 13), np.float32)
+        for q in range(n):
+            p = arr[q].pose
+            out[q] = list(p.pos) + list(p.rot) + list(p.linvel) + list(p.angvel)
+        return out
 
     def read_state(self, out=None) -> tuple[np.ndarray, np.ndarray]:
         """Positions and velocities in reference order; `out=(pos, vel)` reuses caller
@@ -597,6 +646,12 @@ class Batch:
     profile = Scene.profile
     request_state = Scene.request_state
     take_state = Scene.take_state
+    set_body_lattice = Scene.set_body_lattice
+    set_body_poses = Scene.set_body_poses
+    set_spans = Scene.set_spans
+    set_rigid_bodies = Scene.set_rigid_bodies
+    step_coupled = Scene.step_coupled
+    read_rigid_bodies = Scene.read_rigid_bodies
 
     def stats(self) -> Stats:
         s = Stats()

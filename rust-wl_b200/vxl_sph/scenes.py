@@ -140,6 +140,19 @@ def body_lattice(bodies, spacing: float, h: float, layers: int, cache=None):
     return np.concatenate(pts).astype(F), np.concatenate(idx)
 
 
+def box_mass_props(half, density: float):
+    """Mass properties of a box body (crates/vxl-phys-core/src/mass.rs:35-48), float32 in the
+    reference's order: m = rho ex ey ez with e = 2 half, I = m / 12 (e1^2 + e2^2); returns
+    (inv_mass, local inverse inertia diagonal)."""
+    rho = F(density) if density > 0 else F(1.0)
+    ex, ey, ez = (F(2.0) * F(h) for h in half)
+    m = F(F(F(rho * ex) * ey) * ez)
+    ix = F(F(m / F(12.0)) * F(F(ey * ey) + F(ez * ez)))
+    iy = F(F(m / F(12.0)) * F(F(ex * ex) + F(ez * ez)))
+    iz = F(F(m / F(12.0)) * F(F(ex * ex) + F(ey * ey)))
+    return F(F(1.0) / m), (F(F(1.0) / ix), F(F(1.0) / iy), F(F(1.0) / iz))
+
+
 def tank_bodies(inner, t: float, first_id: int = 0) -> list:
     """Floor + four walls (static boxes) around the open box [0, inner]; thickness t
     (the reference's --tank pattern, gpu_tick_probe.rs:20-63, with the tank's own size)."""

@@ -437,6 +437,141 @@ def test_device_body_rebuild_equals_host_upload(vxl, oracle_mod):
     o.close()
 
 
+def _body_states(bodies, dynamic, density):
+    from vxl_sph import scenes
+    st = np.zeros((len(bodies), 18), F32)
+    for q, b in enumerate(bodies):
+        st[q, 0:3] = b.pos
+        st[q, 3:7] = b.rot
+        st[q, 7:10] = b.linvel
+        st[q, 10:13] = b.angvel
+        if dynamic[q]:
+            im, ii = scenes.box_mass_props(b.half, density)
+            st[q, 13] = im
+            st[q, 14:17] = ii
+            st[q, 17] = 1.0
+    return st
+
+
+def _floating_scene(seed=23, dims=(10, 12, 10), shift=(0.0, 0.0, 0.0)):
+    """Tank walls (static) and two boxes (dynamic) floating in the fluid's top layers."""
+    from vxl_sph import scenes
+    s = 0.02
+    tank = (0.6, 0.5, 0.4)
+    walls = scenes.tank_bodies(tank, 2 * s)
+    a = float(np.sin(F32(0.2)))
+    c = float(np.cos(F32(0.2)))
+    top = F32(dims[1]) * F32(s)
+    sx, sy, sz = shift
+    boxes = [scenes.Body(20, (0.05, 0.03, 0.04), (0.1 + sx, float(top) - 0.005, 0.1 + sz), rot=(0.0, a, 0.0, c),
+                         angvel=(0.3, 0.0, -0.2)),
+             scenes.Body(21, (0.03, 0.03, 0.03), (0.16 + sx, float(top) - 0.015 + sy, 0.06 + sz),
+                         linvel=(0.0, -0.2, 0.1))]
+    bodies = walls + boxes
+    dynamic = [False] * len(walls) + [True] * len(boxes)
+    params = scenes.baseline_params(s, substeps=4)
+    fluid = scenes.jitter(scenes.fluid_block((0.0, 0.0, 0.0), dims, s), s, seed)
+    spec = scenes.assemble("floating", params, fluid, bodies, s, 4)
+    local, idx = scenes.body_lattice(bodies, s, 2 * s, params.boundary_layers)
+    return spec, bodies, dynamic, local, idx
+
+
+def _couple(g, spec, bodies, dynamic, local, idx, scene=0):
+    st = _body_states(bodies, dynamic, 400.0)
+    g.set_body_lattice(local, idx, len(bodies), scene=scene)
+    g.set_rigid_bodies(bodies, st[:, 13], st[:, 14:17], dynamic, scene=scene)
+    g.set_spans(spec.spans, scene=scene)
+    return st
+
+
+GRAVITY = np.array([0.0, -9.81, 0.0], F32)
+
+
+@pytest.mark.parametrize("rigid_substeps", [2, 3])
+def test_coupled_loop_on_device_equals_oracle_loop(vxl, oracle_mod, rigid_substeps):
+    """Floating boxes driven by the fluid: vxl_sph_step_coupled (rigid substeps from the
+    previous tick's reactions, boundary rebuilt from the new poses, one fluid tick — all on
+    the device) gives, tick after tick, bitwise the bodies, the fluid state and the
+    reactions of the same loop run on the host around the oracle (rigid substeps, then
+    set_boundary_particles, then step)."""
+    from vxl_sph import scenes
+    spec, bodies, dynamic, local, idx = _floating_scene()
+    boxes = [b for b, d in zip(bodies, dynamic) if d]
+    g = vxl.Scene(spec.params, spec.pos, spec.vel, spec.pmass, spec.n_fluid)
+    o = oracle_mod.OracleSystem.from_scene(spec, threads=4)
+    st = _couple(g, spec, bodies, dynamic, local, idx)
+    nspans = len(spec.spans)
+    dt = float(F32(1.0) / F32(60.0))
+    react = np.zeros((len(bodies), 6), F32)
+    row = {b.id: q for q, b in enumerate(bodies)}
+    felt = set()
+    for t in range(5):
+        oracle_mod.rigid_step(st, react, GRAVITY, float(F32(dt) / F32(rigid_substeps)), rigid_substeps, 100.0, 50.0)
+        posed = [scenes.Body(b.id, b.half, tuple(float(x) for x in st[q, 0:3]), rot=tuple(float(x) for x in st[q, 3:7]),
+                             linvel=tuple(float(x) for x in st[q, 7:10]), angvel=tuple(float(x) for x in st[q, 10:13]))
+                 for q, b in enumerate(bodies)]
+        o.set_bodies(posed)
+        o.step(dt)
+        ro = o.reactions()
+        rg = g.step_coupled(dt, rigid_substeps, GRAVITY, 100.0, 50.0, nspans)
+        dev = g.read_rigid_bodies()
+        assert_bits(dev, st[:, :13], f"tick {t} rigid bodies")
+        assert [x[0] for x in rg] == [x[0] for x in ro]
+        react[:] = 0
+        for (bid, fg, tg), (_, fo, to) in zip(rg, ro):
+            if dynamic[row[bid]]:
+                assert fg.tobytes() == fo.tobytes() and tg.tobytes() == to.tobytes(), (t, bid, fg, fo, tg, to)
+                if np.any(fo != 0):
+                    felt.add(bid)
+            react[row[bid], 0:3] = fo
+            react[row[bid], 3:6] = to
+        r = o.read_f32()
+        p, v = g.read_state()
+        assert_bits(p, r["pos"], f"tick {t} pos")
+        assert_bits(v, r["vel"], f"tick {t} vel")
+    # the fluid pushed every box at some tick, and the boxes moved
+    assert felt == {b.id for b in boxes}, felt
+    assert np.all(np.abs(st[[row[b.id] for b in boxes], 0:3] - np.array([b.pos for b in boxes], F32)) > 0)
+    o.close()
+    g.close()
+
+
+def test_coupled_loop_batched_equals_scenes_alone(vxl):
+    """One vxl_sph_step_coupled over a batch of two floating scenes (different sizes) and one
+    scene without rigid bodies equals each scene stepped alone (coupled or plain), bitwise:
+    bodies, fluid state and reactions."""
+    from vxl_sph import scenes
+    a = _floating_scene(seed=5, dims=(10, 12, 10))
+    b = _floating_scene(seed=9, dims=(14, 10, 9), shift=(0.2, 0.0, 0.1))
+    plain = scenes.small_dam(n=(8, 9, 8), spacing=0.05, tank=(0.8, 0.7, 0.6), seed=3)
+    bat = vxl.Batch([a[0], b[0], plain])
+    alone = [vxl.Scene(x.params, x.pos, x.vel, x.pmass, x.n_fluid) for x in (a[0], b[0], plain)]
+    for q, (x, sc) in enumerate(zip((a, b), alone)):
+        _couple(bat, *x, scene=q)
+        _couple(sc, *x)
+    dt = float(F32(1.0) / F32(60.0))
+    for t in range(4):
+        bat.step_coupled(dt, 2, GRAVITY)
+        rb = bat.reactions()
+        ra = []
+        for q in range(2):
+            ra += alone[q].step_coupled(dt, 2, GRAVITY, nspans=len((a, b)[q][0].spans))
+        ra += alone[2].step_tick(dt, plain.spans)
+        assert len(ra) == len(rb)
+        for (b1, f1, t1), (b2, f2, t2) in zip(ra, rb):
+            assert b1 == b2 and f1.tobytes() == f2.tobytes() and t1.tobytes() == t2.tobytes(), (t, b1)
+        for q in range(3):
+            p1, v1 = bat.read_state(q)
+            p2, v2 = alone[q].read_state()
+            assert_bits(p1, p2, f"tick {t} scene {q} pos")
+            assert_bits(v1, v2, f"tick {t} scene {q} vel")
+        for q in range(2):
+            assert_bits(bat.read_rigid_bodies(q), alone[q].read_rigid_bodies(), f"tick {t} scene {q} bodies")
+    bat.close()
+    for sc in alone:
+        sc.close()
+
+
 def test_deferred_readback_and_vxld_dump(vxl, oracle_mod, tmp_path):
     """vxl_sph_request_state / vxl_sph_take_state return the state that vxl_sph_read_state
     returns, and a VXLD dump's frames are the oracle's fluid positions at those ticks."""

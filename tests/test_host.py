@@ -43,13 +43,24 @@ def test_struct_sizes_match_header(vxl, tmp_path):
         "sizeof(vxl_sph_params),sizeof(vxl_sph_desc),sizeof(vxl_sph_span),sizeof(vxl_sph_reaction),"
         "sizeof(vxl_sph_grid_info),sizeof(vxl_sph_stats),sizeof(vxl_block_header));"
         'printf("%zu %zu %zu %zu\\n",sizeof(vxl_sph_tuning),sizeof(vxl_sph_request_status),sizeof(vxl_sph_serve_report),sizeof(vxl_sph_body_pose));'
+        'printf("%zu\\n",sizeof(vxl_sph_rigid_body));'
         "return 0;}\n")
     exe = tmp_path / "sizes"
     subprocess.run(["gcc", "-std=c99", "-I", str(ROOT / "include"), str(src), "-o", str(exe)], check=True)
     got = [int(x) for x in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
     want = [C.sizeof(t) for t in (vxl.Params, vxl.Desc, vxl.Span, vxl.Reaction, vxl.GridInfo, vxl.Stats,
-                                  vxl.BlockHeader, vxl.Tuning, vxl.RequestStatus, vxl.ServeReport, vxl.BodyPose)]
+                                  vxl.BlockHeader, vxl.Tuning, vxl.RequestStatus, vxl.ServeReport, vxl.BodyPose, vxl.RigidBody)]
     assert got == want
+
+
+@pytest.mark.parametrize("half,density", [((0.2, 0.15, 0.1), 500.0), ((0.05, 0.05, 0.05), 1000.0),
+                                          ((0.3, 0.02, 0.17), -1.0), ((0.125, 0.25, 0.5), 740.0)])
+def test_box_mass_props_bit_identical(vxl, oracle_mod, half, density):
+    from vxl_sph.scenes import box_mass_props
+    im, ii = box_mass_props(half, density)
+    im_o, ii_o = oracle_mod.box_mass_props(half, density)
+    assert np.float32(im).tobytes() == np.float32(im_o).tobytes()
+    assert np.asarray(ii, np.float32).tobytes() == ii_o.tobytes()
 
 
 @pytest.mark.parametrize("h,s", [(0.1, 0.05), (0.04, 0.02), (0.02, 0.01), (0.01, 0.005), (0.1, 0.03)])
