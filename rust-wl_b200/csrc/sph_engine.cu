@@ -1081,7 +1081,7 @@ void Engine::enqueue_substep(bool with_reactions) {
                                                                       spans_d_, chunks_d_, rb_d_, ctl_d_,
                                                                       react_partial_));
       LAUNCH_ON(KID_REACT_SPANS, side_,
-                k_react_spans<<<blocks_for(nspans_, 64), 64, 0, side_>>>(react_partial_, chunk_first_d_,
+                k_react_spans<<<(nspans_ + kReactSpanWarps - 1) / kReactSpanWarps, 32 * kReactSpanWarps, 0, side_>>>(react_partial_, chunk_first_d_,
                                                                          (const float4*)bforce_, (const float4*)bpos_,
                                                                          spans_d_, rb_d_, ctl_d_,
                                                                          breact_d_, nspans_));

@@ -100,10 +100,11 @@ struct SpanChunk {
 };
 
 constexpr uint32_t kReactChunk = 4096;
-// Spans of at most this many particles (bodies, as opposed to tank walls) are summed by one
-// thread in index order: the reference's sum, bit for bit.
+// Spans of at most this many particles (bodies, as opposed to tank walls) are summed in
+// index order: the reference's sum, bit for bit.
 constexpr uint32_t kReactExactSpan = 8192;
 constexpr int kReactThreads = 256;
+constexpr int kReactSpanWarps = 2;  // spans per block of k_react_spans (one warp each)
 
 // Engine-wide control block.
 constexpr int kWorkSlots = 16;  // persistent-kernel work counters per substep
@@ -1216,12 +1217,15 @@ __global__ void __launch_bounds__(128) k_e_bforce(
 }
 
 // Per-span force and torque about the body origin (fluid_boundary.rs:10-28), added to
-// the tick accumulator. A span of at most kReactExactSpan particles is summed by one thread
-// in index order (the reference's sum, bit for bit). Larger spans (tank walls) take a
-// fixed-shape two-level reduction, deterministic run to run: level 1, one block per chunk of
-// <= kReactChunk consecutive particles (thread t sums t, t + blockDim, ... in order, then a
-// fixed tree); level 2, the span's thread adds its chunk partials in chunk order. Span
-// ranges are global reference indices.
+// the tick accumulator. A span of at most kReactExactSpan particles is summed in index order
+// (the reference's sum, bit for bit) by one warp: the lanes load 32 consecutive particles
+// and form each one's force and torque terms, then lane a (a < 6) adds component a of the
+// 32 terms to its running sum in index order — six independent sequential sums, with the
+// loads of a batch in flight together instead of one at a time. Larger spans (tank walls)
+// take a fixed-shape two-level reduction, deterministic run to run: level 1, one block per
+// chunk of <= kReactChunk consecutive particles (thread t sums t, t + blockDim, ... in
+// order, then a fixed tree); level 2, the span's warp adds its chunk partials in chunk
+// order. Span ranges are global reference indices.
 
 // Torque origin of a span: its coupled rigid body's position, or the origin it was given.
 __device__ __forceinline__ void span_origin(const SpanDev& sp, const RigidBodyDev* __restrict__ rb, float& ox,
@@ -1278,28 +1282,38 @@ __global__ void k_react_spans(const float* __restrict__ partial, const uint32_t*
                               const SpanDev* __restrict__ spans, const RigidBodyDev* __restrict__ rb,
                               const EngineCtl* __restrict__ ctl, float* __restrict__ breact, uint32_t nspans) {
   if (ctl->err & kErrCellCap) return;
-  const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= nspans) return;
-  float f[6] = {0, 0, 0, 0, 0, 0};
+  __shared__ float terms[kReactSpanWarps][6][33];
+  const uint32_t w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t q = blockIdx.x * kReactSpanWarps + w;
+  if (q >= nspans) return;  // uniform over the warp
   SpanDev sp = spans[q];
   span_origin(sp, rb, sp.ox, sp.oy, sp.oz);
+  float f = 0.0f;  // lane a < 6: component a (force xyz, torque xyz)
   if (sp.end - sp.start <= kReactExactSpan) {
-    for (uint32_t kk = sp.start; kk < sp.end; ++kk) {
-      const float4 fk = bforce[kk];
-      const float4 p = bpos[kk];
-      const float rx = p.x - sp.ox, ry = p.y - sp.oy, rz = p.z - sp.oz;
-      f[0] = f[0] + fk.x;
-      f[1] = f[1] + fk.y;
-      f[2] = f[2] + fk.z;
-      f[3] = f[3] + (ry * fk.z - rz * fk.y);
-      f[4] = f[4] + (rz * fk.x - rx * fk.z);
-      f[5] = f[5] + (rx * fk.y - ry * fk.x);
+    for (uint32_t b0 = sp.start; b0 < sp.end; b0 += 32) {
+      const uint32_t kk = b0 + lane;
+      if (kk < sp.end) {
+        const float4 fk = bforce[kk];
+        const float4 p = bpos[kk];
+        const float rx = p.x - sp.ox, ry = p.y - sp.oy, rz = p.z - sp.oz;
+        terms[w][0][lane] = fk.x;
+        terms[w][1][lane] = fk.y;
+        terms[w][2][lane] = fk.z;
+        terms[w][3][lane] = ry * fk.z - rz * fk.y;
+        terms[w][4][lane] = rz * fk.x - rx * fk.z;
+        terms[w][5][lane] = rx * fk.y - ry * fk.x;
+      }
+      __syncwarp();
+      if (lane < 6) {
+        const uint32_t nb = min(32u, sp.end - b0);
+        for (uint32_t t = 0; t < nb; ++t) f = f + terms[w][lane][t];
+      }
+      __syncwarp();
     }
-  } else {
-    for (uint32_t c = chunk_first[q]; c < chunk_first[q + 1]; ++c)
-      for (int a = 0; a < 6; ++a) f[a] = f[a] + partial[6 * c + a];
+  } else if (lane < 6) {
+    for (uint32_t c = chunk_first[q]; c < chunk_first[q + 1]; ++c) f = f + partial[6 * c + lane];
   }
-  for (int a = 0; a < 6; ++a) breact[6 * q + a] = breact[6 * q + a] + f[a];
+  if (lane < 6) breact[6 * q + lane] = breact[6 * q + lane] + f;
 }
 
 // Rigid substeps of the coupling loop without contacts, one thread per body, f32 in the
