@@ -814,13 +814,16 @@ __global__ void k_e_halfmask(const float4* __restrict__ pos, const SceneDev* __r
 // Per axis, which halves of the three cells (d = -1, 0, +1) along it a particle at p can
 // reach: bit 2 (d + 1) for the lower half, bit 2 (d + 1) + 1 for the upper half. A half is
 // dropped only when the gap from p to its nominal interval exceeds `reach` (h plus a
-// margin far above the rounding of cell faces and midplanes).
-__device__ __forceinline__ uint32_t half_reach_bits(float p, float l, float B, float reach) {
+// margin far above the rounding of cell faces and midplanes). `last`: p's cell is the last
+// on this axis, whose upper half also holds the particles clamped into it from beyond the
+// grid (an axis at the 16,384-cell cap), p possibly among them: that half has no upper face.
+// (No particle lies below the grid's lower corner, the scene AABB's minimum.)
+__device__ __forceinline__ uint32_t half_reach_bits(float p, float l, float B, float reach, bool last) {
   const float hb = B * 0.5f;
   const float gm_lo = fmaxf(p - (l - hb), 0.0f);
   const float gm_hi = fmaxf(p - l, 0.0f);
   const float g0_lo = fmaxf(fmaxf(l - p, p - (l + hb)), 0.0f);
-  const float g0_hi = fmaxf(fmaxf((l + hb) - p, p - (l + B)), 0.0f);
+  const float g0_hi = fmaxf(fmaxf((l + hb) - p, last ? 0.0f : p - (l + B)), 0.0f);
   const float gp_lo = fmaxf((l + B) - p, 0.0f);
   const float gp_hi = fmaxf((l + B + hb) - p, 0.0f);
   return (gm_lo <= reach ? 1u : 0u) | (gm_hi <= reach ? 2u : 0u) | (g0_lo <= reach ? 4u : 0u) |
@@ -848,9 +851,9 @@ __device__ __forceinline__ void walk27_half(const GridBox& g, const uint32_t* __
   const float gzl = fmaxf(pz - lz, 0.0f), gzr = fmaxf(lz + B - pz, 0.0f);
   const float reach = h + B * (1.0f / 1024.0f);
   const float reach2 = reach * reach;
-  const uint32_t bxs = half_reach_bits(px, lx, B, reach);
-  const uint32_t bys = half_reach_bits(py, ly, B, reach);
-  const uint32_t bzs = half_reach_bits(pz, lz, B, reach);
+  const uint32_t bxs = half_reach_bits(px, lx, B, reach, cx + 1 == g.nx);
+  const uint32_t bys = half_reach_bits(py, ly, B, reach, cy + 1 == g.ny);
+  const uint32_t bzs = half_reach_bits(pz, lz, B, reach, cz + 1 == g.nz);
   for (int dz = -1; dz <= 1; ++dz) {
     const int z = (int)cz + dz;
     if (z < 0 || z >= (int)g.nz) continue;

@@ -276,6 +276,26 @@ def test_far_apart_particles(vxl, oracle_mod):
     _run_both(vxl, oracle_mod, _custom(vxl, pos), substeps=3)
 
 
+def test_clamped_edge_cell_with_doubled_bins(vxl, oracle_mod):
+    """A 1 km long scene at h = 0.01: the budget quadruples the bin to 0.04 and the x axis
+    still hits the 16,384-cell cap, so every particle beyond x = 655.32 is clamped into the
+    last x cell. Two clusters there (x = 900 and x = 1000) find their neighbours in that
+    cell — the half-cell culling must not treat its upper face as a wall."""
+    from vxl_sph import scenes
+    s = 0.005
+    blocks = [scenes.fluid_block(o, (4, 4, 4), s) for o in ((0.0, 0.0, 0.0), (900.0, 0.1, 0.1),
+                                                          (999.98, 0.28, 0.28))]
+    spec = _custom(vxl, np.concatenate(blocks), h=2 * s, spacing=s)
+    lo, hi = spec.pos.min(0), spec.pos.max(0)
+    _, bin_, dims = oracle_mod.grid_box(lo, hi, 2 * s)
+    assert dims[0] == 16384 and bin_ >= 4 * s * 0.999, (bin_, dims)
+    g, o = _run_both(vxl, oracle_mod, spec, substeps=2)
+    dens, _, _, _, _ = g.read_fields()
+    h = 2 * s
+    self_only = spec.params.particle_mass * 315.0 / (64.0 * np.pi * h ** 3)  # mass * W(0)
+    assert np.all(dens[64:] > 1.5 * self_only), "the clamped clusters found their neighbours"
+
+
 def test_boundary_with_many_fluid_neighbours(vxl, oracle_mod):
     """h = 4 s gives boundary particles > 64 fluid neighbours (the gather's slow path)."""
     from vxl_sph import scenes
