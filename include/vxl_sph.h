@@ -340,6 +340,47 @@ vxl_status vxl_sph_step_coupled(vxl_sph_handle* h, float dt_tick, uint32_t rigid
                                 uint32_t nspans);
 vxl_status vxl_sph_read_rigid_bodies(vxl_sph_handle* h, uint32_t scene, vxl_sph_rigid_body* out, uint32_t n);
 
+/* ------------------------------------------------------------------ provider walls
+ * Analytic boundary providers of a scene, queried on the device every substep: the
+ * reference's provider tier of the fluid step (FluidSystem::set_boundaries,
+ * crates/vxl-phys-fluid/src/fluid_access.rs:184-186). For each fluid particle the density
+ * pass collects up to 8 provider planes within h (wall_planes_in, fluid_density.rs:76-118)
+ * and adds, after each neighbour's term, its mirror ghosts in those planes
+ * (fluid_density.rs:38-47); after integration, fluid particles inside a provider are pushed
+ * out and lose their inward normal velocity, and those pushed closer than 0.2 h to an
+ * earlier-indexed pushed particle are separated (boundary_pass / separate_coincident,
+ * fluid_boundary.rs:45-128). Providers are queried in the order given, planes in array order.
+ *   VXL_SPH_PROVIDER_FACES: independent axis-aligned half-space faces (axis, plane = offset,
+ *     sign = outward normal along the axis): a face reports a contact when
+ *     (p[axis] - plane) * sign <= 2 probe (the fluid crate's FloorY / Tank providers,
+ *     crates/vxl-phys-fluid/src/tests.rs:9-110).
+ *   VXL_SPH_PROVIDER_CONVEX: a convex solid {x : normal . x <= offset for every plane};
+ *     the plane of largest normal . x - offset decides (HalfSpaceSet,
+ *     crates/vxl-phys-terrain/src/plane_set.rs:60-76, 166-181).
+ * Other providers (voxel terrain, meshes, splats) stay on the host: they are not on this
+ * path. n = 0 removes the scene's providers. */
+#define VXL_SPH_PROVIDER_FACES 0u
+#define VXL_SPH_PROVIDER_CONVEX 1u
+#define VXL_SPH_MAX_PROVIDER_PLANES 64u  /* planes per scene */
+typedef struct vxl_sph_wall_plane {
+  float normal[3];  /* CONVEX: outward unit normal */
+  float offset;     /* CONVEX: offset d; FACES: the face's plane coordinate */
+  uint32_t axis;    /* FACES: 0, 1, 2 */
+  float sign;       /* FACES: +1 or -1 */
+} vxl_sph_wall_plane;
+
+typedef struct vxl_sph_provider {
+  uint32_t kind;             /* VXL_SPH_PROVIDER_* */
+  uint32_t first_plane;      /* planes [first_plane, first_plane + nplanes) */
+  uint32_t nplanes;
+  uint32_t has_bounds;       /* 1: skip the provider beyond its bounds + h (ProviderColliders::bounds) */
+  float bounds_min[3];
+  float bounds_max[3];
+} vxl_sph_provider;
+
+vxl_status vxl_sph_set_providers(vxl_sph_handle* h, uint32_t scene, const vxl_sph_provider* providers,
+                                 uint32_t nproviders, const vxl_sph_wall_plane* planes, uint32_t nplanes);
+
 /* ------------------------------------------------------------------ served form
  * A request loop (the served workload): scene-step requests are submitted at any time,
  * admitted while their device footprint fits an HBM budget, stepped together with

@@ -46,6 +46,15 @@ class OSpan(C.Structure):
     _fields_ = [("body", C.c_uint32), ("origin", C.c_float * 3), ("start", C.c_uint32), ("end", C.c_uint32)]
 
 
+class OWallPlane(C.Structure):
+    _fields_ = [("normal", C.c_float * 3), ("d", C.c_float), ("axis", C.c_uint32), ("sign", C.c_float)]
+
+
+class OProvider(C.Structure):
+    _fields_ = [("kind", C.c_uint32), ("first", C.c_uint32), ("count", C.c_uint32), ("has_bounds", C.c_uint32),
+                ("bmin", C.c_float * 3), ("bmax", C.c_float * 3)]
+
+
 class OReaction(C.Structure):
     _fields_ = [("body", C.c_uint32), ("force", C.c_float * 3), ("torque", C.c_float * 3)]
 
@@ -97,6 +106,7 @@ def load() -> C.CDLL:
                                      _FP, C.POINTER(C.c_uint64)]),
         "orc_boundary_self_sum": (C.c_float, [_FP, C.c_uint64, C.c_float]),
         "orc_grid_probe_hash": (C.c_uint64, [C.c_uint64, C.c_uint64, C.c_uint32]),
+        "orc_set_providers": (None, [C.c_void_p, C.POINTER(OProvider), C.c_uint32, C.POINTER(OWallPlane)]),
         "orc_rigid_step": (None, [_FP, C.c_uint32, _FP, _FP, C.c_float, C.c_uint32, C.c_float, C.c_float]),
         "orc_box_mass_props": (None, [_FP, C.c_float, _FP, _FP]),
     }
@@ -220,6 +230,34 @@ class OracleSystem:
             for a in range(4):
                 arr[q].rot[a] = b.rot[a]
         return int(self.lib.orc_set_bodies(self._h, arr, len(bodies)))
+
+    def set_providers(self, providers) -> None:
+        """Provider walls: objects with `faces` [(axis, plane, sign)] (axis-aligned faces)
+        or `planes` [((nx, ny, nz), d)] (convex half-space set), and `bounds` or None."""
+        planes, recs = [], []
+        for pr in providers:
+            first = len(planes)
+            if hasattr(pr, "faces"):
+                planes += [((0.0, 0.0, 0.0), pl, ax, sg) for ax, pl, sg in pr.faces]
+                kind = 0
+            else:
+                planes += [(tuple(n), d, 0, 1.0) for n, d in pr.planes]
+                kind = 1
+            recs.append((kind, first, len(planes) - first, pr.bounds))
+        parr = (OProvider * max(len(recs), 1))()
+        for q, (kind, first, cnt, b) in enumerate(recs):
+            parr[q].kind, parr[q].first, parr[q].count = kind, first, cnt
+            parr[q].has_bounds = 0 if b is None else 1
+            if b is not None:
+                for a in range(3):
+                    parr[q].bmin[a] = b[0][a]
+                    parr[q].bmax[a] = b[1][a]
+        warr = (OWallPlane * max(len(planes), 1))()
+        for k, (n, d, ax, sg) in enumerate(planes):
+            for a in range(3):
+                warr[k].normal[a] = n[a]
+            warr[k].d, warr[k].axis, warr[k].sign = d, ax, sg
+        self.lib.orc_set_providers(self._h, parr, len(recs), warr)
 
     def set_boundary_raw(self, pos, vel, pmass, spans):
         pos = np.ascontiguousarray(pos, np.float32)

@@ -54,6 +54,22 @@ struct orc_reaction {
   float force[3];
   float torque[3];
 };
+
+// Provider walls: kind 0 = axis-aligned faces (axis, d = plane, sign), 1 = convex
+// half-space set (normal, d); planes [first, first + count) of the plane array.
+struct orc_wall_plane {
+  float normal[3];
+  float d;
+  uint32_t axis;
+  float sign;
+};
+
+struct orc_provider {
+  uint32_t kind;
+  uint32_t first, count;
+  uint32_t has_bounds;
+  float bmin[3], bmax[3];
+};
 }
 
 namespace {
@@ -180,6 +196,31 @@ uint64_t orc_set_bodies(void* p, const orc_body* bodies, uint32_t n) {
     nb = s.set_boundary_particles(v);
   });
   return nb;
+}
+
+// Register the fluid's boundary providers, in order (FluidSystem::set_boundaries,
+// crates/vxl-phys-fluid/src/fluid_access.rs:184-186, with the providers themselves).
+void orc_set_providers(void* p, const orc_provider* pr, uint32_t n, const orc_wall_plane* planes) {
+  with<float>((Handle*)p, [&](auto& s) {
+    using R = std::decay_t<decltype(s.h)>;
+    s.providers.clear();
+    for (uint32_t i = 0; i < n; ++i) {
+      Provider<R> q;
+      q.kind = pr[i].kind;
+      q.has_bounds = pr[i].has_bounds != 0;
+      q.bmin = V3<R>(pr[i].bmin[0], pr[i].bmin[1], pr[i].bmin[2]);
+      q.bmax = V3<R>(pr[i].bmax[0], pr[i].bmax[1], pr[i].bmax[2]);
+      for (uint32_t k = pr[i].first; k < pr[i].first + pr[i].count; ++k) {
+        WallPlane<R> w;
+        w.n = V3<R>(planes[k].normal[0], planes[k].normal[1], planes[k].normal[2]);
+        w.d = planes[k].d;
+        w.axis = planes[k].axis;
+        w.sign = planes[k].sign;
+        q.planes.push_back(w);
+      }
+      s.providers.push_back(q);
+    }
+  });
 }
 
 // Replace the boundary suffix with explicit particles (the FluidStepper view: the

@@ -20,6 +20,7 @@
 #include <cmath>
 #include <cstddef>
 #include <cstdint>
+#include <limits>
 #include <thread>
 #include <vector>
 
@@ -534,6 +535,75 @@ struct Reaction {
   V3<R> force, torque;
 };
 
+// ---------------------------------------------------------------- provider walls
+// Analytic boundary providers (ProviderColliders, crates/vxl-phys-core/src/interop.rs:162-222)
+// of two kinds, each restated from the reference implementation it follows:
+//  - kFaces: independent axis-aligned half-space faces (the fluid crate's test providers
+//    FloorY / Tank, crates/vxl-phys-fluid/src/tests.rs:9-110): a face (axis, plane, sign)
+//    reports a contact when sdf = (p[axis] - plane) * sign <= 2 probe, at p with its axis
+//    coordinate set to the plane, normal sign along the axis, depth probe - sdf.
+//  - kConvex: a convex solid as an intersection of half-spaces n.x <= d (HalfSpaceSet,
+//    crates/vxl-phys-terrain/src/plane_set.rs:60-76, 166-181): the decisive plane k maximises
+//    s = n.x - d; a contact is reported when depth = -s >= -probe, at x - n (n.x - d).
+// contacts_point_boundary is contacts_point for both (interop.rs:214-222).
+template <class R>
+struct Contact {
+  V3<R> point, normal;
+  R depth;
+};
+
+template <class R>
+struct WallPlane {
+  V3<R> n;       // kConvex: outward normal
+  R d;           // kConvex: offset; kFaces: plane coordinate
+  uint32_t axis; // kFaces
+  R sign;        // kFaces: +1 / -1
+};
+
+template <class R>
+struct Provider {
+  enum : uint32_t { kFaces = 0, kConvex = 1 };
+  uint32_t kind = kFaces;
+  bool has_bounds = false;
+  V3<R> bmin, bmax;
+  std::vector<WallPlane<R>> planes;
+
+  void contacts_point(const V3<R>& p, R probe, std::vector<Contact<R>>& out) const {
+    if (kind == kFaces) {
+      for (const auto& f : planes) {  // tests.rs:81-110
+        R comp = p.axis((int)f.axis);
+        R sdf = (comp - f.d) * f.sign;
+        if (sdf > R(2) * probe) continue;
+        V3<R> point = p;
+        point.set_axis((int)f.axis, f.d);
+        V3<R> normal;
+        normal.set_axis((int)f.axis, f.sign);
+        out.push_back(Contact<R>{point, normal, probe - sdf});
+      }
+      return;
+    }
+    if (planes.empty()) return;  // plane_set.rs:166-169
+    R best = -std::numeric_limits<R>::infinity();
+    size_t k = 0;
+    for (size_t i = 0; i < planes.size(); ++i) {  // plane_set.rs:60-71 (signed)
+      R s = planes[i].n.dot(p) - planes[i].d;
+      if (s > best) { best = s; k = i; }
+    }
+    R depth = -best;
+    if (depth < -probe) return;
+    const auto& pl = planes[k];
+    V3<R> point = p - pl.n * (pl.n.dot(p) - pl.d);  // plane_set.rs:74-76 (project)
+    out.push_back(Contact<R>{point, pl.n, depth});
+  }
+
+  // Prefilter of the fluid passes: a provider with bounds is skipped when p lies outside
+  // them expanded by m (fluid_density.rs:90-101, fluid_boundary.rs:60-71).
+  bool outside(const V3<R>& p, R m) const {
+    return has_bounds && (p.x < bmin.x - m || p.x > bmax.x + m || p.y < bmin.y - m || p.y > bmax.y + m ||
+                          p.z < bmin.z - m || p.z > bmax.z + m);
+  }
+};
+
 // ---------------------------------------------------------------- fluid system
 // crates/vxl-phys-fluid/src/system.rs:5-51 (fields) and fluid_access.rs:7-76 (new)
 template <class R>
@@ -547,6 +617,8 @@ struct FluidSystem {
   std::vector<Reaction<R>> breact;
   UniformGrid<R> grid;
   std::vector<std::pair<Shape<R>, BoundaryLattice<R>>> lattice_cache;
+  std::vector<Provider<R>> providers;  // the registered boundaries, in order
+  R skin;                              // fluid_access.rs:47 (0.15 h)
 
   // crates/vxl-phys-fluid/src/fluid_access.rs:7-76
   FluidSystem(const FluidConfig<R>& c, V3<R> origin, const size_t dims[3], R sp) : cfg(c) {
@@ -556,6 +628,7 @@ struct FluidSystem {
     ks = R(45.0f) / (pi_v<R>() * powi(h, 6));
     w0 = k6 * h2 * h2 * h2;
     b_tait = cfg.sound_speed * cfg.sound_speed * cfg.rest_density / cfg.gamma_tait;
+    skin = R(0.15f) * h;
     size_t n = dims[0] * dims[1] * dims[2];
     pos.reserve(n);
     for (size_t i = 0; i < dims[0]; ++i)
@@ -651,7 +724,7 @@ struct FluidSystem {
     }
   }
 
-  // crates/vxl-phys-fluid/src/fluid_step.rs:91-127 (substep; no providers)
+  // crates/vxl-phys-fluid/src/fluid_step.rs:91-127 (substep)
   void substep(R dt) {
     size_t nf = n_fluid;
     if (nf == 0) return;
@@ -660,6 +733,85 @@ struct FluidSystem {
     pressure_pass();
     force_pass();
     integrate(dt);
+    boundary_pass();
+  }
+
+  // crates/vxl-phys-fluid/src/fluid_density.rs:76-118 (wall_planes_in): the provider
+  // planes within h of a fluid particle (contact point + outward normal, 0 < sdf < h), <= 8.
+  size_t wall_planes(const V3<R>& pi, V3<R> pl_pt[8], V3<R> pl_n[8]) const {
+    size_t np = 0;
+    std::vector<Contact<R>> scratch;
+    for (const auto& pr : providers) {
+      if (pr.outside(pi, h)) continue;
+      scratch.clear();
+      pr.contacts_point(pi, h, scratch);
+      for (const auto& c : scratch) {
+        R sdf = (pi - c.point).dot(c.normal);
+        if (sdf > R(0) && sdf < h && np < 8) {
+          pl_pt[np] = c.point;
+          pl_n[np] = c.normal;
+          ++np;
+        }
+      }
+    }
+    return np;
+  }
+
+  // crates/vxl-phys-fluid/src/fluid_boundary.rs:45-101 (boundary_pass): fluid particles
+  // inside a provider are pushed out along each contact normal by min(pen + skin, h), their
+  // inward normal velocity removed; the pushed ones then go through separate_coincident.
+  void boundary_pass() {
+    if (providers.empty()) return;
+    std::vector<std::pair<size_t, V3<R>>> pushed;
+    std::vector<Contact<R>> contacts;
+    for (size_t i = 0; i < n_fluid; ++i) {
+      V3<R> pi = pos[i];
+      V3<R> p = pi, v = vel[i], n_sum;
+      bool hit = false;
+      for (const auto& pr : providers) {
+        if (pr.outside(pi, h)) continue;
+        contacts.clear();
+        pr.contacts_point(pi, skin, contacts);  // contacts_point_boundary
+        for (const auto& c : contacts) {
+          R sdf = (pi - c.point).dot(c.normal);
+          R pen = -sdf;
+          if (pen <= R(0)) continue;
+          p += c.normal * std::fmin(pen + skin, h);
+          n_sum += c.normal;
+          hit = true;
+          R vn = v.dot(c.normal);
+          if (vn < R(0)) v -= c.normal * vn;
+        }
+        pos[i] = p;
+        vel[i] = v;
+      }
+      if (hit) pushed.emplace_back(i, n_sum);
+    }
+    separate_coincident(pushed);
+  }
+
+  // crates/vxl-phys-fluid/src/fluid_boundary.rs:103-128: among the particles pushed this
+  // substep, in ascending index, each one closer than 0.2 h to an earlier one moves along
+  // its normal sum until r_min apart.
+  void separate_coincident(const std::vector<std::pair<size_t, V3<R>>>& pushed) {
+    R r_min = R(0.2f) * h;
+    for (size_t a = 0; a < pushed.size(); ++a) {
+      size_t ia = pushed[a].first;
+      V3<R> na = pushed[a].second;
+      R nl = na.length();
+      if (nl <= R(1e-9f)) continue;
+      V3<R> dir = na * (R(1) / nl);
+      V3<R> pa = pos[ia];
+      for (size_t b = 0; b < a; ++b) {
+        V3<R> d = pa - pos[pushed[b].first];
+        R r2 = d.length_squared();
+        if (r2 < r_min * r_min) {
+          R r = std::sqrt(r2);
+          pa += dir * (r_min - r);
+        }
+      }
+      pos[ia] = pa;
+    }
   }
 
   // crates/vxl-phys-fluid/src/fluid_step.rs:112-123
@@ -695,18 +847,31 @@ struct FluidSystem {
   }
 
   // crates/vxl-phys-fluid/src/fluid_density.rs:17-70 (serial) and :123-233 (parallel;
-  // bit-identical since each particle's walk order is unchanged). No provider walls, so
-  // the mirror-ghost loop (np = 0) contributes nothing.
+  // bit-identical since each particle's walk order is unchanged). Each neighbour's term is
+  // followed by its mirror ghosts in the particle's provider planes (fluid_density.rs:38-47).
   void density_pass() {
     size_t nf = n_fluid, nt = pos.size();
     parallel_for(0, nf, [&](size_t b, size_t e) {
+      V3<R> pl_pt[8], pl_n[8];
       for (size_t i = b; i < e; ++i) {
+        V3<R> pi = pos[i];
+        size_t np = providers.empty() ? 0 : wall_planes(pi, pl_pt, pl_n);
         R sum = w0, sum_b = R(0);
-        for_neighbors(i, [&](size_t j, const V3<R>&, R r2) {
+        for_neighbors(i, [&](size_t j, const V3<R>& d, R r2) {
           R t = h2 - r2;
           R w = k6 * t * t * t;
           if (j < nf) sum += w;
           else sum_b += pmass[j] * w;
+          for (size_t k = 0; k < np; ++k) {
+            V3<R> pj = pi - d;
+            R dn = (pj - pl_pt[k]).dot(pl_n[k]);
+            V3<R> g = pj - pl_n[k] * (R(2) * dn);
+            R rg2 = (pi - g).length_squared();
+            if (rg2 <= h2) {
+              R tg = h2 - rg2;
+              sum += k6 * tg * tg * tg;
+            }
+          }
         });
         dens[i] = mass * sum + sum_b;
       }

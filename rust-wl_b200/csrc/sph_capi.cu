@@ -218,6 +218,16 @@ vxl_status vxl_sph_read_rigid_bodies(vxl_sph_handle* h, uint32_t scene, vxl_sph_
   }
 }
 
+vxl_status vxl_sph_set_providers(vxl_sph_handle* h, uint32_t scene, const vxl_sph_provider* providers,
+                                 uint32_t nproviders, const vxl_sph_wall_plane* planes, uint32_t nplanes) {
+  HANDLE_OR_FAIL(h);
+  try {
+    return h->e->set_providers(scene, providers, nproviders, planes, nplanes);
+  } catch (...) {
+    return set_error(VXL_PANIC_CAUGHT, "exception in vxl_sph_set_providers");
+  }
+}
+
 vxl_status vxl_sph_set_body_lattice(vxl_sph_handle* h, uint32_t scene, const float* local_xyz,
                                     const uint32_t* body_index, uint64_t nb, uint32_t nbodies) {
   HANDLE_OR_FAIL(h);

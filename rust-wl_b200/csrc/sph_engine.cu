@@ -33,11 +33,12 @@ inline uint32_t blocks_for(uint64_t n, int t = kThreads) { return (uint32_t)((n 
 
 enum KernelId : int {
   KID_CELLOFF, KID_KEYS, KID_SCAN_PARTIAL, KID_SCAN_FINAL, KID_PLACE, KID_CANON,
-  KID_DENSITY, KID_FORCE, KID_BFORCE, KID_REACT_CHUNKS, KID_REACT_SPANS, KID_SCALE, KID_HALFMASK, KID_COUNT
+  KID_DENSITY, KID_FORCE, KID_BFORCE, KID_REACT_CHUNKS, KID_REACT_SPANS, KID_SCALE, KID_HALFMASK, KID_WALLS,
+  KID_COUNT
 };
 const char* const kKernelNames[KID_COUNT] = {
     "k_celloff", "k_keys", "k_scan_partial", "k_scan_final", "k_place", "k_canon",
-    "k_density", "k_force", "k_bforce", "k_react_chunks", "k_react_spans", "k_scale", "k_halfmask"};
+    "k_density", "k_force", "k_bforce", "k_react_chunks", "k_react_spans", "k_scale", "k_halfmask", "k_walls"};
 
 constexpr size_t kSceneHostBytes = offsetof(SceneDev, g);
 
@@ -207,6 +208,13 @@ void Engine::free_all() {
   ev_snap_ = nullptr;
   if (rb_d_) cudaFree(rb_d_);
   rb_d_ = nullptr;
+  void* wd[] = {prov_d_, wplanes_d_, pflag_, pnsum_, plist_, pblk_};
+  for (void* p : wd)
+    if (p) cudaFree(p);
+  prov_d_ = nullptr;
+  wplanes_d_ = nullptr;
+  pflag_ = plist_ = pblk_ = nullptr;
+  pnsum_ = nullptr;
   if (blocal_) cudaFree(blocal_);
   if (poses_d_) cudaFree(poses_d_);
   blocal_ = nullptr;
@@ -303,6 +311,8 @@ vxl_status Engine::push_scene_records(const std::vector<float>& dt) {
     r.vmax2 = r.vmax * r.vmax;
     r.base = si.base;
     r.count = si.nf + si.nb;
+    r.prov_first = q < prov_first_st_.size() ? prov_first_st_[q] : 0u;
+    r.prov_count = q < prov_count_st_.size() ? prov_count_st_[q] : 0u;
   }
   if (!scenes_.empty()) {
     CU(cudaMemcpy2DAsync(sc_d_, sizeof(SceneDev), sc_h_, sizeof(SceneDev), kSceneHostBytes, scenes_.size(),
@@ -435,6 +445,19 @@ vxl_status Engine::remove_scenes(const std::vector<uint32_t>& indices) {
   scenes_.swap(keep);
   spans_local_.swap(keep_spans);
   scene_bodies_.swap(keep_bodies);
+  if (!prov_h_.empty()) {  // provider walls follow their scenes
+    std::vector<std::vector<vxl_sph_provider>> kp;
+    std::vector<std::vector<vxl_sph_wall_plane>> kw;
+    for (uint32_t q = 0; q < drop.size(); ++q)
+      if (!drop[q]) {
+        kp.push_back(q < prov_h_.size() ? prov_h_[q] : std::vector<vxl_sph_provider>());
+        kw.push_back(q < wplanes_h_.size() ? wplanes_h_[q] : std::vector<vxl_sph_wall_plane>());
+      }
+    prov_h_.swap(kp);
+    wplanes_h_.swap(kw);
+    prov_first_st_.clear();  // restaged below, after the slots have moved
+    prov_count_st_.clear();
+  }
   if (!rigid_.empty()) {  // coupled bodies follow their scenes
     std::vector<std::vector<vxl_sph_rigid_body>> keep_rigid;
     for (uint32_t q = 0; q < drop.size(); ++q)
@@ -448,6 +471,7 @@ vxl_status Engine::remove_scenes(const std::vector<uint32_t>& indices) {
   vxl_status s = push_scene_records({});
   for (uint32_t q = 0; s == VXL_OK && q < scenes_.size(); ++q) s = recompute_scene_boxes(q);
   if (s == VXL_OK) s = rebuild_tiles();
+  if (s == VXL_OK && !prov_h_.empty()) s = stage_walls();
   return s;
 }
 
@@ -620,6 +644,121 @@ vxl_status Engine::step_coupled_async(float dt_tick, uint32_t rigid_substeps, co
   vxl_status st = step_tick_async(dt_tick);
   if (st != VXL_OK) return st;
   rb_have_reaction_ = nspans_ > 0;
+  return VXL_OK;
+}
+
+// ---------------------------------------------------------------- provider walls
+
+vxl_status Engine::set_providers(uint32_t q, const vxl_sph_provider* pr, uint32_t n, const vxl_sph_wall_plane* planes,
+                                 uint32_t nplanes) {
+  if (q >= scenes_.size()) return set_error(VXL_INVALID_ARGUMENT, "scene index out of range");
+  if (n && !pr) return set_error(VXL_NULL_POINTER, "providers is NULL");
+  if (nplanes && !planes) return set_error(VXL_NULL_POINTER, "planes is NULL");
+  if (n > VXL_SPH_MAX_PROVIDER_PLANES || nplanes > VXL_SPH_MAX_PROVIDER_PLANES)
+    return set_error(VXL_INVALID_ARGUMENT, "at most 64 providers and 64 planes per scene");
+  auto finite3 = [](const float* v) { return std::isfinite(v[0]) && std::isfinite(v[1]) && std::isfinite(v[2]); };
+  for (uint32_t i = 0; i < n; ++i) {
+    const vxl_sph_provider& p = pr[i];
+    if (p.kind != VXL_SPH_PROVIDER_FACES && p.kind != VXL_SPH_PROVIDER_CONVEX)
+      return set_error(VXL_INVALID_ARGUMENT, "unknown provider kind");
+    if (p.first_plane > nplanes || p.nplanes > nplanes - p.first_plane)
+      return set_error(VXL_INVALID_ARGUMENT, "provider planes out of range");
+    if (p.has_bounds > 1u || (p.has_bounds && (!finite3(p.bounds_min) || !finite3(p.bounds_max))))
+      return set_error(VXL_INVALID_ARGUMENT, "provider bounds must be finite");
+    for (uint32_t k = p.first_plane; k < p.first_plane + p.nplanes; ++k) {
+      const vxl_sph_wall_plane& w = planes[k];
+      if (!std::isfinite(w.offset)) return set_error(VXL_INVALID_ARGUMENT, "plane offset must be finite");
+      if (p.kind == VXL_SPH_PROVIDER_FACES && (w.axis > 2u || (w.sign != 1.0f && w.sign != -1.0f)))
+        return set_error(VXL_INVALID_ARGUMENT, "a face needs axis 0..2 and sign +1 or -1");
+      if (p.kind == VXL_SPH_PROVIDER_CONVEX && !finite3(w.normal))
+        return set_error(VXL_INVALID_ARGUMENT, "plane normal must be finite");
+    }
+  }
+  CU(cudaSetDevice(device_));
+  prof_collect();
+  if (prov_h_.size() < scenes_.size()) {
+    prov_h_.resize(scenes_.size());
+    wplanes_h_.resize(scenes_.size());
+  }
+  prov_h_[q].assign(pr, pr + n);
+  wplanes_h_[q].assign(planes, planes + nplanes);
+  return stage_walls();
+}
+
+// Upload every scene's providers and planes (global plane indices), size the per-substep
+// buffers of the wall passes, and republish the scene records. Runs with the device idle.
+vxl_status Engine::stage_walls() {
+  CU(cudaStreamSynchronize(stream_));
+  if (side_) CU(cudaStreamSynchronize(side_));
+  side_pending_ = false;
+  std::vector<ProviderDev> hp;
+  std::vector<WallPlaneDev> hw;
+  prov_first_st_.assign(scenes_.size(), 0u);
+  prov_count_st_.assign(scenes_.size(), 0u);
+  for (uint32_t q = 0; q < scenes_.size() && q < prov_h_.size(); ++q) {
+    prov_first_st_[q] = (uint32_t)hp.size();
+    prov_count_st_[q] = (uint32_t)prov_h_[q].size();
+    const uint32_t wbase = (uint32_t)hw.size();
+    for (const vxl_sph_wall_plane& w : wplanes_h_[q]) {
+      WallPlaneDev d{};
+      d.nx = w.normal[0];
+      d.ny = w.normal[1];
+      d.nz = w.normal[2];
+      d.d = w.offset;
+      d.axis = w.axis;
+      d.sign = w.sign;
+      hw.push_back(d);
+    }
+    for (const vxl_sph_provider& p : prov_h_[q]) {
+      ProviderDev d{};
+      d.kind = p.kind;
+      d.first = wbase + p.first_plane;
+      d.count = p.nplanes;
+      d.has_bounds = p.has_bounds;
+      d.bminx = p.bounds_min[0];
+      d.bminy = p.bounds_min[1];
+      d.bminz = p.bounds_min[2];
+      d.bmaxx = p.bounds_max[0];
+      d.bmaxy = p.bounds_max[1];
+      d.bmaxz = p.bounds_max[2];
+      hp.push_back(d);
+    }
+  }
+  walls_any_ = !hp.empty();
+  if (hp.size() > prov_cap_) {
+    if (prov_d_) cudaFree(prov_d_);
+    prov_d_ = nullptr;
+    prov_cap_ = 0;
+    vxl_status s = dalloc(&prov_d_, hp.size());
+    if (s != VXL_OK) return s;
+    prov_cap_ = (uint32_t)hp.size();
+  }
+  if (hw.size() > wplanes_cap_) {
+    if (wplanes_d_) cudaFree(wplanes_d_);
+    wplanes_d_ = nullptr;
+    wplanes_cap_ = 0;
+    vxl_status s = dalloc(&wplanes_d_, hw.size());
+    if (s != VXL_OK) return s;
+    wplanes_cap_ = (uint32_t)hw.size();
+  }
+  if (!hp.empty()) CU(cudaMemcpy(prov_d_, hp.data(), hp.size() * sizeof(ProviderDev), cudaMemcpyHostToDevice));
+  if (!hw.empty()) CU(cudaMemcpy(wplanes_d_, hw.data(), hw.size() * sizeof(WallPlaneDev), cudaMemcpyHostToDevice));
+  if (walls_any_ && !pflag_) {
+    vxl_status s = dalloc(&pflag_, slot_cap_);
+    if (s == VXL_OK) s = dalloc((float4**)&pnsum_, slot_cap_);
+    if (s == VXL_OK) s = dalloc(&plist_, slot_cap_);
+    if (s == VXL_OK) s = dalloc(&pblk_, slot_cap_ / kPushedChunk + 2);
+    if (s != VXL_OK) return s;
+  }
+  if (pflag_) CU(cudaMemset(pflag_, 0, slot_cap_ * sizeof(uint32_t)));
+  std::vector<float> dts(scenes_.size());
+  for (uint32_t q = 0; q < scenes_.size(); ++q) dts[q] = sc_h_[q].dt;
+  vxl_status s = push_scene_records(dts);
+  if (s != VXL_OK) return s;
+  if (graph_) {  // the tick's kernels and buffers changed
+    cudaGraphExecDestroy(graph_);
+    graph_ = nullptr;
+  }
   return VXL_OK;
 }
 
@@ -1056,12 +1195,22 @@ void Engine::enqueue_substep(bool with_reactions) {
   const uint32_t gd = grid_density_ ? (uint32_t)grid_density_ : per_tile;
   const uint32_t gf = grid_force_ ? (uint32_t)grid_force_ : per_tile;
   const uint32_t gb = grid_bforce_ ? (uint32_t)grid_bforce_ : std::max<uint32_t>(nbtiles_, 1);
-  if (tuning_.block == 128)
+  if (walls_any_) {  // provider walls: the variant with mirror ghosts
+    if (tuning_.block == 128)
+      LAUNCH(KID_DENSITY, k_e_density<128, true><<<gd, 128, 0, st>>>(
+                              p1, start_, sc_d_, tiles_d_, ntiles_, ctl_d_, halves_, (float2*)rc_, press_, nbr_, nbr_n_,
+                              nbr_cap_, stride, prov_d_, wplanes_d_));
+    else
+      LAUNCH(KID_DENSITY, k_e_density<256, true><<<gd, 256, 0, st>>>(
+                              p1, start_, sc_d_, tiles_d_, ntiles_, ctl_d_, halves_, (float2*)rc_, press_, nbr_, nbr_n_,
+                              nbr_cap_, stride, prov_d_, wplanes_d_));
+  } else if (tuning_.block == 128) {
     LAUNCH(KID_DENSITY, k_e_density<128><<<gd, 128, 0, st>>>(p1, start_, sc_d_, tiles_d_, ntiles_, ctl_d_, halves_,
                                                              (float2*)rc_, press_, nbr_, nbr_n_, nbr_cap_, stride));
-  else
+  } else {
     LAUNCH(KID_DENSITY, k_e_density<256><<<gd, 256, 0, st>>>(p1, start_, sc_d_, tiles_d_, ntiles_, ctl_d_, halves_,
                                                              (float2*)rc_, press_, nbr_, nbr_n_, nbr_cap_, stride));
+  }
   // Reaction branch on the side stream: it reads only the sorted buffer, the densities and
   // the lists, so it runs beside the force pass (which writes the other buffer).
   const bool bforce = nb_total > 0 && ((with_reactions && nspans_ > 0) || rec);
@@ -1099,6 +1248,23 @@ void Engine::enqueue_substep(bool with_reactions) {
                           p1, v1, (const float2*)rc_, start_, nbr_, nbr_n_, nbr_cap_, stride, sc_d_, tiles_d_,
                           ntiles_, ctl_d_, (float4*)pos_[0], (float4*)vel_[0], rec ? (float4*)acc_ : nullptr,
                           rec ? (float4*)xsph_ : nullptr));
+  if (walls_any_) {
+    // boundary_pass of the scenes with providers, on the integrated state (pos_[0], vel_[0],
+    // same slot order as the sorted buffer, so orig_ / slot_of_ apply)
+    const uint32_t nref = (uint32_t)used_;
+    const uint32_t nblk = std::max<uint32_t>((nref + kPushedChunk - 1) / kPushedChunk, 1);
+    LAUNCH(KID_WALLS, k_e_wall_project<<<key_blocks, kThreads, 0, st>>>(
+                          (float4*)pos_[0], (float4*)vel_[0], sc_d_, tiles_d_, ntiles_, ctl_d_, prov_d_, wplanes_d_,
+                          orig_, pflag_, (float4*)pnsum_));
+    LAUNCH(KID_WALLS, k_e_pushed_count<<<nblk, kThreads, 0, st>>>(pflag_, nref, ctl_d_, pblk_));
+    LAUNCH(KID_WALLS, k_e_pushed_emit<<<nblk, kThreads, 0, st>>>(pflag_, nref, pblk_, ctl_d_, plist_));
+    LAUNCH(KID_WALLS, k_e_separate_check<<<148 * 2, kThreads, 0, st>>>((const float4*)pos_[0], sc_d_, plist_,
+                                                                          (const float4*)pnsum_, slot_of_, ctl_d_));
+    LAUNCH(KID_WALLS, k_e_separate<<<1, 1024, 0, st>>>((float4*)pos_[0], sc_d_, S, plist_, (const float4*)pnsum_,
+                                                         slot_of_, ctl_d_));
+    LAUNCH(KID_WALLS, k_e_wall_rebox<<<key_blocks, kThreads, 0, st>>>((const float4*)pos_[0], sc_d_, tiles_d_,
+                                                                        ntiles_, ctl_d_));
+  }
 }
 
 void Engine::enqueue_tick(float /*dt_tick*/) {
@@ -1146,7 +1312,7 @@ vxl_status Engine::step_tick_async(float dt_tick) {
   }
   vxl_status s = stage_spans();
   if (s != VXL_OK) return s;
-  const uint32_t key = (record_ ? 1u : 0u) | (prof_ ? 2u : 0u) | (sub << 2);
+  const uint32_t key = (record_ ? 1u : 0u) | (prof_ ? 2u : 0u) | (walls_any_ ? 4u : 0u) | (sub << 3);
   launches_counter_ = 0;
   if (!use_graph_) {
     prof_used_ = 0;

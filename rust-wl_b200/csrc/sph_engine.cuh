@@ -55,7 +55,8 @@ struct SceneDev {
   float dt, vmax, vmax2, pad0;
   uint32_t base;        // first slot
   uint32_t count;       // slots (fluid + boundary)
-  uint32_t pad1[2];
+  uint32_t prov_first;  // the scene's providers in the engine's provider array
+  uint32_t prov_count;  // 0: no provider walls
   GridBox g;            // this substep's grid
   uint32_t cell_off;    // first global cell this substep
   uint32_t cells;       // cells this substep
@@ -116,8 +117,32 @@ struct EngineCtl {
   uint32_t work[kWorkSlots];
 };
 
-// Work counter indices.
-enum WorkId : int { kWorkDensity = 0, kWorkForce = 1, kWorkBforce = 2, kWorkScan = 3 };
+// Work counter indices (zeroed at the start of every substep). The provider-wall passes
+// keep their per-substep results in slots 4-6: pushed particles, "some pushed pair is
+// closer than 0.2 h", "the separation moved a particle".
+enum WorkId : int {
+  kWorkDensity = 0, kWorkForce = 1, kWorkBforce = 2, kWorkScan = 3,
+  kWorkPushed = 4, kWorkTrigger = 5, kWorkMoved = 6
+};
+
+// Provider walls (analytic ProviderColliders queried on the device). A plane of a FACES
+// provider is (axis, d = plane coordinate, sign); of a CONVEX provider (n, d).
+struct WallPlaneDev {
+  float nx, ny, nz, d;
+  uint32_t axis;
+  float sign;
+  uint32_t pad0, pad1;
+};
+
+struct ProviderDev {
+  uint32_t kind, first, count, has_bounds;
+  float bminx, bminy, bminz, bmaxx, bmaxy, bmaxz;
+  uint32_t pad0, pad1;
+};
+
+constexpr uint32_t kProviderFaces = 0u, kProviderConvex = 1u;
+constexpr uint32_t kMaxWallPlanes = 8;     // mirror planes per particle (fluid_density.rs:110)
+constexpr uint32_t kPushedChunk = 4096;    // reference indices per block of the pushed-list passes
 
 namespace {
 
@@ -897,6 +922,60 @@ __device__ __forceinline__ void walk27_half(const GridBox& g, const uint32_t* __
   }
 }
 
+// ---------------------------------------------------------------- provider walls
+// ProviderColliders::bounds prefilter of the fluid passes: skip the provider when p lies
+// outside its bounds expanded by m (fluid_density.rs:90-101, fluid_boundary.rs:60-71).
+__device__ __forceinline__ bool provider_outside(const ProviderDev& pr, float x, float y, float z, float m) {
+  return pr.has_bounds && (x < pr.bminx - m || x > pr.bmaxx + m || y < pr.bminy - m || y > pr.bmaxy + m ||
+                           z < pr.bminz - m || z > pr.bmaxz + m);
+}
+
+// contacts_point(p, probe) of one provider, calling emit(point xyz, outward normal xyz) for
+// each contact in the provider's order. FACES: every face with (p[axis] - plane) * sign <=
+// 2 probe, at p with that coordinate set to the plane (crates/vxl-phys-fluid/src/tests.rs:
+// 81-110). CONVEX: the decisive plane (largest n.p - d) when -(n.p - d) >= -probe, at
+// p - n (n.p - d) (crates/vxl-phys-terrain/src/plane_set.rs:60-76, 166-181).
+template <class F>
+__device__ __forceinline__ void provider_contacts(const ProviderDev& pr, const WallPlaneDev* __restrict__ pl,
+                                                  float px, float py, float pz, float probe, F&& emit) {
+  if (pr.kind == kProviderFaces) {
+    for (uint32_t k = pr.first; k < pr.first + pr.count; ++k) {
+      const WallPlaneDev f = pl[k];
+      const float comp = f.axis == 0u ? px : (f.axis == 1u ? py : pz);
+      const float sdf = (comp - f.d) * f.sign;
+      if (sdf > 2.0f * probe) continue;
+      float cx = px, cy = py, cz = pz, nx = 0.0f, ny = 0.0f, nz = 0.0f;
+      if (f.axis == 0u) {
+        cx = f.d;
+        nx = f.sign;
+      } else if (f.axis == 1u) {
+        cy = f.d;
+        ny = f.sign;
+      } else {
+        cz = f.d;
+        nz = f.sign;
+      }
+      emit(cx, cy, cz, nx, ny, nz);
+    }
+    return;
+  }
+  if (pr.count == 0u) return;
+  float best = -INFINITY;
+  uint32_t kb = pr.first;
+  for (uint32_t k = pr.first; k < pr.first + pr.count; ++k) {
+    const WallPlaneDev q = pl[k];
+    const float sd = (q.nx * px + q.ny * py + q.nz * pz) - q.d;
+    if (sd > best) {
+      best = sd;
+      kb = k;
+    }
+  }
+  if (-best < -probe) return;
+  const WallPlaneDev q = pl[kb];
+  const float t = (q.nx * px + q.ny * py + q.nz * pz) - q.d;
+  emit(px - q.nx * t, py - q.ny * t, pz - q.nz * t, q.nx, q.ny, q.nz);
+}
+
 // Density (poly6 with self term) + Tait EOS, persistent over tiles, one thread per slot.
 // Fluid: rho = mass * (w0 + sum_fluid W) + sum_boundary pmass_j W
 // (crates/vxl-phys-fluid/src/fluid_density.rs:24-51); boundary: rho = pmass_i w0 +
@@ -905,12 +984,17 @@ __device__ __forceinline__ void walk27_half(const GridBox& g, const uint32_t* __
 // walk order, the slots of the neighbours that contributed (all for fluid, fluid ones for
 // boundary particles): nbr[k * stride + s], k < cap, with the full count in nbr_n[s]
 // (a count above cap sends the consumers back to walking the cells).
-template <int kBlock>
+// kWalls: scenes with provider walls add, for a fluid particle, after each neighbour's term
+// its mirror ghosts in the particle's provider planes (0 < sdf < h, at most 8; ghost
+// g = pj - 2 ((pj - point).n) n with pj = pi - d, W(|pi - g|) if within h), in the
+// reference's order (wall_planes_in and the ghost loop, fluid_density.rs:25-47, 76-118).
+template <int kBlock, bool kWalls = false>
 __global__ void __launch_bounds__(kBlock, VXL_DENSITY_THREADS_PER_SM / kBlock) k_e_density(
     const float4* __restrict__ pos, const uint32_t* __restrict__ start, const SceneDev* __restrict__ sc,
     const TileDev* __restrict__ tiles, uint32_t ntiles, EngineCtl* ctl, const uint32_t* __restrict__ halves,
     float2* __restrict__ rc, float* __restrict__ press_out, uint32_t* __restrict__ nbr,
-    uint32_t* __restrict__ nbr_n, uint32_t cap, uint32_t stride) {
+    uint32_t* __restrict__ nbr_n, uint32_t cap, uint32_t stride, const ProviderDev* __restrict__ prov = nullptr,
+    const WallPlaneDev* __restrict__ wplanes = nullptr) {
   if (ctl->err & kErrCellCap) return;
   for (uint32_t t = first_tile(&ctl->work[kWorkDensity], ntiles); t < ntiles; t = following_tile(&ctl->work[kWorkDensity], ntiles)) {
     const TileDev td = tiles[t];
@@ -930,6 +1014,27 @@ __global__ void __launch_bounds__(kBlock, VXL_DENSITY_THREADS_PER_SM / kBlock) k
       float sum_b = 0.0f;
       uint32_t cnt = 0;
       uint32_t* wp = nbr + s;  // next list entry: nbr[cnt * stride + s]
+      float wpt[kWalls ? 3 * kMaxWallPlanes : 1], wn[kWalls ? 3 * kMaxWallPlanes : 1];
+      uint32_t np = 0;
+      if (kWalls && fluid_i) {
+        for (uint32_t q = S.prov_first; q < S.prov_first + S.prov_count; ++q) {
+          const ProviderDev pr = prov[q];
+          if (provider_outside(pr, pi.x, pi.y, pi.z, h)) continue;
+          provider_contacts(pr, wplanes, pi.x, pi.y, pi.z, h,
+                            [&](float cx_, float cy_, float cz_, float nx_, float ny_, float nz_) {
+                              const float sdf = (pi.x - cx_) * nx_ + (pi.y - cy_) * ny_ + (pi.z - cz_) * nz_;
+                              if (sdf > 0.0f && sdf < h && np < kMaxWallPlanes) {
+                                wpt[3 * np] = cx_;
+                                wpt[3 * np + 1] = cy_;
+                                wpt[3 * np + 2] = cz_;
+                                wn[3 * np] = nx_;
+                                wn[3 * np + 1] = ny_;
+                                wn[3 * np + 2] = nz_;
+                                ++np;
+                              }
+                            });
+        }
+      }
       auto visit = [&](uint32_t j) {  // j != s (the callers skip it)
         const float4 pj = pos[j];
         const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
@@ -941,6 +1046,21 @@ __global__ void __launch_bounds__(kBlock, VXL_DENSITY_THREADS_PER_SM / kBlock) k
           if (fluid_i) {
             if (pj.w > 0.0f) sum += w;
             else sum_b += (-pj.w) * w;
+            if (kWalls) {
+              for (uint32_t q = 0; q < np; ++q) {
+                const float qx = pi.x - dx, qy = pi.y - dy, qz = pi.z - dz;  // pj = pi - d
+                const float dn = (qx - wpt[3 * q]) * wn[3 * q] + (qy - wpt[3 * q + 1]) * wn[3 * q + 1] +
+                                 (qz - wpt[3 * q + 2]) * wn[3 * q + 2];
+                const float t2 = 2.0f * dn;
+                const float ex = pi.x - (qx - wn[3 * q] * t2), ey = pi.y - (qy - wn[3 * q + 1] * t2),
+                            ez = pi.z - (qz - wn[3 * q + 2] * t2);
+                const float rg2 = ex * ex + ey * ey + ez * ez;
+                if (rg2 <= h2) {
+                  const float tg = h2 - rg2;
+                  sum += k6 * tg * tg * tg;
+                }
+              }
+            }
           } else if (pj.w > 0.0f) {
             sum += pj.w * w;
           } else {
@@ -1087,7 +1207,266 @@ __global__ void __launch_bounds__(kBlock, VXL_FORCE_THREADS_PER_SM / kBlock) k_e
           vel_out[s] = make_float4(ux, uy, uz, 0.0f);
         }
       }
-      block_bbox_accumulate(S.fbox, nx, ny, nz, valid && fluid_i);
+      // scenes with provider walls take their fluid AABB after the projection pass
+      if (S.prov_count == 0u) block_bbox_accumulate(S.fbox, nx, ny, nz, valid && fluid_i);
+    }
+  }
+}
+
+// ---------------------------------------------------------------- provider walls after integration
+// boundary_pass (crates/vxl-phys-fluid/src/fluid_boundary.rs:45-101) on the integrated state of
+// the scenes with providers, one thread per fluid slot: for each contact of each provider at the
+// integrated position pi (probe = skin = 0.15 h) with penetration pen = -(pi - point).n > 0, the
+// particle moves by n min(pen + skin, h) and loses its inward normal velocity; the normal sum of a
+// pushed particle is kept for the separation, by reference index (pflag, pnsum; w = scene).
+// The scene's fluid AABB for the next grid is accumulated here, from the projected positions.
+__global__ void k_e_wall_project(float4* __restrict__ pos, float4* __restrict__ vel, SceneDev* __restrict__ sc,
+                                 const TileDev* __restrict__ tiles, uint32_t ntiles, const EngineCtl* __restrict__ ctl,
+                                 const ProviderDev* __restrict__ prov, const WallPlaneDev* __restrict__ wplanes,
+                                 const uint32_t* __restrict__ orig, uint32_t* __restrict__ pflag,
+                                 float4* __restrict__ pnsum) {
+  if (ctl->err & kErrCellCap) return;
+  for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const TileDev td = tiles[t];
+    SceneDev& S = sc[td.scene];
+    if (S.prov_count == 0u) continue;  // uniform over the block
+    const float h = S.k.h, skin = 0.15f * h;  // fluid_access.rs:47
+    for (uint32_t b0 = 0; b0 < td.count; b0 += blockDim.x) {
+      const uint32_t i = b0 + threadIdx.x;
+      const bool valid = i < td.count;
+      float x = 0.0f, y = 0.0f, z = 0.0f;
+      bool fluid = false;
+      if (valid) {
+        const uint32_t sl = td.first + i;
+        const float4 p = pos[sl];
+        fluid = p.w > 0.0f;
+        x = p.x;
+        y = p.y;
+        z = p.z;
+        if (fluid) {
+          const float4 v = vel[sl];
+          float vx = v.x, vy = v.y, vz = v.z, nsx = 0.0f, nsy = 0.0f, nsz = 0.0f;
+          bool hit = false;
+          for (uint32_t q = S.prov_first; q < S.prov_first + S.prov_count; ++q) {
+            const ProviderDev pr = prov[q];
+            if (provider_outside(pr, p.x, p.y, p.z, h)) continue;
+            provider_contacts(pr, wplanes, p.x, p.y, p.z, skin,
+                              [&](float cx, float cy, float cz, float nx, float ny, float nz) {
+                                const float sdf = (p.x - cx) * nx + (p.y - cy) * ny + (p.z - cz) * nz;
+                                const float pen = -sdf;
+                                if (pen <= 0.0f) return;
+                                const float m = fminf(pen + skin, h);
+                                x = x + nx * m;
+                                y = y + ny * m;
+                                z = z + nz * m;
+                                nsx = nsx + nx;
+                                nsy = nsy + ny;
+                                nsz = nsz + nz;
+                                hit = true;
+                                const float vn = vx * nx + vy * ny + vz * nz;
+                                if (vn < 0.0f) {
+                                  vx = vx - nx * vn;
+                                  vy = vy - ny * vn;
+                                  vz = vz - nz * vn;
+                                }
+                              });
+          }
+          pos[sl] = make_float4(x, y, z, p.w);
+          vel[sl] = make_float4(vx, vy, vz, v.w);
+          const uint32_t o = orig[sl];
+          pflag[o] = hit ? 1u : 0u;
+          if (hit) pnsum[o] = make_float4(nsx, nsy, nsz, __uint_as_float(td.scene));
+        }
+      }
+      block_bbox_accumulate(S.fbox, x, y, z, valid && fluid);
+    }
+  }
+}
+
+// The pushed particles in ascending reference index (plist), in two passes over chunks of
+// kPushedChunk indices: per-chunk counts, then each chunk's entries at its offset. The last
+// chunk stores the total in ctl->work[kWorkPushed].
+__device__ __forceinline__ uint32_t block_sum(uint32_t v, uint32_t* sh) {
+  for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+  __syncthreads();
+  if (lane == 0) sh[wid] = v;
+  __syncthreads();
+  uint32_t tot = 0;
+  for (int w = 0; w < nw; ++w) tot += sh[w];
+  return tot;
+}
+
+__global__ void k_e_pushed_count(const uint32_t* __restrict__ pflag, uint32_t n, const EngineCtl* __restrict__ ctl,
+                                 uint32_t* __restrict__ blk) {
+  if (ctl->err & kErrCellCap) return;
+  __shared__ uint32_t sh[32];
+  const uint32_t base = blockIdx.x * kPushedChunk;
+  uint32_t c = 0;
+  for (uint32_t k = threadIdx.x; k < kPushedChunk; k += blockDim.x) {
+    const uint32_t o = base + k;
+    if (o < n && pflag[o]) ++c;
+  }
+  c = block_sum(c, sh);
+  if (threadIdx.x == 0) blk[blockIdx.x] = c;
+}
+
+__global__ void k_e_pushed_emit(const uint32_t* __restrict__ pflag, uint32_t n, const uint32_t* __restrict__ blk,
+                                EngineCtl* __restrict__ ctl, uint32_t* __restrict__ plist) {
+  if (ctl->err & kErrCellCap) return;
+  __shared__ uint32_t sh[32], wtot[32];
+  uint32_t part = 0;
+  for (uint32_t k = threadIdx.x; k < blockIdx.x; k += blockDim.x) part += blk[k];
+  uint32_t off = block_sum(part, sh);
+  const uint32_t base = blockIdx.x * kPushedChunk;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+  for (uint32_t r0 = 0; r0 < kPushedChunk; r0 += blockDim.x) {
+    const uint32_t o = base + r0 + threadIdx.x;
+    const bool f = o < n && pflag[o] != 0u;
+    const uint32_t bal = __ballot_sync(0xffffffffu, f);
+    __syncthreads();
+    if (lane == 0) wtot[wid] = __popc(bal);
+    __syncthreads();
+    uint32_t before = 0, total = 0;
+    for (int w = 0; w < nw; ++w) {
+      if (w < wid) before += wtot[w];
+      total += wtot[w];
+    }
+    if (f) plist[off + before + __popc(bal & ((1u << lane) - 1u))] = o;
+    off += total;
+  }
+  if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) ctl->work[kWorkPushed] = off;
+}
+
+// First position in the ascending list a[0, n) whose value is >= key.
+__device__ __forceinline__ uint32_t lower_bound_u32(const uint32_t* __restrict__ a, uint32_t n, uint32_t key) {
+  uint32_t lo = 0, hi = n;
+  while (lo < hi) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (a[mid] < key) lo = mid + 1;
+    else hi = mid;
+  }
+  return lo;
+}
+
+// separate_coincident (fluid_boundary.rs:103-128) moves a pushed particle only if some
+// earlier pushed particle of its scene lies closer than r_min = 0.2 h. If no pair is that
+// close at the projected positions, nothing moves (by induction over the sequential loop):
+// this pass, one thread per pushed particle, decides whether the sequential pass must run.
+// A scene's reference indices are [base, base + count), so its pushed particles are one run
+// of the ascending list, found by binary search.
+__global__ void k_e_separate_check(const float4* __restrict__ pos, const SceneDev* __restrict__ sc,
+                                   const uint32_t* __restrict__ plist, const float4* __restrict__ pnsum,
+                                   const uint32_t* __restrict__ slot_of, EngineCtl* __restrict__ ctl) {
+  if (ctl->err & kErrCellCap) return;
+  const uint32_t P = ctl->work[kWorkPushed];
+  for (uint32_t a = blockIdx.x * blockDim.x + threadIdx.x; a < P; a += gridDim.x * blockDim.x) {
+    const uint32_t oa = plist[a];
+    const float4 na = pnsum[oa];
+    const float nl = sqrtf(na.x * na.x + na.y * na.y + na.z * na.z);
+    if (nl <= 1e-9f) continue;  // never moves
+    const uint32_t q = __float_as_uint(na.w);
+    const float r_min = 0.2f * sc[q].k.h;
+    const float rm2 = r_min * r_min;
+    if (*(volatile const uint32_t*)&ctl->work[kWorkTrigger]) return;
+    const float4 pa = pos[slot_of[oa]];
+    for (uint32_t b = lower_bound_u32(plist, a, sc[q].base); b < a; ++b) {
+      const float4 pb = pos[slot_of[plist[b]]];
+      const float dx = pa.x - pb.x, dy = pa.y - pb.y, dz = pa.z - pb.z;
+      if (dx * dx + dy * dy + dz * dz < rm2) {
+        atomicOr(&ctl->work[kWorkTrigger], 1u);
+        break;
+      }
+    }
+  }
+}
+
+// The sequential separation itself, one block, only when the check found a close pair: for
+// each pushed particle a in order (normal sum n_a, |n_a| > 1e-9), for each earlier pushed b of
+// its scene in order, with the current (already separated) positions: if |pa - pb|^2 < r_min^2,
+// pa += n_a / |n_a| (r_min - |pa - pb|). The block tests a window of b in parallel against the
+// current pa and applies the first hit, then resumes after it. If anything moved, the AABB
+// accumulators of the scenes with providers are reset for k_e_wall_rebox.
+__global__ void __launch_bounds__(1024) k_e_separate(float4* __restrict__ pos, SceneDev* __restrict__ sc,
+                                                     uint32_t nscenes, const uint32_t* __restrict__ plist,
+                                                     const float4* __restrict__ pnsum,
+                                                     const uint32_t* __restrict__ slot_of, EngineCtl* __restrict__ ctl) {
+  if ((ctl->err & kErrCellCap) || !ctl->work[kWorkTrigger]) return;
+  const uint32_t P = ctl->work[kWorkPushed];
+  __shared__ float4 pa_s;
+  __shared__ uint32_t first;
+  bool moved = false;  // thread 0
+  for (uint32_t a = 0; a < P; ++a) {
+    const uint32_t oa = plist[a];
+    const float4 na = pnsum[oa];
+    const float nl = sqrtf(na.x * na.x + na.y * na.y + na.z * na.z);
+    if (nl <= 1e-9f) continue;  // uniform over the block
+    const uint32_t q = __float_as_uint(na.w);
+    const float r_min = 0.2f * sc[q].k.h;
+    const float rm2 = r_min * r_min;
+    const float inv = 1.0f / nl;
+    const float dirx = na.x * inv, diry = na.y * inv, dirz = na.z * inv;
+    const uint32_t sa = slot_of[oa];
+    if (threadIdx.x == 0) pa_s = pos[sa];
+    __syncthreads();
+    uint32_t b0 = lower_bound_u32(plist, a, sc[q].base);  // the scene's first pushed particle
+    while (b0 < a) {
+      if (threadIdx.x == 0) first = 0xffffffffu;
+      __syncthreads();
+      const float4 cur = pa_s;
+      const uint32_t b = b0 + threadIdx.x;
+      if (b < a) {
+        const float4 pb = pos[slot_of[plist[b]]];
+        const float dx = cur.x - pb.x, dy = cur.y - pb.y, dz = cur.z - pb.z;
+        if (dx * dx + dy * dy + dz * dz < rm2) atomicMin(&first, b);
+      }
+      __syncthreads();
+      const uint32_t f = first;
+      if (f == 0xffffffffu) {
+        b0 += blockDim.x;
+      } else {
+        if (threadIdx.x == 0) {
+          const float4 pb = pos[slot_of[plist[f]]];
+          const float dx = cur.x - pb.x, dy = cur.y - pb.y, dz = cur.z - pb.z;
+          const float r = sqrtf(dx * dx + dy * dy + dz * dz);
+          const float m = r_min - r;
+          pa_s = make_float4(cur.x + dirx * m, cur.y + diry * m, cur.z + dirz * m, cur.w);
+          moved = true;
+        }
+        b0 = f + 1;
+      }
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) pos[sa] = pa_s;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0 && moved) {
+    ctl->work[kWorkMoved] = 1u;
+    for (uint32_t q = 0; q < nscenes; ++q)
+      if (sc[q].prov_count) {
+        for (int c = 0; c < 3; ++c) {
+          sc[q].fbox[c] = 0xffffffffu;
+          sc[q].fbox[3 + c] = 0u;
+        }
+      }
+  }
+}
+
+// After a separation that moved particles: the fluid AABB of the scenes with providers again,
+// from the final positions.
+__global__ void k_e_wall_rebox(const float4* __restrict__ pos, SceneDev* __restrict__ sc,
+                               const TileDev* __restrict__ tiles, uint32_t ntiles, const EngineCtl* __restrict__ ctl) {
+  if ((ctl->err & kErrCellCap) || !ctl->work[kWorkMoved]) return;
+  for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const TileDev td = tiles[t];
+    SceneDev& S = sc[td.scene];
+    if (S.prov_count == 0u) continue;
+    for (uint32_t b0 = 0; b0 < td.count; b0 += blockDim.x) {
+      const uint32_t i = b0 + threadIdx.x;
+      const bool valid = i < td.count;
+      float4 p = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+      if (valid) p = pos[td.first + i];
+      block_bbox_accumulate(S.fbox, p.x, p.y, p.z, valid && p.w > 0.0f);
     }
   }
 }

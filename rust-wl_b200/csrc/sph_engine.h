@@ -23,6 +23,8 @@ struct SpanDev;
 struct SpanChunk;
 struct BodyPoseDev;
 struct RigidBodyDev;
+struct ProviderDev;
+struct WallPlaneDev;
 
 // Launch shape of the particle passes (chosen by the autotuner for batches).
 struct Tuning {
@@ -79,6 +81,10 @@ class Engine {
   vxl_status step_coupled_async(float dt_tick, uint32_t rigid_substeps, const float gravity[3], float max_linear,
                                 float max_angular);
   vxl_status read_rigid_bodies(uint32_t scene, vxl_sph_rigid_body* out, uint32_t n);
+  // Provider walls of a scene (analytic ProviderColliders queried on the device every
+  // substep: mirror ghosts in the density, projection and separation after integration).
+  vxl_status set_providers(uint32_t scene, const vxl_sph_provider* providers, uint32_t n,
+                           const vxl_sph_wall_plane* planes, uint32_t nplanes);
   vxl_status write_state(uint32_t scene, const float* pos, const float* vel);
   vxl_status read_state(uint32_t scene, float* pos, float* vel);
   // Deferred readback of every slot's position (reference order, scene after scene):
@@ -162,7 +168,7 @@ class Engine {
   void* bpos_ = nullptr;
   uint32_t* nbr_ = nullptr;
   uint32_t* nbr_n_ = nullptr;
-  uint32_t* halves_ = nullptr;
+  uint32_t* halves_ = nullptr;  // 4 words per 32 slots: upper-half masks along x, y, z
   float4* blocal_ = nullptr;         // body-frame lattice per boundary slot (reference order), lazily
   BodyPoseDev* poses_d_ = nullptr;   // poses of one scene's bodies (staged per call)
   uint32_t poses_cap_ = 0;
@@ -175,10 +181,23 @@ class Engine {
   bool rb_live_ = false;           // rb_d_ holds the bodies' current (evolved) states
   vxl_status rb_pull();
   void rb_layout();
+  // provider walls
+  std::vector<std::vector<vxl_sph_provider>> prov_h_;     // per scene (first_plane into wplanes_h_[q])
+  std::vector<std::vector<vxl_sph_wall_plane>> wplanes_h_;
+  ProviderDev* prov_d_ = nullptr;    // all scenes' providers, scene after scene
+  WallPlaneDev* wplanes_d_ = nullptr;
+  uint32_t prov_cap_ = 0, wplanes_cap_ = 0;
+  uint32_t* pflag_ = nullptr;   // per reference index: pushed this substep
+  void* pnsum_ = nullptr;       // float4 per reference index: normal sum, scene
+  uint32_t* plist_ = nullptr;   // pushed reference indices, ascending
+  uint32_t* pblk_ = nullptr;    // pushed count per chunk
+  std::vector<uint32_t> prov_first_st_, prov_count_st_;  // per scene, as staged on the device
+  bool walls_any_ = false;      // some scene has providers (selects the walls kernels)
+  vxl_status stage_walls();
   float* snap_h_ = nullptr;  // pinned, 3 floats per slot
   uint64_t snap_cap_ = 0, snap_n_ = 0;
   cudaEvent_t ev_snap_ = nullptr;
-  bool snap_pending_ = false;  // 4 words per 32 slots: upper-half masks along x, y, z
+  bool snap_pending_ = false;
   float* stage_ = nullptr;  // 8 floats per slot: staging for host transfers
   // cells (cell_cap_ + 1)
   uint32_t* counts_ = nullptr;

@@ -13,6 +13,7 @@ from __future__ import annotations
 
 import ctypes as C
 import os
+from dataclasses import dataclass
 from pathlib import Path
 
 import numpy as np
@@ -128,6 +129,64 @@ class RigidBody(C.Structure):
                 ("dynamic", C.c_uint32)]
 
 
+class WallPlane(C.Structure):
+    _fields_ = [("normal", C.c_float * 3), ("offset", C.c_float), ("axis", C.c_uint32), ("sign", C.c_float)]
+
+
+class Provider(C.Structure):
+    _fields_ = [("kind", C.c_uint32), ("first_plane", C.c_uint32), ("nplanes", C.c_uint32),
+                ("has_bounds", C.c_uint32), ("bounds_min", C.c_float * 3), ("bounds_max", C.c_float * 3)]
+
+
+PROVIDER_FACES, PROVIDER_CONVEX = 0, 1
+
+
+@dataclass
+class Faces:
+    """Independent axis-aligned half-space faces (axis, plane, sign): solid where
+    (p[axis] - plane) * sign < 0; bounds ((min xyz), (max xyz)) or None."""
+    faces: list
+    bounds: tuple | None = None
+
+
+@dataclass
+class Convex:
+    """Convex solid {x : n . x <= d for every (n, d) in planes}; bounds or None."""
+    planes: list
+    bounds: tuple | None = None
+
+
+def providers_arrays(providers):
+    """(Provider array, n, WallPlane array, nplanes) for a list of Faces / Convex."""
+    planes = []
+    recs = []
+    for pr in providers:
+        first = len(planes)
+        if isinstance(pr, Faces):
+            for axis, plane, sign in pr.faces:
+                planes.append(((0.0, 0.0, 0.0), plane, axis, sign))
+            kind = PROVIDER_FACES
+        else:
+            for n, d in pr.planes:
+                planes.append((tuple(n), d, 0, 1.0))
+            kind = PROVIDER_CONVEX
+        recs.append((kind, first, len(planes) - first, pr.bounds))
+    parr = (Provider * max(len(recs), 1))()
+    for q, (kind, first, cnt, b) in enumerate(recs):
+        parr[q].kind, parr[q].first_plane, parr[q].nplanes = kind, first, cnt
+        parr[q].has_bounds = 0 if b is None else 1
+        if b is not None:
+            for a in range(3):
+                parr[q].bounds_min[a] = b[0][a]
+                parr[q].bounds_max[a] = b[1][a]
+    warr = (WallPlane * max(len(planes), 1))()
+    for k, (n, d, axis, sign) in enumerate(planes):
+        for a in range(3):
+            warr[k].normal[a] = n[a]
+        warr[k].offset, warr[k].axis, warr[k].sign = d, axis, sign
+    return parr, len(recs), warr, len(planes)
+
+
 def poses_array(bodies):
     """BodyPose array from objects with id, pos, rot, linvel, angvel (e.g. scenes.Body)."""
     arr = (BodyPose * max(len(bodies), 1))()
@@ -193,6 +252,8 @@ SIGNATURES = {
     "vxl_sph_request_state": (C.c_int, [_H]),
     "vxl_sph_take_state": (C.c_int, [_H, _FP, C.c_uint64]),
     "vxl_sph_set_rigid_bodies": (C.c_int, [_H, C.c_uint32, C.POINTER(RigidBody), C.c_uint32]),
+    "vxl_sph_set_providers": (C.c_int, [_H, C.c_uint32, C.POINTER(Provider), C.c_uint32, C.POINTER(WallPlane),
+                                        C.c_uint32]),
     "vxl_sph_step_coupled": (C.c_int, [_H, C.c_float, C.c_uint32, _FP, C.c_float, C.c_float, C.POINTER(Reaction),
                                        C.c_uint32]),
     "vxl_sph_read_rigid_bodies": (C.c_int, [_H, C.c_uint32, C.POINTER(RigidBody), C.c_uint32]),
@@ -399,6 +460,11 @@ class Scene:
         """Rebuild the boundary segment on the device from the bodies' poses."""
         arr, n = poses_array(bodies)
         _check(self.lib.vxl_sph_set_body_poses(self._h, scene, arr, n))
+
+    def set_providers(self, providers, scene: int = 0) -> None:
+        """Provider walls (a list of Faces / Convex, in the fluid's boundaries order)."""
+        parr, n, warr, nw = providers_arrays(providers)
+        _check(self.lib.vxl_sph_set_providers(self._h, scene, parr, n, warr, nw))
 
     def set_spans(self, spans, scene: int = 0) -> None:
         """Spans for ticks that take none (vxl_sph_step_coupled)."""
@@ -646,6 +712,7 @@ class Batch:
     profile = Scene.profile
     request_state = Scene.request_state
     take_state = Scene.take_state
+    set_providers = Scene.set_providers
     set_body_lattice = Scene.set_body_lattice
     set_body_poses = Scene.set_body_poses
     set_spans = Scene.set_spans

@@ -140,6 +140,37 @@ def body_lattice(bodies, spacing: float, h: float, layers: int, cache=None):
     return np.concatenate(pts).astype(F), np.concatenate(idx)
 
 
+def floor_provider():
+    """The fluid crate's FloorY test provider: solid half-space y < 0, bounds (-50, -1, -50)
+    to (50, 0, 50) (crates/vxl-phys-fluid/src/tests.rs:9-44)."""
+    from . import Faces
+    return Faces([(1, 0.0, 1.0)], ((-50.0, -1.0, -50.0), (50.0, 0.0, 50.0)))
+
+
+def tank_provider(half_width: float = 0.2):
+    """The fluid crate's Tank test provider: floor y = 0 and four walls at x, z = +-0.2
+    (half-spaces extending outward), bounds +-50 (crates/vxl-phys-fluid/src/tests.rs:46-110)."""
+    from . import Faces
+    w = half_width
+    return Faces([(1, 0.0, 1.0), (0, -w, 1.0), (0, w, -1.0), (2, -w, 1.0), (2, w, -1.0)],
+                 ((-50.0, -50.0, -50.0), (50.0, 50.0, 50.0)))
+
+
+def box_obstacle(center, half):
+    """A solid box as a convex half-space set (outward normals +-x, +-y, +-z)."""
+    from . import Convex
+    c, h = center, half
+    planes = []
+    for a in range(3):
+        for sgn in (1.0, -1.0):
+            n = [0.0, 0.0, 0.0]
+            n[a] = sgn
+            planes.append((tuple(n), float(F(F(sgn) * F(c[a])) + F(h[a]))))
+    lo = tuple(float(F(c[a]) - F(h[a])) for a in range(3))
+    hi = tuple(float(F(c[a]) + F(h[a])) for a in range(3))
+    return Convex(planes, (lo, hi))
+
+
 def box_mass_props(half, density: float):
     """Mass properties of a box body (crates/vxl-phys-core/src/mass.rs:35-48), float32 in the
     reference's order: m = rho ex ey ez with e = 2 half, I = m / 12 (e1^2 + e2^2); returns

@@ -43,13 +43,14 @@ def test_struct_sizes_match_header(vxl, tmp_path):
         "sizeof(vxl_sph_params),sizeof(vxl_sph_desc),sizeof(vxl_sph_span),sizeof(vxl_sph_reaction),"
         "sizeof(vxl_sph_grid_info),sizeof(vxl_sph_stats),sizeof(vxl_block_header));"
         'printf("%zu %zu %zu %zu\\n",sizeof(vxl_sph_tuning),sizeof(vxl_sph_request_status),sizeof(vxl_sph_serve_report),sizeof(vxl_sph_body_pose));'
-        'printf("%zu\\n",sizeof(vxl_sph_rigid_body));'
+        'printf("%zu %zu %zu\\n",sizeof(vxl_sph_rigid_body),sizeof(vxl_sph_wall_plane),sizeof(vxl_sph_provider));'
         "return 0;}\n")
     exe = tmp_path / "sizes"
     subprocess.run(["gcc", "-std=c99", "-I", str(ROOT / "include"), str(src), "-o", str(exe)], check=True)
     got = [int(x) for x in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
     want = [C.sizeof(t) for t in (vxl.Params, vxl.Desc, vxl.Span, vxl.Reaction, vxl.GridInfo, vxl.Stats,
-                                  vxl.BlockHeader, vxl.Tuning, vxl.RequestStatus, vxl.ServeReport, vxl.BodyPose, vxl.RigidBody)]
+                                  vxl.BlockHeader, vxl.Tuning, vxl.RequestStatus, vxl.ServeReport, vxl.BodyPose, vxl.RigidBody, vxl.WallPlane,
+                                  vxl.Provider)]
     assert got == want
 
 
