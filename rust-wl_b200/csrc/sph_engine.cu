@@ -93,7 +93,7 @@ uint64_t Engine::bytes_per_slot(uint32_t nbr_cap) {
   return 4 * 16 + 4 + 4 + 8 + 8 + 8 + 4 + 16 + 16 + 16 + 16 + (uint64_t)nbr_cap * 4 + 4 + 32 + 1;
 }
 
-uint64_t Engine::bytes_per_cell() { return 8; }
+uint64_t Engine::bytes_per_cell() { return 12; }  // counts, start, wet
 
 template <class T>
 vxl_status Engine::dalloc(T** p, size_t count) {
@@ -167,6 +167,7 @@ vxl_status Engine::alloc_all() {
   A(dalloc(&halves_, 4 * (n / 32 + 2)));
   A(dalloc(&stage_, 8 * n));
   A(dalloc(&counts_, cell_cap_ + 1));
+  A(dalloc(&wet_, cell_cap_ + 1));
   A(dalloc(&start_, cell_cap_ + 1));
   A(dalloc(&partial_, cell_cap_ / kScanTile + 2));
   A(dalloc(&sc_d_, scene_cap_));
@@ -179,6 +180,7 @@ vxl_status Engine::alloc_all() {
   std::memset(sc_h_, 0, scene_cap_ * sizeof(SceneDev));
   std::memset(ctl_h_, 0, sizeof(EngineCtl));
   CU(cudaMemsetAsync(counts_, 0, (cell_cap_ + 1) * 4, stream_));
+  CU(cudaMemsetAsync(wet_, 0, (cell_cap_ + 1) * 4, stream_));
   CU(cudaMemsetAsync(start_, 0, (cell_cap_ + 1) * 4, stream_));
   CU(cudaMemsetAsync(ctl_d_, 0, sizeof(EngineCtl), stream_));
   CU(cudaMemsetAsync(sc_d_, 0, scene_cap_ * sizeof(SceneDev), stream_));
@@ -195,7 +197,7 @@ void Engine::free_all() {
   if (graph_) cudaGraphExecDestroy(graph_);
   graph_ = nullptr;
   void* d[] = {pos_[0], pos_[1], vel_[0], vel_[1], orig_, slot_of_, cellrank_, items_, rc_, press_, acc_, xsph_,
-               bforce_, bpos_, nbr_, nbr_n_, halves_, stage_, counts_, start_, partial_, sc_d_, tiles_d_, ctl_d_, spans_d_,
+               bforce_, bpos_, nbr_, nbr_n_, halves_, stage_, counts_, wet_, start_, partial_, sc_d_, tiles_d_, ctl_d_, spans_d_,
                chunks_d_, chunk_first_d_, react_partial_, breact_d_};
   for (void* p : d)
     if (p) cudaFree(p);
@@ -1181,7 +1183,7 @@ void Engine::enqueue_substep(bool with_reactions) {
   LAUNCH(KID_CELLOFF, k_e_celloff<<<1, 1024, 0, st>>>(sc_d_, S, ctl_d_, (uint32_t)cell_cap_));
   LAUNCH(KID_KEYS, k_e_keys<<<key_blocks, kThreads, 0, st>>>(p0, sc_d_, tiles_d_, ntiles_, ctl_d_, counts_,
                                                              (uint2*)cellrank_, halves_,
-                                                             (uint32_t)(4 * (used_ / 32 + 1))));
+                                                             (uint32_t)(4 * (used_ / 32 + 1)), wet_));
   LAUNCH(KID_SCAN_PARTIAL, k_e_scan_partial<<<148 * 4, kScanThreads, 0, st>>>(counts_, ctl_d_, partial_, start_));
   LAUNCH(KID_SCAN_FINAL, k_e_scan_final<<<148 * 4, kScanThreads, 0, st>>>(counts_, ctl_d_, partial_, start_));
   LAUNCH(KID_PLACE, k_e_place<<<key_blocks, kThreads, 0, st>>>((const uint2*)cellrank_, start_, orig_, tiles_d_,
@@ -1199,17 +1201,17 @@ void Engine::enqueue_substep(bool with_reactions) {
     if (tuning_.block == 128)
       LAUNCH(KID_DENSITY, k_e_density<128, true><<<gd, 128, 0, st>>>(
                               p1, start_, sc_d_, tiles_d_, ntiles_, ctl_d_, halves_, (float2*)rc_, press_, nbr_, nbr_n_,
-                              nbr_cap_, stride, prov_d_, wplanes_d_));
+                              nbr_cap_, stride, wet_, prov_d_, wplanes_d_));
     else
       LAUNCH(KID_DENSITY, k_e_density<256, true><<<gd, 256, 0, st>>>(
                               p1, start_, sc_d_, tiles_d_, ntiles_, ctl_d_, halves_, (float2*)rc_, press_, nbr_, nbr_n_,
-                              nbr_cap_, stride, prov_d_, wplanes_d_));
+                              nbr_cap_, stride, wet_, prov_d_, wplanes_d_));
   } else if (tuning_.block == 128) {
     LAUNCH(KID_DENSITY, k_e_density<128><<<gd, 128, 0, st>>>(p1, start_, sc_d_, tiles_d_, ntiles_, ctl_d_, halves_,
-                                                             (float2*)rc_, press_, nbr_, nbr_n_, nbr_cap_, stride));
+                                                             (float2*)rc_, press_, nbr_, nbr_n_, nbr_cap_, stride, wet_));
   } else {
     LAUNCH(KID_DENSITY, k_e_density<256><<<gd, 256, 0, st>>>(p1, start_, sc_d_, tiles_d_, ntiles_, ctl_d_, halves_,
-                                                             (float2*)rc_, press_, nbr_, nbr_n_, nbr_cap_, stride));
+                                                             (float2*)rc_, press_, nbr_, nbr_n_, nbr_cap_, stride, wet_));
   }
   // Reaction branch on the side stream: it reads only the sorted buffer, the densities and
   // the lists, so it runs beside the force pass (which writes the other buffer).

@@ -39,6 +39,11 @@
 #define VXL_FORCE_THREADS_PER_SM 1280
 #endif
 
+// 1: boundary particles with no fluid particle in their 27 cells skip the density walk.
+#ifndef VXL_DRY_SKIP
+#define VXL_DRY_SKIP 1
+#endif
+
 // 1: the half-culled walk takes cells with every half reachable as a plain range.
 #ifndef VXL_HALF_FULL_RANGE
 #define VXL_HALF_FULL_RANGE 0
@@ -114,6 +119,7 @@ struct EngineCtl {
   uint32_t err;
   uint32_t slow_gathers;
   uint32_t doubled;  // some scene's bins are at least 2h this substep (half-cell masks needed)
+  uint32_t epoch;    // substep counter: wet[c] == epoch marks cells holding fluid this substep
   uint32_t work[kWorkSlots];
 };
 
@@ -396,6 +402,7 @@ __global__ void k_e_celloff(SceneDev* __restrict__ sc, uint32_t nscenes, EngineC
     doubled = 0;
   }
   if (threadIdx.x < kWorkSlots) ctl->work[threadIdx.x] = 0;  // persistent-pass counters of this substep
+  if (threadIdx.x == 0) ctl->epoch = ctl->epoch + 1u;
   __syncthreads();
   for (uint32_t b0 = 0; b0 < nscenes; b0 += 1024) {
     const uint32_t q = b0 + threadIdx.x;
@@ -448,12 +455,13 @@ __global__ void k_e_celloff(SceneDev* __restrict__ sc, uint32_t nscenes, EngineC
 
 // Cell key + arrival rank per slot (tiles, one block per tile in turn). Lanes with equal
 // keys share one atomic (warp-aggregated); the rank is only a placement ticket — canon
-// makes the final order deterministic.
+// makes the final order deterministic. Cells holding a fluid particle get wet[c] = epoch.
 __global__ void k_e_keys(const float4* __restrict__ pos, const SceneDev* __restrict__ sc,
                          const TileDev* __restrict__ tiles, uint32_t ntiles, const EngineCtl* __restrict__ ctl,
                          uint32_t* __restrict__ counts, uint2* __restrict__ cellrank, uint32_t* __restrict__ halves,
-                         uint32_t half_words) {
+                         uint32_t half_words, uint32_t* __restrict__ wet) {
   if (ctl->err & kErrCellCap) return;
+  const uint32_t epoch = ctl->epoch;
   if (ctl->doubled)  // clear the half-cell masks that k_e_halfmask fills after the sort
     for (uint32_t w = blockIdx.x * blockDim.x + threadIdx.x; w < half_words; w += gridDim.x * blockDim.x)
       halves[w] = 0u;
@@ -468,6 +476,7 @@ __global__ void k_e_keys(const float4* __restrict__ pos, const SceneDev* __restr
       if (valid) {
         const float4 p = pos[td.first + i];
         c = off + cell_index(g, p.x, p.y, p.z);
+        if (VXL_DRY_SKIP && p.w > 0.0f) wet[c] = epoch;
       }
       const uint32_t active = __ballot_sync(0xffffffffu, valid);
       if (valid) {
@@ -993,8 +1002,8 @@ __global__ void __launch_bounds__(kBlock, VXL_DENSITY_THREADS_PER_SM / kBlock) k
     const float4* __restrict__ pos, const uint32_t* __restrict__ start, const SceneDev* __restrict__ sc,
     const TileDev* __restrict__ tiles, uint32_t ntiles, EngineCtl* ctl, const uint32_t* __restrict__ halves,
     float2* __restrict__ rc, float* __restrict__ press_out, uint32_t* __restrict__ nbr,
-    uint32_t* __restrict__ nbr_n, uint32_t cap, uint32_t stride, const ProviderDev* __restrict__ prov = nullptr,
-    const WallPlaneDev* __restrict__ wplanes = nullptr) {
+    uint32_t* __restrict__ nbr_n, uint32_t cap, uint32_t stride, const uint32_t* __restrict__ wet,
+    const ProviderDev* __restrict__ prov = nullptr, const WallPlaneDev* __restrict__ wplanes = nullptr) {
   if (ctl->err & kErrCellCap) return;
   for (uint32_t t = first_tile(&ctl->work[kWorkDensity], ntiles); t < ntiles; t = following_tile(&ctl->work[kWorkDensity], ntiles)) {
     const TileDev td = tiles[t];
@@ -1004,6 +1013,7 @@ __global__ void __launch_bounds__(kBlock, VXL_DENSITY_THREADS_PER_SM / kBlock) k
     const uint32_t* cst = start + S.cell_off;
     const float h = k.h, h2 = k.h2, k6 = k.k6, w0 = k.w0, mass = k.mass;
     const bool half_walk = halves != nullptr && g.bin >= 2.0f * h;  // uniform over the tile
+    const uint32_t epoch = ctl->epoch;
     for (uint32_t i = threadIdx.x; i < td.count; i += kBlock) {
       const uint32_t s = td.first + i;
       const float4 pi = pos[s];
@@ -1075,12 +1085,34 @@ __global__ void __launch_bounds__(kBlock, VXL_DENSITY_THREADS_PER_SM / kBlock) k
           }
         }
       };
-      if (half_walk)
+      // A boundary particle sums fluid neighbours only: with no fluid particle in its 27
+      // cells (none marked wet this substep) its walk would accept nothing.
+      bool dry = false;
+      if (VXL_DRY_SKIP && !fluid_i) {
+        const uint32_t* wc = wet + S.cell_off;
+        dry = true;
+        for (int dz = -1; dz <= 1; ++dz) {
+          const int z = (int)cz + dz;
+          if (z < 0 || z >= (int)g.nz) continue;
+          for (int dy = -1; dy <= 1; ++dy) {
+            const int y = (int)cy + dy;
+            if (y < 0 || y >= (int)g.ny) continue;
+            for (int dx = -1; dx <= 1; ++dx) {
+              const int x = (int)cx + dx;
+              if (x < 0 || x >= (int)g.nx) continue;
+              if (wc[((uint32_t)x * g.ny + (uint32_t)y) * g.nz + (uint32_t)z] == epoch) dry = false;
+            }
+          }
+        }
+      }
+      if (dry) {
+      } else if (half_walk) {
         walk27_half(g, cst, halves, pi.x, pi.y, pi.z, cx, cy, cz, h, [&](uint32_t j) {
           if (j != s) visit(j);
         });
-      else
+      } else {
         walk27<true>(g, cst, pi.x, pi.y, pi.z, cx, cy, cz, h, visit, s);
+      }
       nbr_n[s] = cnt;
       const float rho = fluid_i ? (mass * sum + sum_b) : ((-pi.w) * w0 + sum);
       const float p = tait(k, rho);

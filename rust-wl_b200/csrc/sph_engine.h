@@ -201,6 +201,7 @@ class Engine {
   float* stage_ = nullptr;  // 8 floats per slot: staging for host transfers
   // cells (cell_cap_ + 1)
   uint32_t* counts_ = nullptr;
+  uint32_t* wet_ = nullptr;  // per cell: the substep epoch of the last substep it held fluid
   uint32_t* start_ = nullptr;
   uint32_t* partial_ = nullptr;
   // scenes / tiles / control
