@@ -44,10 +44,6 @@
 #define VXL_DRY_SKIP 1
 #endif
 
-// 1: the half-culled walk takes cells with every half reachable as a plain range.
-#ifndef VXL_HALF_FULL_RANGE
-#define VXL_HALF_FULL_RANGE 0
-#endif
 
 namespace vxl {
 
@@ -157,6 +153,7 @@ constexpr int kScanThreads = 256;
 constexpr int kCanonSmem = 1024;
 constexpr int kCanonWindow = kCanonSmem / 2;  // window path: keys + segment table in one warp's buffer
 constexpr int kBGatherCap = 64;
+constexpr uint32_t kListPrefetch = 4;  // force pass: list entries fetched into L2 this far ahead
 
 // Block-level ordered-uint min/max of (x, y, z), one atomic per component into acc.
 __device__ __forceinline__ void block_bbox_accumulate(uint32_t* acc, float x, float y, float z, bool valid) {
@@ -909,12 +906,6 @@ __device__ __forceinline__ void walk27_half(const GridBox& g, const uint32_t* __
         if (!xsel || !ysel || !zsel) continue;
         const uint32_t idx = ((uint32_t)x * g.ny + (uint32_t)y) * g.nz + (uint32_t)z;
         const uint32_t j0 = start[idx], j1 = start[idx + 1];
-#if VXL_HALF_FULL_RANGE
-        if ((xsel & ysel & zsel) == 3u) {
-          for (uint32_t j = j0; j < j1; ++j) f(j);
-          continue;
-        }
-#endif
         for (uint32_t base = j0 & ~31u; base < j1; base += 32) {
           const uint4 hm = *reinterpret_cast<const uint4*>(halves + 4 * (base >> 5));
           uint32_t m = half_select(xsel, hm.x) & half_select(ysel, hm.y) & half_select(zsel, hm.z);
@@ -1078,7 +1069,7 @@ __global__ void __launch_bounds__(kBlock, VXL_DENSITY_THREADS_PER_SM / kBlock) k
           }
           if (rec) {
             if (cnt < cap) {
-              *wp = j;
+              __stcs(wp, j);  // streaming store: the list is read once, by the force pass
               wp += stride;
             }
             ++cnt;
@@ -1176,13 +1167,16 @@ __global__ void __launch_bounds__(kBlock, VXL_FORCE_THREADS_PER_SM / kBlock) k_e
             az = az + dz * q;
             const float vx = vi.x - vj.x, vy = vi.y - vj.y, vz = vi.z - vj.z;
             const float vdn = -(vx * dx + vy * dy + vz * dz);
-            if (vdn > 0.0f) {
+            {
+              // artificial viscosity only when approaching (vdn > 0): computed for every pair and
+              // selected, so the warp does not diverge around it (the sums are the same)
               const float mu = vdn * h / (r2 + h001);
               const float c = mj * (alpha_c * mu / (0.5f * (rho_i + rho_j))) * (ks * tt * tt);
               const float q2 = c / denom;
-              ax = ax + dx * q2;
-              ay = ay + dy * q2;
-              az = az + dz * q2;
+              const bool take = vdn > 0.0f;
+              ax = take ? ax + dx * q2 : ax;
+              ay = take ? ay + dy * q2 : ay;
+              az = take ? az + dz * q2 : az;
             }
             const float t2 = h2 - r2;
             const float w = k6 * t2 * t2 * t2;
@@ -1194,12 +1188,15 @@ __global__ void __launch_bounds__(kBlock, VXL_FORCE_THREADS_PER_SM / kBlock) k_e
           const uint32_t cnt = nbr_n[s];
           if (cnt <= cap) {
             // the next list entry is loaded one neighbour ahead, so each iteration waits on
-            // one dependent gather (pos/vel/rc of j) instead of two (measured: 6-8% faster)
+            // one dependent gather (pos/vel/rc of j) instead of two (measured: 6-8% faster),
+            // and the one kListPrefetch ahead is fetched into L2 (the list is not L2-resident)
             const uint32_t* np = nbr + s;
             uint32_t jn = cnt ? *np : 0u;
             for (uint32_t q = 0; q < cnt; ++q) {
               const uint32_t j = jn;
               np += stride;
+              if (q + kListPrefetch < cnt)  // the entry kListPrefetch ahead into L2
+                asm volatile("prefetch.global.L2 [%0];" ::"l"(np + (size_t)(kListPrefetch - 1) * stride));
               if (q + 1 < cnt) jn = *np;
               const float4 pj = pos[j];
               const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
