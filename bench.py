@@ -700,7 +700,11 @@ def run_ncu_case(args) -> None:
         print(json.dumps({"ncu_case": "batched", "scenes": args.scenes, "ticks": max(args.warmup, 1),
                           "n_fluid": sum(s.n_fluid for s in specs), "n_boundary": sum(s.n_boundary for s in specs)}))
         return
-    spec = build_scene(args.workload)
+    if args.workload == "dam10m" and args.ncu_block:
+        from vxl_sph import scenes
+        spec = scenes.dam10m_block(args.ncu_block)
+    else:
+        spec = build_scene(args.workload)
     scene = vxl_sph.Scene(spec.params, spec.pos, spec.vel, spec.pmass, spec.n_fluid)
     for _ in range(max(args.warmup, 1)):
         scene.step_tick(dt_tick, spec.spans)
@@ -725,6 +729,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-threads", type=int, default=0, help="reference arm: host threads (default: all)")
     ap.add_argument("--ncu-case", action="store_true", help="build + warm-up ticks only (for ncu captures)")
+    ap.add_argument("--ncu-block", type=int, default=0,
+                    help="ncu case of dam10m: an N^3 fluid block in the same tank (bins still doubled)")
     args = ap.parse_args()
     if args.ncu_case:
         run_ncu_case(args)

@@ -273,6 +273,14 @@ def dam10m(seed: int = 2, boxes: int = 64) -> SceneSpec:
     return dam_break("dam10m", (215, 215, 215), 0.005, (2.5, 1.2, 1.2), 120, seed, extra_bodies=extra)
 
 
+def dam10m_block(n: int = 100, seed: int = 2, boxes: int = 64) -> SceneSpec:
+    """The dam10m tank, walls and boxes with an n^3 fluid block instead of 215^3: the grid
+    box is still the tank's, so the bins are still doubled to 2h (64 particles per cell in the
+    block), at a size a profiler can capture."""
+    extra = floating_boxes(boxes, seed + 1000, (1.2, 0.05, 0.05), (2.45, 1.1, 1.15), 0.025, 0.075, 5, 0.02)
+    return dam_break(f"dam10m_block{n}", (n, n, n), 0.005, (2.5, 1.2, 1.2), 120, seed, extra_bodies=extra)
+
+
 def small_dam(n=(8, 8, 8), spacing: float = 0.05, tank=(0.8, 0.6, 0.6), seed: int = 3, substeps: int = 4,
               ticks: int = 10, **over) -> SceneSpec:
     """A small tank scene for parity tests (same construction, smaller sizes)."""
