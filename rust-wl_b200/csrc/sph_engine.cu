@@ -89,8 +89,8 @@ namespace vxl {
 
 uint64_t Engine::bytes_per_slot(uint32_t nbr_cap) {
   // pos, vel (x2), orig, slot_of, cellrank, items, rc, press, acc, xsph, bforce, bpos,
-  // neighbour list + count, staging
-  return 4 * 16 + 4 + 4 + 8 + 8 + 8 + 4 + 16 + 16 + 16 + 16 + (uint64_t)nbr_cap * 4 + 4 + 32 + 1;
+  // neighbour list + count, staging, density thread order at doubled bins
+  return 4 * 16 + 4 + 4 + 8 + 8 + 8 + 4 + 16 + 16 + 16 + 16 + (uint64_t)nbr_cap * 4 + 4 + 32 + 1 + 4;
 }
 
 uint64_t Engine::bytes_per_cell() { return 12; }  // counts, start, wet
@@ -168,6 +168,7 @@ vxl_status Engine::alloc_all() {
   A(dalloc(&stage_, 8 * n));
   A(dalloc(&counts_, cell_cap_ + 1));
   A(dalloc(&wet_, cell_cap_ + 1));
+  A(dalloc(&xorder_, slot_cap_));
   A(dalloc(&start_, cell_cap_ + 1));
   A(dalloc(&partial_, cell_cap_ / kScanTile + 2));
   A(dalloc(&sc_d_, scene_cap_));
@@ -197,7 +198,7 @@ void Engine::free_all() {
   if (graph_) cudaGraphExecDestroy(graph_);
   graph_ = nullptr;
   void* d[] = {pos_[0], pos_[1], vel_[0], vel_[1], orig_, slot_of_, cellrank_, items_, rc_, press_, acc_, xsph_,
-               bforce_, bpos_, nbr_, nbr_n_, halves_, stage_, counts_, wet_, start_, partial_, sc_d_, tiles_d_, ctl_d_, spans_d_,
+               bforce_, bpos_, nbr_, nbr_n_, halves_, xorder_, stage_, counts_, wet_, start_, partial_, sc_d_, tiles_d_, ctl_d_, spans_d_,
                chunks_d_, chunk_first_d_, react_partial_, breact_d_};
   for (void* p : d)
     if (p) cudaFree(p);
@@ -1191,6 +1192,7 @@ void Engine::enqueue_substep(bool with_reactions) {
   LAUNCH(KID_CANON, k_e_canon<<<148 * 8, 256, 0, st>>>((const uint2*)items_, start_, ctl_d_, p0, v0, (float4*)pos_[1],
                                                        (float4*)vel_[1], orig_, slot_of_));
   LAUNCH(KID_HALFMASK, k_e_halfmask<<<key_blocks, kThreads, 0, st>>>(p1, sc_d_, tiles_d_, ntiles_, ctl_d_, halves_));
+  LAUNCH(KID_HALFMASK, k_e_xorder<<<148 * 8, kThreads, 0, st>>>(start_, ctl_d_, halves_, xorder_));
   const uint32_t stride = (uint32_t)slot_cap_;
   const bool rec = record_;
   const uint32_t per_tile = std::max<uint32_t>(ntiles_, 1);
@@ -1201,17 +1203,19 @@ void Engine::enqueue_substep(bool with_reactions) {
     if (tuning_.block == 128)
       LAUNCH(KID_DENSITY, k_e_density<128, true><<<gd, 128, 0, st>>>(
                               p1, start_, sc_d_, tiles_d_, ntiles_, ctl_d_, halves_, (float2*)rc_, press_, nbr_, nbr_n_,
-                              nbr_cap_, stride, wet_, prov_d_, wplanes_d_));
+                              nbr_cap_, stride, wet_, xorder_, prov_d_, wplanes_d_));
     else
       LAUNCH(KID_DENSITY, k_e_density<256, true><<<gd, 256, 0, st>>>(
                               p1, start_, sc_d_, tiles_d_, ntiles_, ctl_d_, halves_, (float2*)rc_, press_, nbr_, nbr_n_,
-                              nbr_cap_, stride, wet_, prov_d_, wplanes_d_));
+                              nbr_cap_, stride, wet_, xorder_, prov_d_, wplanes_d_));
   } else if (tuning_.block == 128) {
     LAUNCH(KID_DENSITY, k_e_density<128><<<gd, 128, 0, st>>>(p1, start_, sc_d_, tiles_d_, ntiles_, ctl_d_, halves_,
-                                                             (float2*)rc_, press_, nbr_, nbr_n_, nbr_cap_, stride, wet_));
+                                                             (float2*)rc_, press_, nbr_, nbr_n_, nbr_cap_, stride, wet_,
+                                                             xorder_));
   } else {
     LAUNCH(KID_DENSITY, k_e_density<256><<<gd, 256, 0, st>>>(p1, start_, sc_d_, tiles_d_, ntiles_, ctl_d_, halves_,
-                                                             (float2*)rc_, press_, nbr_, nbr_n_, nbr_cap_, stride, wet_));
+                                                             (float2*)rc_, press_, nbr_, nbr_n_, nbr_cap_, stride, wet_,
+                                                             xorder_));
   }
   // Reaction branch on the side stream: it reads only the sorted buffer, the densities and
   // the lists, so it runs beside the force pass (which writes the other buffer).

@@ -842,6 +842,43 @@ __global__ void k_e_halfmask(const float4* __restrict__ pos, const SceneDev* __r
   }
 }
 
+// Thread order of the half-culled density walk: within each cell, the slots in the lower x
+// half first, then those in the upper half (each group in slot order), from the half-cell
+// masks. At 2h bins a particle's reachable halves follow from the halves it lies in, so a
+// warp whose lanes share their x half skips the x-side cells its lanes cannot reach together
+// (every lane in the lower half leaves the +x cells out) instead of idling through them.
+// order[p] is the slot the density pass processes at position p; it permutes each cell's own
+// slots, so every slot is processed once and each result is unchanged. One warp per cell.
+__global__ void k_e_xorder(const uint32_t* __restrict__ start, const EngineCtl* __restrict__ ctl,
+                           const uint32_t* __restrict__ halves, uint32_t* __restrict__ order) {
+  if ((ctl->err & kErrCellCap) || !ctl->doubled) return;
+  const uint32_t total = ctl->cells;
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t lt = (1u << lane) - 1u;
+  const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; c < total; c += nw) {
+    const uint32_t b = start[c], n = start[c + 1] - b;
+    uint32_t nlow = 0;
+    for (uint32_t k0 = 0; k0 < n; k0 += 32) {
+      const uint32_t sl = b + k0 + lane;
+      const bool valid = k0 + lane < n;
+      const bool up = valid && ((halves[4 * (sl >> 5)] >> (sl & 31)) & 1u);
+      nlow += __popc(__ballot_sync(0xffffffffu, valid && !up));
+    }
+    uint32_t lo = 0, hi = 0;
+    for (uint32_t k0 = 0; k0 < n; k0 += 32) {
+      const uint32_t sl = b + k0 + lane;
+      const bool valid = k0 + lane < n;
+      const bool up = valid && ((halves[4 * (sl >> 5)] >> (sl & 31)) & 1u);
+      const uint32_t ml = __ballot_sync(0xffffffffu, valid && !up);
+      const uint32_t mh = __ballot_sync(0xffffffffu, up);
+      if (valid) order[b + (up ? nlow + hi + __popc(mh & lt) : lo + __popc(ml & lt))] = sl;
+      lo += __popc(ml);
+      hi += __popc(mh);
+    }
+  }
+}
+
 // Per axis, which halves of the three cells (d = -1, 0, +1) along it a particle at p can
 // reach: bit 2 (d + 1) for the lower half, bit 2 (d + 1) + 1 for the upper half. A half is
 // dropped only when the gap from p to its nominal interval exceeds `reach` (h plus a
@@ -994,7 +1031,8 @@ __global__ void __launch_bounds__(kBlock, VXL_DENSITY_THREADS_PER_SM / kBlock) k
     const TileDev* __restrict__ tiles, uint32_t ntiles, EngineCtl* ctl, const uint32_t* __restrict__ halves,
     float2* __restrict__ rc, float* __restrict__ press_out, uint32_t* __restrict__ nbr,
     uint32_t* __restrict__ nbr_n, uint32_t cap, uint32_t stride, const uint32_t* __restrict__ wet,
-    const ProviderDev* __restrict__ prov = nullptr, const WallPlaneDev* __restrict__ wplanes = nullptr) {
+    const uint32_t* __restrict__ xorder, const ProviderDev* __restrict__ prov = nullptr,
+    const WallPlaneDev* __restrict__ wplanes = nullptr) {
   if (ctl->err & kErrCellCap) return;
   for (uint32_t t = first_tile(&ctl->work[kWorkDensity], ntiles); t < ntiles; t = following_tile(&ctl->work[kWorkDensity], ntiles)) {
     const TileDev td = tiles[t];
@@ -1006,7 +1044,7 @@ __global__ void __launch_bounds__(kBlock, VXL_DENSITY_THREADS_PER_SM / kBlock) k
     const bool half_walk = halves != nullptr && g.bin >= 2.0f * h;  // uniform over the tile
     const uint32_t epoch = ctl->epoch;
     for (uint32_t i = threadIdx.x; i < td.count; i += kBlock) {
-      const uint32_t s = td.first + i;
+      const uint32_t s = half_walk ? xorder[td.first + i] : td.first + i;
       const float4 pi = pos[s];
       const bool fluid_i = pi.w > 0.0f;
       uint32_t cx, cy, cz;

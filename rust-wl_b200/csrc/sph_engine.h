@@ -169,6 +169,7 @@ class Engine {
   uint32_t* nbr_ = nullptr;
   uint32_t* nbr_n_ = nullptr;
   uint32_t* halves_ = nullptr;  // 4 words per 32 slots: upper-half masks along x, y, z
+  uint32_t* xorder_ = nullptr;  // density thread order at doubled bins (lower x halves first)
   float4* blocal_ = nullptr;         // body-frame lattice per boundary slot (reference order), lazily
   BodyPoseDev* poses_d_ = nullptr;   // poses of one scene's bodies (staged per call)
   uint32_t poses_cap_ = 0;
