@@ -144,3 +144,38 @@ def test_set_providers_rejects_bad_input(vxl):
     g.set_providers([scenes.floor_provider()])  # still usable
     g.step_tick(float(F32(1.0) / F32(60.0)))
     g.close()
+
+
+def test_coupled_loop_with_provider_floor(vxl, oracle_mod):
+    """The device coupling loop (floating boxes) on a handle that also has a provider floor:
+    bodies and fluid stay bitwise equal to the oracle loop with the same provider."""
+    from test_gpu_parity import GRAVITY, _couple, _floating_scene
+    from vxl_sph import scenes
+    spec, bodies, dynamic, local, idx = _floating_scene()
+    floor = [vxl.Faces([(1, 0.01, 1.0)], ((-50.0, -1.0, -50.0), (50.0, 0.01, 50.0)))]
+    g = vxl.Scene(spec.params, spec.pos, spec.vel, spec.pmass, spec.n_fluid)
+    o = oracle_mod.OracleSystem.from_scene(spec, threads=4)
+    g.set_providers(floor)
+    o.set_providers(floor)
+    st = _couple(g, spec, bodies, dynamic, local, idx)
+    dt = float(F32(1.0) / F32(60.0))
+    react = np.zeros((len(bodies), 6), F32)
+    row = {b.id: q for q, b in enumerate(bodies)}
+    for t in range(4):
+        oracle_mod.rigid_step(st, react, GRAVITY, float(F32(dt) / F32(2)), 2, 100.0, 50.0)
+        posed = [scenes.Body(b.id, b.half, tuple(float(x) for x in st[q, 0:3]), rot=tuple(float(x) for x in st[q, 3:7]),
+                             linvel=tuple(float(x) for x in st[q, 7:10]), angvel=tuple(float(x) for x in st[q, 10:13]))
+                 for q, b in enumerate(bodies)]
+        o.set_bodies(posed)
+        o.step(dt)
+        g.step_coupled(dt, 2, GRAVITY, 100.0, 50.0, 0)
+        assert_bits(g.read_rigid_bodies(), st[:, :13], f"tick {t} bodies")
+        for bid, fo, to in o.reactions():
+            react[row[bid], 0:3] = fo
+            react[row[bid], 3:6] = to
+        p, v = g.read_state()
+        r = o.read_f32()
+        assert_bits(p, r["pos"], f"tick {t} pos")
+        assert_bits(v, r["vel"], f"tick {t} vel")
+    o.close()
+    g.close()

@@ -225,3 +225,20 @@ def test_vxld_round_trip(tmp_path):
         assert fr["systems"][0].tobytes() == p.tobytes()
     # header size: magic + 4 words + voxel block (28 B) + 3 counts
     assert path.stat().st_size == 4 + 16 + 28 + 12 + 3 * (12 + 1 + 4 + 17 * 12)
+
+
+def test_provider_arrays_packing(vxl):
+    """Faces and Convex providers pack into the C ABI's provider and plane arrays in order,
+    each provider's planes as one run of the plane array."""
+    from vxl_sph import scenes
+    prs = [scenes.tank_provider(0.3), scenes.box_obstacle((0.0, 0.1, 0.0), (0.05, 0.1, 0.05)), vxl.Faces([(2, 1.5, -1.0)])]
+    parr, n, warr, nw = vxl.providers_arrays(prs)
+    assert n == 3 and nw == 5 + 6 + 1
+    assert [(parr[q].kind, parr[q].first_plane, parr[q].nplanes, parr[q].has_bounds) for q in range(n)] == \
+        [(vxl.PROVIDER_FACES, 0, 5, 1), (vxl.PROVIDER_CONVEX, 5, 6, 1), (vxl.PROVIDER_FACES, 11, 1, 0)]
+    assert (warr[1].axis, np.float32(warr[1].offset), warr[1].sign) == (0, np.float32(-0.3), 1.0)
+    assert (warr[2].axis, np.float32(warr[2].offset), warr[2].sign) == (0, np.float32(0.3), -1.0)
+    # box obstacle: +x face at c + h, -x face at -(c - h)
+    assert list(warr[5].normal) == [1.0, 0.0, 0.0] and np.isclose(warr[5].offset, 0.05)
+    assert list(warr[6].normal) == [-1.0, 0.0, 0.0] and np.isclose(warr[6].offset, 0.05)
+    assert (warr[11].axis, warr[11].offset, warr[11].sign) == (2, 1.5, -1.0)
