@@ -39,11 +39,6 @@
 #define VXL_FORCE_THREADS_PER_SM 1280
 #endif
 
-// 1: boundary particles with no fluid particle in their 27 cells skip the density walk.
-#ifndef VXL_DRY_SKIP
-#define VXL_DRY_SKIP 1
-#endif
-
 
 namespace vxl {
 
@@ -473,7 +468,7 @@ __global__ void k_e_keys(const float4* __restrict__ pos, const SceneDev* __restr
       if (valid) {
         const float4 p = pos[td.first + i];
         c = off + cell_index(g, p.x, p.y, p.z);
-        if (VXL_DRY_SKIP && p.w > 0.0f) wet[c] = epoch;
+        if (p.w > 0.0f) wet[c] = epoch;
       }
       const uint32_t active = __ballot_sync(0xffffffffu, valid);
       if (valid) {
@@ -1117,7 +1112,7 @@ __global__ void __launch_bounds__(kBlock, VXL_DENSITY_THREADS_PER_SM / kBlock) k
       // A boundary particle sums fluid neighbours only: with no fluid particle in its 27
       // cells (none marked wet this substep) its walk would accept nothing.
       bool dry = false;
-      if (VXL_DRY_SKIP && !fluid_i) {
+      if (!fluid_i) {
         const uint32_t* wc = wet + S.cell_off;
         dry = true;
         for (int dz = -1; dz <= 1; ++dz) {
