@@ -179,3 +179,41 @@ def test_coupled_loop_with_provider_floor(vxl, oracle_mod):
         assert_bits(v, r["vel"], f"tick {t} vel")
     o.close()
     g.close()
+
+
+def test_provider_walls_at_doubled_bins(vxl, oracle_mod):
+    """Provider walls with a cell budget that doubles the bins (the half-culled density walk
+    with mirror ghosts, and the x-half thread order): bitwise with the oracle."""
+    from vxl_sph import scenes
+    pos = scenes.jitter(scenes.fluid_block((-0.3, 0.05, -0.2), (12, 10, 8), 0.05), 0.05, 5)
+    spec = _custom(vxl, pos, h=0.1, spacing=0.05, max_bins=64, xsph_viscosity=0.05)
+    walls = [scenes.floor_provider(), scenes.box_obstacle((0.0, 0.08, 0.0), (0.08, 0.08, 0.08))]
+    g, o = _run(vxl, oracle_mod, spec, walls, ticks=12, check_every=3)
+    _, _, _, info = g.export_grid()
+    assert info.bin >= 0.2 * 0.999, info.bin  # bins of at least 2h
+    o.close()
+    g.close()
+
+
+def test_batch_mixing_doubled_and_h_bins(vxl):
+    """One batch holding a scene whose bins doubled and one at h-sized bins equals each
+    scene stepped alone, bitwise."""
+    from vxl_sph import scenes
+    pos = scenes.jitter(scenes.fluid_block((0.0, 0.0, 0.0), (12, 10, 8), 0.05), 0.05, 11)
+    a = _custom(vxl, pos, h=0.1, spacing=0.05, max_bins=64)
+    b = scenes.small_dam(n=(8, 9, 8), spacing=0.05, tank=(0.8, 0.7, 0.6), seed=3)
+    bat = vxl.Batch([a, b])
+    alone = [vxl.Scene(x.params, x.pos, x.vel, x.pmass, x.n_fluid) for x in (a, b)]
+    dt = float(F32(1.0) / F32(60.0))
+    for t in range(5):
+        bat.step_tick(dt)
+        alone[0].step_tick(dt)
+        alone[1].step_tick(dt, b.spans)
+        for q in range(2):
+            p1, v1 = bat.read_state(q)
+            p2, v2 = alone[q].read_state()
+            assert_bits(p1, p2, f"tick {t} scene {q} pos")
+            assert_bits(v1, v2, f"tick {t} scene {q} vel")
+    assert bat.export_grid(0)[3].bin > 0.1 and bat.export_grid(1)[3].bin <= 0.1 + 1e-6
+    for x in [bat] + alone:
+        x.close()
