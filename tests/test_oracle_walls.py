@@ -75,3 +75,54 @@ def test_walls_change_the_density_only_near_them(oracle_mod):
     assert da[~bottom].tobytes() == db[~bottom].tobytes()
     a.close()
     b.close()
+
+
+def test_projection_and_separation_against_a_direct_restatement(oracle_mod):
+    """Two isolated particles 1e-4 apart inside FloorY, one substep: no pressure (the Tait
+    pressure clamps at 0), no viscosity or XSPH (equal velocities), so each integrates
+    gravity, is projected out of the floor (boundary_pass, fluid_boundary.rs:45-101) and the
+    later one is separated from the earlier (separate_coincident, :103-128). The oracle's
+    result equals this float32 restatement of those three steps bit for bit."""
+    from vxl_sph import scenes
+    f = F32
+    c = oracle_mod.default_cfg()
+    o = oracle_mod.OracleSystem(c, origin=(0.0, 0.0, 0.0), dims=(2, 1, 1), spacing=0.05)
+    p0 = np.array([[0.0, -0.001, 0.0], [0.0001, -0.001, 0.0]], F32)
+    o.set_state(p0, np.zeros_like(p0))
+    o.set_providers([scenes.floor_provider()])
+    dt = f(f(f(1.0) / f(60.0)) / f(4.0))
+    o.substep(float(dt))
+    got = o.read_f32()
+    h, eps, g = f(0.1), f(c.xsph_viscosity), f(-9.81)
+    skin = f(0.15) * h
+    vmax = f(0.4) * h / dt
+    pos, vel = [], []
+    for p in p0:
+        # v = vel + acc dt + xsph eps with acc = gravity, vel = xsph = 0 (fluid_step.rs:112-123)
+        v = np.array([f(f(0.0) + f(0.0) * dt) + f(0.0) * eps, f(f(0.0) + g * dt) + f(0.0) * eps,
+                      f(f(0.0) + f(0.0) * dt) + f(0.0) * eps], F32)
+        assert f(f(v[0] * v[0] + v[1] * v[1]) + v[2] * v[2]) <= vmax * vmax
+        q = np.array([p[a] + v[a] * dt for a in range(3)], F32)
+        # FloorY contact at (x, 0, z), normal +y; sdf = (q - point) . n
+        sdf = f(f(f(q[0] - q[0]) * f(0.0) + f(q[1] - f(0.0)) * f(1.0)) + f(q[2] - q[2]) * f(0.0))
+        pen = -sdf
+        assert pen > 0
+        m = min(f(pen + skin), h)
+        q = np.array([q[0] + f(0.0) * m, q[1] + f(1.0) * m, q[2] + f(0.0) * m], F32)
+        vn = f(f(v[0] * f(0.0) + v[1] * f(1.0)) + v[2] * f(0.0))
+        if vn < 0:
+            v = np.array([v[0] - f(0.0) * vn, v[1] - f(1.0) * vn, v[2] - f(0.0) * vn], F32)
+        pos.append(q)
+        vel.append(v)
+    # the later particle moves along its normal sum (0, 1, 0) until r_min from the earlier one
+    r_min = f(0.2) * h
+    inv = f(1.0) / np.sqrt(f(f(f(0.0) + f(1.0)) + f(0.0)), dtype=F32)
+    d = np.array([pos[1][a] - pos[0][a] for a in range(3)], F32)
+    r2 = f(f(d[0] * d[0] + d[1] * d[1]) + d[2] * d[2])
+    assert r2 < r_min * r_min
+    r = np.sqrt(r2, dtype=F32)
+    step = f(r_min - r)
+    pos[1] = np.array([pos[1][a] + f(n * inv) * step for a, n in enumerate((f(0.0), f(1.0), f(0.0)))], F32)
+    assert got["pos"].astype(F32).tobytes() == np.array(pos, F32).tobytes(), (got["pos"], pos)
+    assert got["vel"].astype(F32).tobytes() == np.array(vel, F32).tobytes(), (got["vel"], vel)
+    o.close()
