@@ -106,6 +106,7 @@ def load() -> C.CDLL:
                                      _FP, C.POINTER(C.c_uint64)]),
         "orc_boundary_self_sum": (C.c_float, [_FP, C.c_uint64, C.c_float]),
         "orc_grid_probe_hash": (C.c_uint64, [C.c_uint64, C.c_uint64, C.c_uint32]),
+        "orc_consts": (None, [C.c_void_p, _DP]),
         "orc_set_providers": (None, [C.c_void_p, C.POINTER(OProvider), C.c_uint32, C.POINTER(OWallPlane)]),
         "orc_rigid_step": (None, [_FP, C.c_uint32, _FP, _FP, C.c_float, C.c_uint32, C.c_float, C.c_float]),
         "orc_box_mass_props": (None, [_FP, C.c_float, _FP, _FP]),
@@ -230,6 +231,14 @@ class OracleSystem:
             for a in range(4):
                 arr[q].rot[a] = b.rot[a]
         return int(self.lib.orc_set_bodies(self._h, arr, len(bodies)))
+
+    def consts(self) -> dict:
+        """h, h2, k6, ks, w0, skin (as float32 values) and the particle mass."""
+        out = np.zeros(6)
+        self.lib.orc_consts(self._h, out.ctypes.data_as(_DP))
+        d = dict(zip(("h", "h2", "k6", "ks", "w0", "skin"), (np.float32(x) for x in out)))
+        d["mass"] = np.float32(self.lib.orc_mass(self._h))
+        return d
 
     def set_providers(self, providers) -> None:
         """Provider walls: objects with `faces` [(axis, plane, sign)] (axis-aligned faces)

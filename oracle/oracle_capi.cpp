@@ -152,6 +152,17 @@ double orc_mass(void* p) {
   with<float>((Handle*)p, [&](auto& s) { m = (double)s.mass; });
   return m;
 }
+// The system's kernel constants (fluid_access.rs:7-13): h, h2, k6, ks, w0, skin.
+void orc_consts(void* p, double out[6]) {
+  with<float>((Handle*)p, [&](auto& s) {
+    out[0] = (double)s.h;
+    out[1] = (double)s.h2;
+    out[2] = (double)s.k6;
+    out[3] = (double)s.ks;
+    out[4] = (double)s.w0;
+    out[5] = (double)s.skin;
+  });
+}
 void orc_set_threads(void* p, uint32_t t) {
   with<float>((Handle*)p, [&](auto& s) { s.cfg.threads = t; });
 }

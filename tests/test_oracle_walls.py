@@ -126,3 +126,43 @@ def test_projection_and_separation_against_a_direct_restatement(oracle_mod):
     assert got["pos"].astype(F32).tobytes() == np.array(pos, F32).tobytes(), (got["pos"], pos)
     assert got["vel"].astype(F32).tobytes() == np.array(vel, F32).tobytes(), (got["vel"], vel)
     o.close()
+
+
+def test_mirror_ghost_density_against_a_direct_restatement(oracle_mod):
+    """One fluid particle 0.03 above FloorY with one neighbour: its density is
+    mass (w0 + W(r) + W(|pi - g|)) with g the neighbour mirrored in the floor plane collected
+    by wall_planes_in (fluid_density.rs:25-47, 76-118), each term in the reference's order;
+    the neighbour, 0.04 up, gets its own ghost of the first. Bit for bit."""
+    from vxl_sph import scenes
+    f = F32
+    c = oracle_mod.default_cfg()
+    o = oracle_mod.OracleSystem(c, origin=(0.0, 0.0, 0.0), dims=(2, 1, 1), spacing=0.05)
+    p0 = np.array([[0.0, 0.03, 0.0], [0.02, 0.04, 0.01]], F32)
+    o.set_state(p0, np.zeros_like(p0))
+    o.set_providers([scenes.floor_provider()])
+    k = o.consts()
+    o.substep(float(f(f(1.0) / f(240.0))))
+    got = o.read_f32()["dens"]
+    h, h2, k6, w0, mass = k["h"], k["h2"], k["k6"], k["w0"], k["mass"]
+
+    def W(r2):
+        t = f(h2 - r2)
+        return f(f(f(k6 * t) * t) * t)
+
+    want = []
+    for i, j in ((0, 1), (1, 0)):
+        pi, pj = p0[i], p0[j]
+        d = np.array([pi[a] - pj[a] for a in range(3)], F32)
+        r2 = f(f(d[0] * d[0] + d[1] * d[1]) + d[2] * d[2])
+        total = f(w0 + W(r2))
+        # the plane: contact (pi.x, 0, pi.z), normal +y; sdf = pi.y in (0, h)
+        q = np.array([pi[a] - d[a] for a in range(3)], F32)  # pj as pi - d
+        dn = f(f(f(q[0] - pi[0]) * f(0.0) + f(q[1] - f(0.0)) * f(1.0)) + f(q[2] - pi[2]) * f(0.0))
+        gpt = np.array([q[0] - f(0.0) * f(f(2.0) * dn), q[1] - f(1.0) * f(f(2.0) * dn), q[2] - f(0.0) * f(f(2.0) * dn)], F32)
+        e = np.array([pi[a] - gpt[a] for a in range(3)], F32)
+        rg2 = f(f(e[0] * e[0] + e[1] * e[1]) + e[2] * e[2])
+        if rg2 <= h2:
+            total = f(total + W(rg2))
+        want.append(f(f(mass * total) + f(0.0)))
+    assert np.asarray(got, F32)[:2].tobytes() == np.array(want, F32).tobytes(), (got, want)
+    o.close()
