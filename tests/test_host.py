@@ -242,3 +242,73 @@ def test_provider_arrays_packing(vxl):
     assert list(warr[5].normal) == [1.0, 0.0, 0.0] and np.isclose(warr[5].offset, 0.05)
     assert list(warr[6].normal) == [-1.0, 0.0, 0.0] and np.isclose(warr[6].offset, 0.05)
     assert (warr[11].axis, warr[11].offset, warr[11].sign) == (2, 1.5, -1.0)
+
+
+def _rigid_substep_restated(b, react, g, dt, maxl, maxa):
+    """One rigid substep of the coupling loop, float32, written from the reference's formulas:
+    gravity field force m g with m = 1 / inv_mass (crates/vxl-phys-field/src/lib.rs:22-31), the
+    fluid reaction added, Integrator::integrate_velocities with gravity zero and whole-vector
+    clamps, integrate_positions with Quat::integrate_angular (crates/vxl-phys-integrate/src/
+    lib.rs:18-60, crates/vxl-phys-core/src/math.rs:216-252, body.rs:172-176)."""
+    f = np.float32
+    pos, q, v, w = [list(map(f, b[a:c])) for a, c in ((0, 3), (3, 7), (7, 10), (10, 13))]
+    inv_m, ii = f(b[13]), list(map(f, b[14:17]))
+    mass = f(f(1.0) / inv_m)
+    force = [f(f(0.0) + f(g[a]) * mass) for a in range(3)]
+    force = [f(force[a] + f(react[a])) for a in range(3)]
+    torque = [f(f(0.0) + f(react[3 + a])) for a in range(3)]
+    v = [f(v[a] + f(f(0.0) + f(force[a] * inv_m)) * f(dt)) for a in range(3)]
+    x, y, z, qw = q
+    xx, yy, zz, xy, xz, yz, wx, wy, wz = (f(x * x), f(y * y), f(z * z), f(x * y), f(x * z), f(y * z), f(qw * x),
+                                          f(qw * y), f(qw * z))
+    m = [[f(1.0) - f(2.0) * f(yy + zz), f(2.0) * f(xy - wz), f(2.0) * f(xz + wy)],
+         [f(2.0) * f(xy + wz), f(1.0) - f(2.0) * f(xx + zz), f(2.0) * f(yz - wx)],
+         [f(2.0) * f(xz - wy), f(2.0) * f(yz + wx), f(1.0) - f(2.0) * f(xx + yy)]]
+    lt = [f(f(f(m[0][c] * torque[0]) + f(m[1][c] * torque[1])) + f(m[2][c] * torque[2])) for c in range(3)]
+    lt = [f(lt[c] * ii[c]) for c in range(3)]
+    aa = [f(f(f(m[r][0] * lt[0]) + f(m[r][1] * lt[1])) + f(m[r][2] * lt[2])) for r in range(3)]
+    w = [f(w[a] + f(aa[a] * f(dt))) for a in range(3)]
+    sp = np.sqrt(f(f(f(v[0] * v[0]) + f(v[1] * v[1])) + f(v[2] * v[2])), dtype=f)
+    if sp > f(maxl):
+        s = f(f(maxl) / sp)
+        v = [f(c * s) for c in v]
+    ws = np.sqrt(f(f(f(w[0] * w[0]) + f(w[1] * w[1])) + f(w[2] * w[2])), dtype=f)
+    if ws > f(maxa):
+        s = f(f(maxa) / ws)
+        w = [f(c * s) for c in w]
+    pos = [f(pos[a] + f(v[a] * f(dt))) for a in range(3)]
+    # dq = (w, 0) * q, Hamilton product
+    dqw = f(f(f(f(f(0.0) * qw) - f(w[0] * x)) - f(w[1] * y)) - f(w[2] * z))
+    dqx = f(f(f(f(f(0.0) * x) + f(w[0] * qw)) + f(w[1] * z)) - f(w[2] * y))
+    dqy = f(f(f(f(f(0.0) * y) - f(w[0] * z)) + f(w[1] * qw)) + f(w[2] * x))
+    dqz = f(f(f(f(f(0.0) * z) + f(w[0] * y)) - f(w[1] * x)) + f(w[2] * qw))
+    hd = f(f(0.5) * f(dt))
+    nq = [f(x + f(dqx * hd)), f(y + f(dqy * hd)), f(z + f(dqz * hd)), f(qw + f(dqw * hd))]
+    len2 = f(f(f(f(nq[0] * nq[0]) + f(nq[1] * nq[1])) + f(nq[2] * nq[2])) + f(nq[3] * nq[3]))
+    inv = f(f(1.0) / np.sqrt(len2, dtype=f))
+    nq = [f(c * inv) for c in nq]
+    return pos + nq + v + w
+
+
+@pytest.mark.parametrize("case", range(4))
+def test_oracle_rigid_substep_equals_direct_restatement(oracle_mod, case):
+    """The oracle's rigid substep (what the device coupling loop is checked against) equals a
+    float32 restatement of the reference's integrator formulas, bit for bit, including the
+    speed clamps."""
+    rng = np.random.default_rng(100 + case)
+    q = rng.normal(size=4).astype(np.float32)
+    q /= np.linalg.norm(q)
+    st = np.zeros((1, 18), np.float32)
+    st[0, 0:3] = rng.uniform(-1, 1, 3)
+    st[0, 3:7] = q
+    st[0, 7:10] = rng.uniform(-2, 2, 3) * (60.0 if case == 3 else 1.0)
+    st[0, 10:13] = rng.uniform(-3, 3, 3) * (30.0 if case == 3 else 1.0)
+    st[0, 13] = np.float32(1.0) / np.float32(rng.uniform(0.5, 5.0))
+    st[0, 14:17] = rng.uniform(1.0, 40.0, 3)
+    st[0, 17] = 1.0
+    react = rng.uniform(-20, 20, (1, 6)).astype(np.float32)
+    g = (0.0, -9.81, 0.0)
+    dt = float(np.float32(np.float32(1.0) / np.float32(60.0)) / np.float32(2.0))
+    want = _rigid_substep_restated(st[0].copy(), react[0], g, dt, 100.0, 50.0)
+    oracle_mod.rigid_step(st, react, g, dt, 1, 100.0, 50.0)
+    assert st[0, :13].tobytes() == np.array(want, np.float32).tobytes(), (st[0, :13], want)
