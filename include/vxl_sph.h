@@ -361,7 +361,7 @@ vxl_status vxl_sph_read_rigid_bodies(vxl_sph_handle* h, uint32_t scene, vxl_sph_
  * path. n = 0 removes the scene's providers. */
 #define VXL_SPH_PROVIDER_FACES 0u
 #define VXL_SPH_PROVIDER_CONVEX 1u
-#define VXL_SPH_MAX_PROVIDER_PLANES 64u  /* planes per scene */
+#define VXL_SPH_MAX_PROVIDER_PLANES 64u  /* planes per scene, and providers per scene */
 typedef struct vxl_sph_wall_plane {
   float normal[3];  /* CONVEX: outward unit normal */
   float offset;     /* CONVEX: offset d; FACES: the face's plane coordinate */
