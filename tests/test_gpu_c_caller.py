@@ -1,18 +1,19 @@
 """The library driven from C (tests/c/stepper_loop.c), the way a Rust shim or a C++ engine
 calls it: the FluidStepper::step pattern over several ticks gives the same state and
 reactions, bit for bit, as the same calls made through the Python binding."""
-import subprocess
+import ctypes as C
 import struct
+import subprocess
+from pathlib import Path
 
 import numpy as np
 import pytest
 
 pytestmark = pytest.mark.gpu
-ROOT = __import__("pathlib").Path(__file__).resolve().parent.parent
+ROOT = Path(__file__).resolve().parent.parent
 
 
 def test_c_caller_equals_python_binding(vxl, tmp_path):
-    import ctypes as C
     from vxl_sph import scenes
     spec = scenes.small_dam(n=(10, 12, 9), spacing=0.05, tank=(0.8, 0.7, 0.6))
     nf, nb = spec.n_fluid, spec.n_boundary
