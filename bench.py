@@ -145,6 +145,57 @@ def build_scene(workload: str):
     return scenes.CONFIGS[workload]()
 
 
+def measure_coupled(spec, local: int, steps: int, warmup: int, density: float = 500.0) -> dict:
+    """The scene's boxes as dynamic rigid bodies kept on the device (vxl_sph_step_coupled:
+    two rigid substeps from the previous tick's reactions, the boundary rebuilt from the new
+    poses, the fluid tick; the tank walls static; no contact solver), `steps` coupled ticks
+    from the initial state and the initial bodies, the reactions back on the host each tick."""
+    import torch
+    import vxl_sph
+    from vxl_sph import scenes
+    bodies, dynamic = spec.meta["bodies"], spec.meta["dynamic"]
+    p = spec.params
+    lat, idx = scenes.body_lattice(bodies, spec.spacing, p.smoothing_radius, p.boundary_layers)
+    inv_mass, inertia = [], []
+    for b, d in zip(bodies, dynamic):
+        im, ii = scenes.box_mass_props(b.half, density) if d else (0.0, (0.0, 0.0, 0.0))
+        inv_mass.append(im)
+        inertia.append(ii)
+    g = vxl_sph.Scene(spec.params, spec.pos, spec.vel, spec.pmass, spec.n_fluid, device=local)
+    stream = torch.cuda.Stream(device=local)
+    g.set_stream(stream.cuda_stream)
+    g.set_body_lattice(lat, idx, len(bodies))
+    g.set_spans(spec.spans)
+    dt = float(np.float32(1.0) / np.float32(60.0))
+    grav = (0.0, -9.81, 0.0)
+    nspans = len(spec.spans)
+
+    def reset():
+        g.write_state(spec.pos, spec.vel)
+        g.set_rigid_bodies(bodies, inv_mass, inertia, dynamic)
+
+    reset()
+    for _ in range(max(warmup, 2)):
+        g.step_coupled(dt, 2, grav, 100.0, 50.0, nspans)
+    reset()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        e0.record(stream)
+    for _ in range(steps):
+        g.step_coupled(dt, 2, grav, 100.0, 50.0, nspans)
+    with torch.cuda.stream(stream):
+        e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    g.close()
+    upd = spec.n_fluid * spec.params.substeps * steps
+    return {"workload": f"{spec.name} with its {sum(dynamic)} boxes dynamic (density {density} kg/m^3), "
+                        "the coupling loop on the device, no contact solver",
+            "value": upd / (ms / 1e3), "unit": UNIT, "ms_per_tick": ms / steps, "rigid_substeps": 2,
+            "call": "vxl_sph_step_coupled per tick (reactions to the host; bodies stay on the device)"}
+
+
 def cpu_baseline(spec, budget_s: float = 12.0) -> dict:
     """The oracle (C++ restatement of the reference's phase-parallel CPU path) on the host
     cores, on a bounded sample of the same workload: whole substeps from the scene's
@@ -384,6 +435,8 @@ def run_ours(args) -> None:
                   "vxl_sph_read_state (positions), pinned host buffers: the FluidStepper::step pattern"}
 
     mix = {}
+    if world == 1 and spec.meta.get("dynamic") and any(spec.meta["dynamic"]) and not args.no_coupled:
+        mix["coupled"] = measure_coupled(spec, local, steps=args.steps, warmup=args.warmup)
     if world == 1 and not args.no_mix:
         scene.close()
         mix["batched"] = measure_batched(local, steps=3, warmup=3)
@@ -727,6 +780,7 @@ def main():
     ap.add_argument("--scenes", type=int, default=256, help="batched: number of tanks")
     ap.add_argument("--no-plain", action="store_true", help="batched/served: skip the plain-path comparison")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-coupled", action="store_true", help="skip the coupled-bodies line of scenes with boxes")
     ap.add_argument("--cpu-threads", type=int, default=0, help="reference arm: host threads (default: all)")
     ap.add_argument("--ncu-case", action="store_true", help="build + warm-up ticks only (for ncu captures)")
     ap.add_argument("--ncu-block", type=int, default=0,

@@ -237,10 +237,12 @@ def dam_break(name: str, dims, spacing: float, tank, ticks: int, seed: int, extr
               layers: int = 1, **over) -> SceneSpec:
     params = baseline_params(spacing, substeps=substeps, layers=layers, **over)
     fluid = jitter(fluid_block((0.0, 0.0, 0.0), dims, spacing), spacing, seed)
-    bodies = tank_bodies(tank, 2.0 * spacing) + list(extra_bodies)
+    walls = tank_bodies(tank, 2.0 * spacing)
+    bodies = walls + list(extra_bodies)
     fill = float(np.prod(np.asarray(dims) * spacing) / np.prod(tank))
     return assemble(name, params, fluid, bodies, spacing, ticks,
-                    {"dims": tuple(dims), "tank": tuple(tank), "fill": fill, "seed": seed})
+                    {"dims": tuple(dims), "tank": tuple(tank), "fill": fill, "seed": seed, "bodies": bodies,
+                     "dynamic": [False] * len(walls) + [True] * len(extra_bodies)})
 
 
 def floating_boxes(n: int, seed: int, lo, hi, half_lo: float, half_hi: float, first_id: int, gap: float) -> list:
