@@ -144,18 +144,20 @@ def test_multi_tick_bit_exact_with_reactions(vxl, oracle_mod, ticks):
     compare_grid(g, o, "final grid")
 
 
-@pytest.mark.parametrize("case", [c for c in GOLDEN["cases"] if c["n"] in (40, 50)], ids=lambda c: f"n{c['n']}")
+@pytest.mark.parametrize("case", GOLDEN["cases"], ids=lambda c: f"n{c['n']}_bins{c['max_bins']}")
 def test_published_hash_through_gpu(vxl, oracle_mod, case):
     """The reference's grid-probe scene run on the GPU: 5 + 1 ticks of the default
     config, then the FNV hash of the table of the last substep equals the published
-    CPU hash (crates/vxl-phys-gpu/examples/gpu_grid_probe.rs:181-226)."""
+    CPU hash (crates/vxl-phys-gpu/examples/gpu_grid_probe.rs:181-226) — for every published
+    case, up to the 9,938,375-particle lattice, whose 2^20 cell budget doubles the bins (the
+    half-culled density walk at full size)."""
     n = case["n"]
     s = F32(0.05)
     nf = F32(n)
     origin = (-nf * s * F32(0.5), F32(0.5), -nf * s * F32(0.5))
     from vxl_sph import scenes
     pos = scenes.fluid_block(origin, (n, n, n), 0.05)
-    p = vxl.make_params()
+    p = vxl.make_params(max_bins=case["max_bins"])
     p.particle_mass = vxl.lattice_mass(p, 0.05)
     g = vxl.Scene(p, pos, np.zeros_like(pos), np.full(pos.shape[0], F32(p.particle_mass)), pos.shape[0])
     dt_tick = float(F32(1.0) / F32(60.0))
