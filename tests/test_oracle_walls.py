@@ -149,7 +149,7 @@ def test_mirror_ghost_density_against_a_direct_restatement(oracle_mod):
         t = f(h2 - r2)
         return f(f(f(k6 * t) * t) * t)
 
-    want = []
+    want, ghosts = [], 0
     for i, j in ((0, 1), (1, 0)):
         pi, pj = p0[i], p0[j]
         d = np.array([pi[a] - pj[a] for a in range(3)], F32)
@@ -163,6 +163,60 @@ def test_mirror_ghost_density_against_a_direct_restatement(oracle_mod):
         rg2 = f(f(e[0] * e[0] + e[1] * e[1]) + e[2] * e[2])
         if rg2 <= h2:
             total = f(total + W(rg2))
+            ghosts += 1
         want.append(f(f(mass * total) + f(0.0)))
+    assert ghosts == 2
+    assert np.asarray(got, F32)[:2].tobytes() == np.array(want, F32).tobytes(), (got, want)
+    o.close()
+
+
+def test_convex_provider_decisive_plane_ghost_against_a_direct_restatement(oracle_mod):
+    """Two particles 0.02 and 0.03 off the +x face of a convex box obstacle (HalfSpaceSet): the plane of
+    largest n.p - d decides (plane_set.rs:60-76), its contact point p - n (n.p - d) and
+    normal give the mirror plane; the particle's density with one neighbour is
+    mass (w0 + W(r) + W(|pi - g|)) in the reference's order, bit for bit."""
+    from vxl_sph import scenes
+    f = F32
+    c = oracle_mod.default_cfg()
+    o = oracle_mod.OracleSystem(c, origin=(0.0, 0.0, 0.0), dims=(2, 1, 1), spacing=0.05)
+    p0 = np.array([[0.07, 0.1, 0.0], [0.08, 0.11, 0.01]], F32)  # the box spans x in [-0.05, 0.05]
+    o.set_state(p0, np.zeros_like(p0))
+    box = scenes.box_obstacle((0.0, 0.1, 0.0), (0.05, 0.1, 0.05))
+    o.set_providers([box])
+    k = o.consts()
+    o.substep(float(f(f(1.0) / f(240.0))))
+    got = o.read_f32()["dens"]
+    h, h2, k6, w0, mass = k["h"], k["h2"], k["k6"], k["w0"], k["mass"]
+
+    def W(r2):
+        t = f(h2 - r2)
+        return f(f(f(k6 * t) * t) * t)
+
+    def dot(a, b):
+        return f(f(f(a[0] * b[0]) + f(a[1] * b[1])) + f(a[2] * b[2]))
+
+    planes = [(np.array(n, F32), f(d)) for n, d in box.planes]
+    want, ghosts = [], 0
+    for i, j in ((0, 1), (1, 0)):
+        pi, pj = p0[i], p0[j]
+        ss = [f(dot(n, pi) - d) for n, d in planes]
+        kb = int(np.argmax(ss))  # first maximum, like the strict > scan
+        n, d = planes[kb]
+        t = f(dot(n, pi) - d)
+        point = np.array([pi[a] - f(n[a] * t) for a in range(3)], F32)
+        sdf = dot(np.array([pi[a] - point[a] for a in range(3)], F32), n)
+        dvec = np.array([pi[a] - pj[a] for a in range(3)], F32)
+        total = f(w0 + W(dot(dvec, dvec)))
+        if f(0.0) < sdf < h:
+            q = np.array([pi[a] - dvec[a] for a in range(3)], F32)
+            dn = dot(np.array([q[a] - point[a] for a in range(3)], F32), n)
+            gpt = np.array([q[a] - f(n[a] * f(f(2.0) * dn)) for a in range(3)], F32)
+            e = np.array([pi[a] - gpt[a] for a in range(3)], F32)
+            rg2 = dot(e, e)
+            if rg2 <= h2:
+                total = f(total + W(rg2))
+                ghosts += 1
+        want.append(f(f(mass * total) + f(0.0)))
+    assert ghosts == 2  # each particle's neighbour has a mirror image within h
     assert np.asarray(got, F32)[:2].tobytes() == np.array(want, F32).tobytes(), (got, want)
     o.close()
