@@ -220,3 +220,53 @@ def test_convex_provider_decisive_plane_ghost_against_a_direct_restatement(oracl
     assert ghosts == 2  # each particle's neighbour has a mirror image within h
     assert np.asarray(got, F32)[:2].tobytes() == np.array(want, F32).tobytes(), (got, want)
     o.close()
+
+
+def _still_box(bid, half, pos):
+    from vxl_sph import scenes
+    return scenes.Body(bid, half, pos)
+
+
+def test_boundary_particles_hold_fluid_column(oracle_mod):
+    """tests.rs:439-476: a 12x12x10 block on an Akinci floor (a box body, no providers) for 60
+    ticks stays finite and its core does not leak below -0.06."""
+    o = _system(oracle_mod, (-0.3, 0.0, -0.3), (12, 12, 10), [])
+    floor = [_still_box(0, (0.5, 0.05, 0.5), (0.0, -0.05, 0.0))]
+    assert o.set_bodies(floor) > 0
+    dt = float(F32(1.0) / F32(60.0))
+    for _ in range(60):
+        o.set_bodies(floor)
+        o.step(dt)
+    p = o.read_f32()["pos"][:o.n_fluid]
+    assert np.all(np.isfinite(p))
+    core = (np.abs(p[:, 0]) <= 0.25) & (np.abs(p[:, 2]) <= 0.25)
+    assert p[core, 1].min() > -0.06, p[core, 1].min()
+    o.close()
+
+
+def test_submerged_box_gets_buoyant_reaction(oracle_mod):
+    """tests.rs:492-561: a box (half 0.06) held in a 7^3 column in the Tank provider: over a
+    60-tick window after 180 ticks of settling, the mean reaction on it is 0.5-2 rho V g up,
+    its sideways components and torque near zero — the Akinci reactions and the provider
+    walls together (the oracle gives 1.07 rho V g up)."""
+    from vxl_sph import scenes
+    o = _system(oracle_mod, (-0.15, 0.05, -0.15), (7, 7, 7), [scenes.tank_provider()], xsph_viscosity=0.05)
+    half = 0.06
+    body = [_still_box(7, (half, half, half), (0.0, 0.12, 0.0))]
+    dt = float(F32(1.0) / F32(60.0))
+    for _ in range(180):
+        o.set_bodies(body)
+        o.step(dt)
+    f_sum, t_sum = np.zeros(3), np.zeros(3)
+    for _ in range(60):
+        o.set_bodies(body)
+        o.step(dt)
+        r = [x for x in o.reactions() if x[0] == 7][0]
+        f_sum += r[1]
+        t_sum += r[2]
+    force, tau = f_sum / 60, t_sum / 60
+    expect = 1000.0 * (2 * half) ** 3 * 9.81
+    assert 0.5 * expect < force[1] < 2.0 * expect, (force, expect)
+    assert abs(force[0]) < 0.5 * expect and abs(force[2]) < 0.5 * expect, force
+    assert np.linalg.norm(tau) < 0.5 * expect * half, tau
+    o.close()
