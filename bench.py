@@ -145,6 +145,37 @@ def build_scene(workload: str):
     return scenes.CONFIGS[workload]()
 
 
+# The CPU path's bounded sample of each plain workload: one substep of the dam10m tank
+# (walls, 64 boxes, constants and doubled bins as in the workload) holding a 100^3 fluid
+# block instead of 215^3, so that a step of the reference arm takes seconds, not half a
+# minute; dam0 and dam1 are sampled whole.
+SAMPLE_BLOCK = {"dam10m": 100}
+
+
+def cpu_sample_spec(workload: str):
+    from vxl_sph import scenes
+    if workload in SAMPLE_BLOCK:
+        return scenes.dam10m_block(SAMPLE_BLOCK[workload])
+    return build_scene(workload)
+
+
+def workload_config(spec) -> dict:
+    """The `config` object of both arms' lines for a plain workload (identical in each)."""
+    tank = spec.meta.get("tank")
+    return {"workload": spec.name, "n_fluid": spec.n_fluid, "n_boundary": spec.n_boundary,
+            "substeps": int(spec.params.substeps), "h": float(spec.params.smoothing_radius),
+            "spacing": float(spec.spacing), "tank": list(tank) if tank else None, "fill": spec.meta.get("fill"),
+            "bodies": len(spec.spans), "dynamic_boxes": int(sum(spec.meta.get("dynamic", []))),
+            "unit_of_work": "one fluid particle advanced through one full substep"}
+
+
+def use_oracle_lattice() -> None:
+    """Build scenes with the oracle's lattice restatement (the CPU arm loads no CUDA library)."""
+    from oracle import oracle as orc
+    from vxl_sph import scenes
+    scenes.use_lattice_source(*orc.scene_lattice_source())
+
+
 def measure_coupled(spec, local: int, steps: int, warmup: int, density: float = 500.0) -> dict:
     """The scene's boxes as dynamic rigid bodies kept on the device (vxl_sph_step_coupled:
     two rigid substeps from the previous tick's reactions, the boundary rebuilt from the new
@@ -196,11 +227,12 @@ def measure_coupled(spec, local: int, steps: int, warmup: int, density: float = 
             "call": "vxl_sph_step_coupled per tick (reactions to the host; bodies stay on the device)"}
 
 
-def cpu_baseline(spec, budget_s: float = 12.0) -> dict:
+def cpu_baseline(workload: str, budget_s: float = 12.0) -> dict:
     """The oracle (C++ restatement of the reference's phase-parallel CPU path) on the host
-    cores, on a bounded sample of the same workload: whole substeps from the scene's
-    initial state until budget_s of wall time is used."""
+    cores, on a bounded sample of the same workload (cpu_sample_spec): whole substeps from
+    the sample's initial state until budget_s of wall time is used."""
     from oracle import oracle as orc
+    spec = cpu_sample_spec(workload)
     cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
     o = orc.OracleSystem.from_scene(spec, threads=cores)
     dt = float(np.float32(np.float32(1.0) / np.float32(60.0)) / np.float32(spec.params.substeps))
@@ -219,9 +251,13 @@ def cpu_baseline(spec, budget_s: float = 12.0) -> dict:
 
 
 def run_reference(args) -> None:
+    """The reference arm: the reference's CPU path (the oracle, its C++ restatement; Rust is
+    not buildable here) on all host cores, rank 0 only. Scenes are built with the oracle's
+    lattice, so this process loads no library of this repository's product."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
+    use_oracle_lattice()
     from oracle import oracle as orc
     cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
     if args.cpu_threads:
@@ -230,10 +266,13 @@ def run_reference(args) -> None:
         run_reference_mix(args, orc, cores)
         return
     spec = build_scene(args.workload)
-    o = orc.OracleSystem.from_scene(spec, threads=cores)
-    dt_sub = float(np.float32(np.float32(1.0) / np.float32(60.0)) / np.float32(spec.params.substeps))
-    # one step = one substep of the workload (a bounded sample of the tick the GPU arm
-    # times; the metric is per particle-update so the two are comparable)
+    config = workload_config(spec)
+    del spec
+    sample = cpu_sample_spec(args.workload)
+    o = orc.OracleSystem.from_scene(sample, threads=cores)
+    dt_sub = float(np.float32(np.float32(1.0) / np.float32(60.0)) / np.float32(sample.params.substeps))
+    # one step = one substep of the bounded sample (the metric is per particle-update, so
+    # it compares with the GPU arm's ticks of the whole workload)
     for _ in range(args.warmup):
         o.substep(dt_sub)
     times = []
@@ -241,17 +280,19 @@ def run_reference(args) -> None:
         t0 = time.perf_counter()
         o.substep(dt_sub)
         times.append(time.perf_counter() - t0)
+    o.close()
     total = sum(times)
-    value = spec.n_fluid * args.steps / total
+    value = sample.n_fluid * args.steps / total
+    desc = (f"{args.steps} substeps of {sample.name} ({sample.n_fluid} fluid + {sample.n_boundary} boundary "
+            f"particles) after {args.warmup} warm-up substeps, {cores} threads")
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic (seeded dam break)",
-        "config": {"workload": spec.name, "n_fluid": spec.n_fluid, "n_boundary": spec.n_boundary,
-                   "step": "one substep on the host cores (reference CPU path restated in C++; Rust not buildable here)"},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
-                         "sample": f"{args.steps} substeps of {spec.name} after {args.warmup} warm-up substeps"},
+        "data": "synthetic: seeded dam break in an Akinci-walled tank (no public dataset exists)",
+        "config": config,
+        "step": "one substep of the bounded sample on the host cores (the reference CPU path restated in C++)",
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": desc},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -437,14 +478,16 @@ def run_ours(args) -> None:
     mix = {}
     if world == 1 and spec.meta.get("dynamic") and any(spec.meta["dynamic"]) and not args.no_coupled:
         mix["coupled"] = measure_coupled(spec, local, steps=args.steps, warmup=args.warmup)
-    if world == 1 and not args.no_mix:
+    if not args.no_mix:
+        # scene-parallel on several GPUs: each rank takes its share of the tanks / requests
         scene.close()
-        mix["batched"] = measure_batched(local, steps=3, warmup=3)
-        mix["served"] = measure_served(local, n_requests=args.requests, rate=args.rate, tick_scale=args.tick_scale)
+        mix["batched"] = measure_batched(local, steps=3, warmup=3, rank=rank, world=world, dist=dist)
+        mix["served"] = measure_served(local, n_requests=args.requests, rate=args.rate, tick_scale=args.tick_scale,
+                                       rank=rank, world=world, dist=dist)
 
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(spec)
+        cpu = cpu_baseline(args.workload)
 
     if rank == 0:
         line = {
@@ -452,12 +495,11 @@ def run_ours(args) -> None:
             "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32",
             "data": "synthetic: seeded dam break in an Akinci-walled tank (no public dataset exists)",
-            "config": {"workload": spec.name, "n_fluid": spec.n_fluid, "n_boundary": spec.n_boundary,
-                       "substeps": sub, "cells": cells, "step": "one 60 Hz tick (10 substeps)",
-                       "l2": "flushed between steps (256 MiB write outside the timed events)",
-                       "parallelism": f"replicas x{world}", "h": spec.params.smoothing_radius,
-                       "tuning": tune,
-                       "spacing": spec.spacing, "fill": spec.meta.get("fill")},
+            "config": workload_config(spec),
+            "step": "one 60 Hz tick (10 substeps) of the whole workload on the GPU",
+            "run": {"cells": cells, "l2": "flushed between steps (256 MiB write outside the timed events)",
+                    "parallelism": f"replicas x{world} (each rank steps its own copy of the scene)",
+                    "tuning": tune},
             "roofline": roofline,
             "cpu_baseline": cpu,
             "e2e": e2e,
@@ -766,13 +808,27 @@ def run_ncu_case(args) -> None:
                       "n_boundary": spec.n_boundary}))
 
 
+def launch_ranks(n: int, argv=None) -> int:
+    """`--gpus N` started directly (no WORLD_SIZE in the environment): run N ranks of this
+    script with the same arguments under torch.distributed.run on this node (one process
+    per GPU, rendezvous on 127.0.0.1) and return the launcher's exit status."""
+    import socket
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={n}",
+           "--master-addr", "127.0.0.1", "--master-port", str(port), str(Path(__file__).resolve()),
+           *(sys.argv[1:] if argv is None else argv)]
+    return subprocess.call(cmd)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", default="dam1", choices=["dam0", "dam1", "dam10m", "batched", "served"])
+    ap.add_argument("--workload", default="dam10m", choices=["dam0", "dam1", "dam10m", "batched", "served"])
     ap.add_argument("--requests", type=int, default=48, help="served: number of requests")
     ap.add_argument("--rate", type=float, default=200.0, help="served: Poisson arrival rate (1/s)")
     ap.add_argument("--tick-scale", type=float, default=0.1, help="served: factor on the 60-600 tick counts")
@@ -786,6 +842,8 @@ def main():
     ap.add_argument("--ncu-block", type=int, default=0,
                     help="ncu case of dam10m: an N^3 fluid block in the same tank (bins still doubled)")
     args = ap.parse_args()
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ and not args.ncu_case:
+        sys.exit(launch_ranks(args.gpus))
     if args.ncu_case:
         run_ncu_case(args)
     elif args.impl == "reference":

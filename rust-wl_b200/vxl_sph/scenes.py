@@ -25,9 +25,36 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from . import Params, boundary_lattice, lattice_mass, make_params
+from . import Params, make_params
 
 F = np.float32
+
+# Where the lattice-mass calibration and the Akinci body lattices come from. By default
+# the library's own host code (vxl_sph_lattice_mass, vxl_sph_boundary_lattice); a
+# caller that must not load the CUDA library (the CPU baseline) installs another source
+# computing the same float32 values with use_lattice_source().
+_LATTICE_SOURCE = None
+
+
+def use_lattice_source(mass_fn=None, lattice_fn=None) -> None:
+    """Install mass_fn(params, spacing) -> float and lattice_fn(shape, half, radius,
+    spacing, h, layers) -> (points (N, 3) float32, volume); None restores the library's."""
+    global _LATTICE_SOURCE
+    _LATTICE_SOURCE = None if mass_fn is None else (mass_fn, lattice_fn)
+
+
+def lattice_mass(params: Params, spacing: float) -> float:
+    if _LATTICE_SOURCE is not None:
+        return _LATTICE_SOURCE[0](params, spacing)
+    from . import lattice_mass as lib_mass
+    return lib_mass(params, spacing)
+
+
+def boundary_lattice(shape: int, half, radius: float, spacing: float, h: float, layers: int):
+    if _LATTICE_SOURCE is not None:
+        return _LATTICE_SOURCE[1](shape, half, radius, spacing, h, layers)
+    from . import boundary_lattice as lib_lattice
+    return lib_lattice(shape, half, radius, spacing, h, layers)
 
 
 @dataclass

@@ -41,3 +41,37 @@ def test_reference_arm_on_the_batched_sample():
     line = json.loads(r.stdout.strip().splitlines()[-1])
     assert line["impl"] == "reference" and line["value"] > 0
     assert line["config"]["workload"] == "batched" and line["config"]["scenes"] == 2
+
+
+def test_reference_arm_loads_no_product_library():
+    """The reference arm builds its scene with the oracle's lattice restatement: the
+    process maps the oracle library and never the CUDA library of the product."""
+    code = ("import sys; sys.argv = ['bench.py', '--impl', 'reference', '--workload', 'dam0', '--steps', '1', "
+            "'--warmup', '0']; import bench; bench.main(); "
+            "maps = open('/proc/self/maps').read(); "
+            "print('MAPS', 'libvxl_sph' in maps, 'liboracle_wcsph' in maps)")
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=600, cwd=ROOT)
+    assert r.returncode == 0, r.stderr
+    assert "MAPS False True" in r.stdout, r.stdout[-500:]
+
+
+def test_reference_arm_config_is_the_gpu_arms():
+    """Both arms print the same `config` object for a plain workload."""
+    r = _run({}, "--workload", "dam0", "--steps", "1", "--warmup", "0")
+    assert r.returncode == 0, r.stderr
+    line = json.loads(r.stdout.strip().splitlines()[-1])
+    sys.path[:0] = [str(ROOT), str(ROOT / "rust-wl_b200")]
+    import bench
+    assert line["config"] == json.loads(json.dumps(bench.workload_config(bench.build_scene("dam0"))))
+
+
+def test_gpus_flag_launches_ranks():
+    """`--gpus 2` without a launcher starts two ranks itself (torch.distributed.run on
+    127.0.0.1); on the reference arm rank 0 alone prints its line, with n_gpus 2."""
+    env = {k: v for k, v in os.environ.items() if k not in ("RANK", "WORLD_SIZE", "LOCAL_RANK")}
+    r = subprocess.run([sys.executable, str(ROOT / "bench.py"), "--impl", "reference", "--gpus", "2",
+                        "--workload", "dam0", "--steps", "1", "--warmup", "0"],
+                       capture_output=True, text=True, env=env, timeout=600, cwd=ROOT)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [json.loads(x) for x in r.stdout.splitlines() if x.startswith("{")]
+    assert len(lines) == 1 and lines[0]["n_gpus"] == 2 and lines[0]["impl"] == "reference"
