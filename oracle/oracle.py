@@ -97,6 +97,7 @@ def load() -> C.CDLL:
         "orc_read_f32": (None, [C.c_void_p] + [_FP] * 8),
         "orc_grid": (C.c_uint64, [C.c_void_p, _U32P, C.c_uint64, _U32P, _FP, _FP, _U32P]),
         "orc_reactions": (C.c_uint32, [C.c_void_p, C.POINTER(OReaction), C.c_uint32]),
+        "orc_neighbors": (C.c_uint64, [C.c_void_p, C.POINTER(C.c_uint64), _U32P, C.c_uint64]),
         "orc_aggregate_with": (None, [C.c_void_p, _FP, C.c_int]),
         "orc_scale_reactions": (None, [C.c_void_p, C.c_float]),
         "orc_spans": (C.c_uint32, [C.c_void_p, C.POINTER(OSpan), C.c_uint32]),
@@ -319,6 +320,16 @@ class OracleSystem:
                           None)
         return {"start": start, "items": items, "min": mn, "inv": ib[0], "bin": ib[1], "dims": dims, "total": total}
 
+    def neighbors(self):
+        """The next substep's neighbour lists (walk order; fluid neighbours only for boundary
+        particles) from the current positions, as CSR (offsets (n + 1,) uint64, entries uint32)."""
+        n = self.n_total
+        offs = np.empty(n + 1, np.uint64)
+        total = int(self.lib.orc_neighbors(self._h, offs.ctypes.data_as(C.POINTER(C.c_uint64)), None, 0))
+        ent = np.empty(max(total, 1), np.uint32)
+        self.lib.orc_neighbors(self._h, offs.ctypes.data_as(C.POINTER(C.c_uint64)), ent.ctypes.data_as(_U32P), total)
+        return offs, ent[:total]
+
     def reactions(self):
         arr = (OReaction * 4096)()
         n = int(self.lib.orc_reactions(self._h, arr, 4096))
@@ -420,3 +431,19 @@ def box_mass_props(half, density: float):
     ii = np.zeros(3, np.float32)
     lib.orc_box_mass_props(_f(h), float(density), C.byref(im), _f(ii))
     return np.float32(im.value), ii
+
+
+def lattice_mass(params, spacing: float) -> float:
+    """FluidSystem::new's mass calibration (crates/vxl-phys-fluid/src/fluid_access.rs:27-42)
+    for a library Params struct."""
+    return float(load().orc_lattice_mass(C.byref(cfg_from_params(params)), spacing))
+
+
+def scene_lattice_source():
+    """(mass_fn, lattice_fn) for vxl_sph.scenes.use_lattice_source: the oracle's own
+    restatement of the lattice-mass calibration and of boundary::lattice, so a CPU-only
+    caller builds the same scenes without loading the CUDA library."""
+    def lat(shape, half, radius, spacing, h, layers):
+        pts, vol, _ = lattice(shape, half, radius, spacing, h, layers)
+        return pts, vol
+    return lattice_mass, lat

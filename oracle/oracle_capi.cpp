@@ -328,6 +328,34 @@ uint64_t orc_grid(void* p, uint32_t* start, uint64_t start_cap, uint32_t* items,
   return total;
 }
 
+// The neighbour lists of the next substep, the lists its density pass walks: the grid is
+// rebuilt from the current positions exactly as FluidSystem::substep does
+// (crates/vxl-phys-fluid/src/fluid_step.rs:96-100, grid.rs:29-76), and for every particle
+// i the neighbours j of UniformGrid::for_neighbors_in (grid.rs:115-155) are listed in its
+// walk order — all of them for a fluid particle, the fluid ones for a boundary particle
+// (fluid_density.rs:59-69). CSR in particle order: offsets[0..n], entries[offsets[i]..
+// offsets[i + 1]]. Returns the entry count; entries are written only if cap holds them.
+uint64_t orc_neighbors(void* p, uint64_t* offsets, uint32_t* entries, uint64_t cap) {
+  auto* hd = (Handle*)p;
+  if (!hd->f) return 0;
+  auto& s = *hd->f;
+  UniformGrid<float> g;
+  g.rebuild(s.pos, s.h, s.cfg.max_bins);
+  const size_t n = s.pos.size(), nf = s.n_fluid;
+  uint64_t total = 0;
+  for (size_t i = 0; i < n; ++i) {
+    if (offsets) offsets[i] = total;
+    const bool fluid_i = i < nf;
+    g.for_neighbors_in(s.pos, s.h2, i, [&](size_t j, const V3<float>&, float) {
+      if (!fluid_i && j >= nf) return;
+      if (entries && total < cap) entries[total] = (uint32_t)j;
+      ++total;
+    });
+  }
+  if (offsets) offsets[n] = total;
+  return total;
+}
+
 uint32_t orc_reactions(void* p, orc_reaction* out, uint32_t cap) {
   uint32_t n = 0;
   with<float>((Handle*)p, [&](auto& s) {
