@@ -109,6 +109,7 @@ def load() -> C.CDLL:
         "orc_grid_probe_hash": (C.c_uint64, [C.c_uint64, C.c_uint64, C.c_uint32]),
         "orc_consts": (None, [C.c_void_p, _DP]),
         "orc_set_providers": (None, [C.c_void_p, C.POINTER(OProvider), C.c_uint32, C.POINTER(OWallPlane)]),
+        "orc_set_wall_contacts": (None, [C.c_void_p, C.c_uint32, _U32P, _U32P, C.c_uint32, _FP]),
         "orc_rigid_step": (None, [_FP, C.c_uint32, _FP, _FP, C.c_float, C.c_uint32, C.c_float, C.c_float]),
         "orc_box_mass_props": (None, [_FP, C.c_float, _FP, _FP]),
     }
@@ -268,6 +269,15 @@ class OracleSystem:
                 warr[k].normal[a] = n[a]
             warr[k].d, warr[k].axis, warr[k].sign = d, ax, sg
         self.lib.orc_set_providers(self._h, parr, len(recs), warr)
+
+    def set_wall_contacts(self, side: int, ids, start, planes) -> None:
+        """Contact table of one side (0 mirror, 1 projection): ids (E,) ascending fluid
+        indices, start (E + 1,), planes (P, 6) point + outward normal; E = 0 removes it."""
+        ids = np.ascontiguousarray(ids, np.uint32)
+        start = np.ascontiguousarray(start, np.uint32)
+        planes = np.ascontiguousarray(planes, np.float32).reshape(-1, 6)
+        self.lib.orc_set_wall_contacts(self._h, side, ids.ctypes.data_as(_U32P), start.ctypes.data_as(_U32P),
+                                       ids.shape[0], _f(planes))
 
     def set_boundary_raw(self, pos, vel, pmass, spans):
         pos = np.ascontiguousarray(pos, np.float32)

@@ -234,6 +234,36 @@ void orc_set_providers(void* p, const orc_provider* pr, uint32_t n, const orc_wa
   });
 }
 
+// Contact table of one side (0: mirror, 1: projection) as the GPU tier uploads it
+// (WallStage::upload, crates/vxl-phys-gpu/src/pipeline/walls.rs:100-121): entries e with
+// particle ids[e] (fluid, ascending) and planes [start[e], start[e + 1]) of `planes`
+// (point xyz, outward normal xyz). n_entries = 0 removes the table.
+void orc_set_wall_contacts(void* p, uint32_t side, const uint32_t* ids, const uint32_t* start, uint32_t n_entries,
+                           const float* planes) {
+  with<float>((Handle*)p, [&](auto& s) {
+    using R = std::decay_t<decltype(s.h)>;
+    auto& t = s.ctab[side & 1u];
+    t.off.clear();
+    t.pt.clear();
+    t.n.clear();
+    if (n_entries == 0) return;
+    t.off.assign(s.n_fluid + 1, 0);
+    std::vector<uint32_t> cnt(s.n_fluid, 0);
+    for (uint32_t e = 0; e < n_entries; ++e) cnt[ids[e]] = start[e + 1] - start[e];
+    for (size_t i = 0; i < s.n_fluid; ++i) t.off[i + 1] = t.off[i] + cnt[i];
+    t.pt.resize(t.off[s.n_fluid]);
+    t.n.resize(t.off[s.n_fluid]);
+    for (uint32_t e = 0; e < n_entries; ++e) {
+      uint32_t o = t.off[ids[e]];
+      for (uint32_t k = start[e]; k < start[e + 1]; ++k, ++o) {
+        const float* q = planes + 6 * (size_t)k;
+        t.pt[o] = V3<R>(q[0], q[1], q[2]);
+        t.n[o] = V3<R>(q[3], q[4], q[5]);
+      }
+    }
+  });
+}
+
 // Replace the boundary suffix with explicit particles (the FluidStepper view: the
 // facade hands over pos/vel/pmass of the boundary segment plus the span table).
 int orc_set_boundary_raw(void* p, uint64_t nb, const float* pos, const float* vel, const float* pm,

@@ -604,6 +604,24 @@ struct Provider {
   }
 };
 
+// Contact tables of the GPU tier's provider walls (crates/vxl-phys-gpu/src/pipeline/walls.rs:
+// 143-215, WallStage::upload :100-121): the host gathers, once per tick, for each fluid
+// particle the contacts of every ProviderColliders — of any kind, voxel, mesh or SDF —
+// as (point, outward normal) planes, one table for the mirror ghosts (contacts_point,
+// 0 < sdf < h) and one for the projection (contacts_point_boundary, sdf < h), at most 8
+// per particle; the substeps of that tick read the tables instead of querying providers.
+// Here a table acts as one more provider after the registered ones, queried by particle
+// index: its contacts for particle i are the table's planes of i (no bounds prefilter).
+template <class R>
+struct ContactTable {
+  std::vector<uint32_t> off;   // n_fluid + 1 offsets into pt / n (empty: no table)
+  std::vector<V3<R>> pt, n;
+  void contacts(size_t i, std::vector<Contact<R>>& out) const {
+    if (off.empty() || i + 1 >= off.size()) return;
+    for (uint32_t k = off[i]; k < off[i + 1]; ++k) out.push_back(Contact<R>{pt[k], n[k], R(0)});
+  }
+};
+
 // ---------------------------------------------------------------- fluid system
 // crates/vxl-phys-fluid/src/system.rs:5-51 (fields) and fluid_access.rs:7-76 (new)
 template <class R>
@@ -618,6 +636,8 @@ struct FluidSystem {
   UniformGrid<R> grid;
   std::vector<std::pair<Shape<R>, BoundaryLattice<R>>> lattice_cache;
   std::vector<Provider<R>> providers;  // the registered boundaries, in order
+  ContactTable<R> ctab[2];             // contact tables: [0] mirror, [1] projection
+  bool walls() const { return !providers.empty() || !ctab[0].off.empty() || !ctab[1].off.empty(); }
   R skin;                              // fluid_access.rs:47 (0.15 h)
 
   // crates/vxl-phys-fluid/src/fluid_access.rs:7-76
@@ -738,13 +758,10 @@ struct FluidSystem {
 
   // crates/vxl-phys-fluid/src/fluid_density.rs:76-118 (wall_planes_in): the provider
   // planes within h of a fluid particle (contact point + outward normal, 0 < sdf < h), <= 8.
-  size_t wall_planes(const V3<R>& pi, V3<R> pl_pt[8], V3<R> pl_n[8]) const {
+  size_t wall_planes(size_t i, const V3<R>& pi, V3<R> pl_pt[8], V3<R> pl_n[8]) const {
     size_t np = 0;
     std::vector<Contact<R>> scratch;
-    for (const auto& pr : providers) {
-      if (pr.outside(pi, h)) continue;
-      scratch.clear();
-      pr.contacts_point(pi, h, scratch);
+    auto take = [&]() {
       for (const auto& c : scratch) {
         R sdf = (pi - c.point).dot(c.normal);
         if (sdf > R(0) && sdf < h && np < 8) {
@@ -753,7 +770,16 @@ struct FluidSystem {
           ++np;
         }
       }
+    };
+    for (const auto& pr : providers) {
+      if (pr.outside(pi, h)) continue;
+      scratch.clear();
+      pr.contacts_point(pi, h, scratch);
+      take();
     }
+    scratch.clear();
+    ctab[0].contacts(i, scratch);  // the mirror table (contacts_point, gathered per tick)
+    take();
     return np;
   }
 
@@ -761,17 +787,14 @@ struct FluidSystem {
   // inside a provider are pushed out along each contact normal by min(pen + skin, h), their
   // inward normal velocity removed; the pushed ones then go through separate_coincident.
   void boundary_pass() {
-    if (providers.empty()) return;
+    if (providers.empty() && ctab[1].off.empty()) return;
     std::vector<std::pair<size_t, V3<R>>> pushed;
     std::vector<Contact<R>> contacts;
     for (size_t i = 0; i < n_fluid; ++i) {
       V3<R> pi = pos[i];
       V3<R> p = pi, v = vel[i], n_sum;
       bool hit = false;
-      for (const auto& pr : providers) {
-        if (pr.outside(pi, h)) continue;
-        contacts.clear();
-        pr.contacts_point(pi, skin, contacts);  // contacts_point_boundary
+      auto apply = [&]() {
         for (const auto& c : contacts) {
           R sdf = (pi - c.point).dot(c.normal);
           R pen = -sdf;
@@ -784,6 +807,17 @@ struct FluidSystem {
         }
         pos[i] = p;
         vel[i] = v;
+      };
+      for (const auto& pr : providers) {
+        if (pr.outside(pi, h)) continue;
+        contacts.clear();
+        pr.contacts_point(pi, skin, contacts);  // contacts_point_boundary
+        apply();
+      }
+      if (!ctab[1].off.empty()) {  // the projection table (contacts_point_boundary, gathered per tick)
+        contacts.clear();
+        ctab[1].contacts(i, contacts);
+        apply();
       }
       if (hit) pushed.emplace_back(i, n_sum);
     }
@@ -855,7 +889,7 @@ struct FluidSystem {
       V3<R> pl_pt[8], pl_n[8];
       for (size_t i = b; i < e; ++i) {
         V3<R> pi = pos[i];
-        size_t np = providers.empty() ? 0 : wall_planes(pi, pl_pt, pl_n);
+        size_t np = walls() ? wall_planes(i, pi, pl_pt, pl_n) : 0;
         R sum = w0, sum_b = R(0);
         for_neighbors(i, [&](size_t j, const V3<R>& d, R r2) {
           R t = h2 - r2;

@@ -270,3 +270,63 @@ def test_submerged_box_gets_buoyant_reaction(oracle_mod):
     assert abs(force[0]) < 0.5 * expect and abs(force[2]) < 0.5 * expect, force
     assert np.linalg.norm(tau) < 0.5 * expect * half, tau
     o.close()
+
+
+class _FloorSdf:
+    """A floor y = 0 answered as a host-side provider (closest point and normal), the same
+    contacts the fluid crate's FloorY face provider reports (tests.rs:9-44, 81-110)."""
+
+    def bounds(self, bid):
+        return ((-50.0, -1.0, -50.0), (50.0, 0.0, 50.0))
+
+    def contacts_point(self, bid, p, probe):
+        if p[1] > F32(2) * F32(probe):
+            return []
+        return [(np.array([p[0], 0.0, p[2]], F32), np.array([0.0, 1.0, 0.0], F32))]
+
+
+def test_contact_tables_equal_the_floor_provider_at_one_substep(oracle_mod):
+    """With one substep per tick a table gathered each tick from the current positions is
+    exactly the provider's answer for that substep, so the table-driven oracle (the GPU
+    tier's gather, crates/vxl-phys-gpu/src/pipeline/walls.rs:164-215) and the oracle that
+    queries FloorY itself give the same state bit for bit through landing and rest."""
+    from vxl_sph import scenes, walls
+    a = _system(oracle_mod, (-0.1, 0.3, -0.1), (5, 5, 5), [scenes.floor_provider()], xsph_viscosity=0.05,
+                substeps=1)
+    b = _system(oracle_mod, (-0.1, 0.3, -0.1), (5, 5, 5), [], xsph_viscosity=0.05, substeps=1)
+    h = 0.1
+    dt = float(F32(1.0) / F32(60.0))
+    entries = 0
+    for t in range(60):
+        ps = b.read_f32()["pos"]
+        for side in (walls.MIRROR, walls.PROJECT):
+            ids, start, planes = walls.gather_contacts([0], h, ps, _FloorSdf(), side)
+            entries = max(entries, ids.shape[0])
+            b.set_wall_contacts(side, ids, start, planes)
+        a.step(dt)
+        b.step(dt)
+        ra, rb = a.read_f32(), b.read_f32()
+        assert ra["pos"].tobytes() == rb["pos"].tobytes(), f"tick {t}"
+        assert ra["vel"].tobytes() == rb["vel"].tobytes(), f"tick {t}"
+    assert entries > 20
+    assert ra["pos"][:, 1].min() > -0.01
+    a.close()
+    b.close()
+
+
+def test_gather_contacts_rules():
+    """Mirror keeps 0 < sdf < h, projection sdf < h, at most 8 planes, bounds grown by h."""
+    from vxl_sph import walls
+
+    class Many:
+        def bounds(self, bid):
+            return ((-1.0, -1.0, -1.0), (1.0, 0.0, 1.0))
+
+        def contacts_point(self, bid, p, probe):
+            return [(np.array([p[0], 0.0, p[2]], F32), np.array([0.0, 1.0, 0.0], F32))] * 5
+
+    ps = np.array([[0.0, 0.05, 0.0], [0.0, -0.02, 0.0], [0.0, 0.5, 0.0], [5.0, 0.05, 0.0]], F32)
+    ids, start, planes = walls.gather_contacts([0, 1], 0.1, ps, Many(), walls.MIRROR)
+    assert ids.tolist() == [0] and start.tolist() == [0, 8] and planes.shape == (8, 6)
+    ids, start, _ = walls.gather_contacts([0], 0.1, ps, Many(), walls.PROJECT)
+    assert ids.tolist() == [0, 1] and start.tolist() == [0, 5, 10]
