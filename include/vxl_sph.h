@@ -197,6 +197,20 @@ vxl_status vxl_sph_read_fields(vxl_sph_handle* h, float* dens, float* press, flo
 vxl_status vxl_sph_export_grid(vxl_sph_handle* h, uint32_t* items, uint32_t* start, uint64_t start_cap,
                                uint32_t* bins, vxl_sph_grid_info* info);
 
+/* Neighbour lists of the last substep, as its density pass recorded them and its force
+ * pass and boundary reactions read them: for particle i (reference index order) the
+ * neighbours j != i within h, in the walk order of UniformGrid::for_neighbors_in
+ * (crates/vxl-phys-fluid/src/grid.rs:115-155, over the table FluidSystem::neighbor_grid
+ * exposes, fluid_access.rs:125-133) — every neighbour of a fluid particle, the fluid ones
+ * of a boundary particle (the terms of fluid_density.rs:17-70). CSR: offsets[n_total + 1]
+ * (offsets_len must be n_total + 1) and entries[offsets[i] .. offsets[i + 1]]. With
+ * entries NULL only offsets and *total are written (call once to size, once to fill);
+ * entries_cap below the total is VXL_SIZE_MISMATCH. Lists longer than the recorded cap
+ * are walked again from that substep's sorted positions, as the consumers do. Valid until
+ * the next substep starts. */
+vxl_status vxl_sph_export_neighbors(vxl_sph_handle* h, uint64_t* offsets, uint64_t offsets_len, uint32_t* entries,
+                                    uint64_t entries_cap, uint64_t* total);
+
 /* Counts for the caller's own accounting: particles, cells of the last substep,
  * kernel launches of the last tick, bytes of device memory held. */
 typedef struct vxl_sph_stats {
@@ -381,6 +395,28 @@ typedef struct vxl_sph_provider {
 vxl_status vxl_sph_set_providers(vxl_sph_handle* h, uint32_t scene, const vxl_sph_provider* providers,
                                  uint32_t nproviders, const vxl_sph_wall_plane* planes, uint32_t nplanes);
 
+/* Provider walls of ANY ProviderColliders (voxel terrain, meshes, splats, SDFs), as the
+ * reference's GPU tier feeds them (GpuFluidStepper::gather_walls,
+ * crates/vxl-phys-gpu/src/pipeline/stepper.rs:118-137; gather_wall_contacts /
+ * gather_wall_project_contacts and WallStage::upload, pipeline/walls.rs:100-215): once per
+ * tick the caller reads the fluid positions, queries its providers on the host and uploads
+ * two contact tables. side 0 (mirror): for each fluid particle the planes of
+ * contacts_point(bid, p, h) with 0 < sdf < h; side 1 (projection): those of
+ * contacts_point_boundary(bid, p, h) with sdf < h; at most 8 per particle, sdf =
+ * (p - point) . normal. ids[n_entries] are ascending scene-local fluid indices, entry e
+ * owns planes [start[e], start[e + 1]) (start has n_entries + 1 values from 0 to
+ * n_planes) and planes holds n_planes x (point xyz, outward normal xyz). The tables then
+ * act as one more provider of the scene, after its analytic ones, for every substep until
+ * replaced: each substep the mirror planes within 0 < sdf < h of the particle's current
+ * position give its mirror ghosts (fluid_density.rs:25-47), and after integration the
+ * projection planes push penetrating particles out (fluid_boundary.rs:45-128), with the
+ * coincident-particle separation of the CPU path. n_entries = 0 clears that side. */
+#define VXL_SPH_WALLS_MIRROR 0u
+#define VXL_SPH_WALLS_PROJECT 1u
+vxl_status vxl_sph_set_wall_contacts(vxl_sph_handle* h, uint32_t scene, uint32_t side, const uint32_t* ids,
+                                     const uint32_t* start, uint32_t n_entries, const float* planes,
+                                     uint32_t n_planes);
+
 /* ------------------------------------------------------------------ served form
  * A request loop (the served workload): scene-step requests are submitted at any time,
  * admitted while their device footprint fits an HBM budget, stepped together with
@@ -424,6 +460,12 @@ vxl_status vxl_sph_serve_submit(vxl_sph_server* s, const vxl_sph_desc* desc, uin
 /* Retire finished scenes, admit queued ones that fit, then advance every admitted scene by
  * one substep of its own dt = dt_tick / substeps. Synchronous. */
 vxl_status vxl_sph_serve_step(vxl_sph_server* s, float dt_tick, vxl_sph_serve_report* report);
+/* Latency knob of the served form: admission stops while the admitted scenes hold
+ * max_fluid_particles fluid particles or more (a request larger than that is admitted
+ * when nothing else runs), which bounds the work of each substep and so the per-tick
+ * latency of admitted requests, at the cost of queueing the rest longer. 0 (the
+ * default) admits while the memory budget allows. No counterpart in the reference. */
+vxl_status vxl_sph_serve_set_batch_cap(vxl_sph_server* s, uint64_t max_fluid_particles);
 vxl_status vxl_sph_serve_poll(vxl_sph_server* s, uint64_t id, vxl_sph_request_status* out);
 /* Positions/velocities of a running or finished request (scene-local order). */
 vxl_status vxl_sph_serve_read(vxl_sph_server* s, uint64_t id, float* pos_xyz, float* vel_xyz);
@@ -448,11 +490,18 @@ vxl_status vxl_sph_serve_tick_times(vxl_sph_server* s, uint64_t id, double* out_
  * Limits: n <= 524,288 particles and max_bins <= 524,288 cells (0 means 524,288);
  * larger sizes return VXL_INVALID_ARGUMENT. Working memory is one fixed array of about
  * 8.4 MB inside the library, held by every GPU that loads it until the process exits;
- * the call makes no cudaMalloc, cudaFree or other allocating call. The first call on a
- * device looks the array's address up (cudaGetSymbolAddress): make that first call
- * before any stream capture on that device. Every call reuses the same array (the
- * counts it needs zeroed are cleared at the start of each call), so calls that overlap
- * on the GPU — from two streams or two host threads — race and must not be made. */
+ * the call makes no cudaMalloc, cudaFree or other allocating call of its own. The first
+ * call on a device is the set-up: the CUDA runtime loads the library's device code there
+ * (mapping the array, which takes device memory and may synchronise the device), the
+ * call looks the array's address up (cudaGetSymbolAddress) and raises one kernel's
+ * shared-memory limit. Make that first call at start-up, as a warm-up (n = 1 will do),
+ * before reserving the rest of the device's memory; later calls on that device take no
+ * device memory. Every call is synchronous (it copies the grid box back and waits for
+ * its stream), so no call may be made inside stream capture. Every call reuses the same
+ * array (the counts it needs zeroed are cleared at the start of each call), so calls
+ * that overlap on the GPU — from two streams or two host threads — race and must not be
+ * made. Cells of any size are sorted in bounded time (warp, shared-memory rank, or a
+ * bitmap of the particle indices for cells above 2,048 entries). */
 vxl_status vxl_sph_build_grid_static(const float* d_pos_xyz, uint32_t n, float h, uint32_t max_bins,
                                      uint32_t* d_items, uint32_t* d_start, uint64_t start_cap,
                                      vxl_sph_grid_info* info, void* cuda_stream);

@@ -228,6 +228,17 @@ vxl_status vxl_sph_set_providers(vxl_sph_handle* h, uint32_t scene, const vxl_sp
   }
 }
 
+vxl_status vxl_sph_set_wall_contacts(vxl_sph_handle* h, uint32_t scene, uint32_t side, const uint32_t* ids,
+                                     const uint32_t* start, uint32_t n_entries, const float* planes,
+                                     uint32_t n_planes) {
+  HANDLE_OR_FAIL(h);
+  try {
+    return h->e->set_wall_contacts(scene, side, ids, start, n_entries, planes, n_planes);
+  } catch (...) {
+    return set_error(VXL_PANIC_CAUGHT, "exception in vxl_sph_set_wall_contacts");
+  }
+}
+
 vxl_status vxl_sph_set_body_lattice(vxl_sph_handle* h, uint32_t scene, const float* local_xyz,
                                     const uint32_t* body_index, uint64_t nb, uint32_t nbodies) {
   HANDLE_OR_FAIL(h);
@@ -362,6 +373,12 @@ vxl_status vxl_sph_export_grid_scene(vxl_sph_handle* h, uint32_t scene, uint32_t
   if (info && !check_header(info->hdr, sizeof(vxl_sph_grid_info)))
     return set_error(VXL_SIZE_MISMATCH, "grid_info header");
   return h->e->export_grid(scene, items, start, start_cap, bins, info);
+}
+
+vxl_status vxl_sph_export_neighbors(vxl_sph_handle* h, uint64_t* offsets, uint64_t offsets_len, uint32_t* entries,
+                                    uint64_t entries_cap, uint64_t* total) {
+  HANDLE_OR_FAIL(h);
+  return h->e->export_neighbors(0, offsets, offsets_len, entries, entries_cap, total);
 }
 
 vxl_status vxl_sph_get_stats(vxl_sph_handle* h, vxl_sph_stats* out) {

@@ -34,11 +34,13 @@ inline uint32_t blocks_for(uint64_t n, int t = kThreads) { return (uint32_t)((n 
 enum KernelId : int {
   KID_CELLOFF, KID_KEYS, KID_SCAN_PARTIAL, KID_SCAN_FINAL, KID_PLACE, KID_CANON,
   KID_DENSITY, KID_FORCE, KID_BFORCE, KID_REACT_CHUNKS, KID_REACT_SPANS, KID_SCALE, KID_HALFMASK, KID_WALLS,
-  KID_COUNT
+  KID_GROUPS, KID_COUNT
 };
 const char* const kKernelNames[KID_COUNT] = {
     "k_celloff", "k_keys", "k_scan_partial", "k_scan_final", "k_place", "k_canon",
-    "k_density", "k_force", "k_bforce", "k_react_chunks", "k_react_spans", "k_scale", "k_halfmask", "k_walls"};
+    "k_density", "k_force", "k_bforce", "k_react_chunks", "k_react_spans", "k_scale", "k_halfmask", "k_walls",
+    "k_groups"};
+constexpr int kSegWarps = 8;  // warps per block of the grouped density pass
 
 constexpr size_t kSceneHostBytes = offsetof(SceneDev, g);
 
@@ -89,8 +91,9 @@ namespace vxl {
 
 uint64_t Engine::bytes_per_slot(uint32_t nbr_cap) {
   // pos, vel (x2), orig, slot_of, cellrank, items, rc, press, acc, xsph, bforce, bpos,
-  // neighbour list + count, staging, density thread order at doubled bins
-  return 4 * 16 + 4 + 4 + 8 + 8 + 8 + 4 + 16 + 16 + 16 + 16 + (uint64_t)nbr_cap * 4 + 4 + 32 + 1 + 4;
+  // neighbour list + count, staging, half masks, density thread orders (walls variant and
+  // grouped pass), density segments
+  return 4 * 16 + 4 + 4 + 8 + 8 + 8 + 4 + 16 + 16 + 16 + 16 + (uint64_t)nbr_cap * 4 + 4 + 32 + 1 + 4 + 4 + 8;
 }
 
 uint64_t Engine::bytes_per_cell() { return 12; }  // counts, start, wet
@@ -169,6 +172,8 @@ vxl_status Engine::alloc_all() {
   A(dalloc(&counts_, cell_cap_ + 1));
   A(dalloc(&wet_, cell_cap_ + 1));
   A(dalloc(&xorder_, slot_cap_));
+  A(dalloc(&order_, slot_cap_));
+  A(dalloc((uint2**)&segs_, slot_cap_));
   A(dalloc(&start_, cell_cap_ + 1));
   A(dalloc(&partial_, cell_cap_ / kScanTile + 2));
   A(dalloc(&sc_d_, scene_cap_));
@@ -198,7 +203,7 @@ void Engine::free_all() {
   if (graph_) cudaGraphExecDestroy(graph_);
   graph_ = nullptr;
   void* d[] = {pos_[0], pos_[1], vel_[0], vel_[1], orig_, slot_of_, cellrank_, items_, rc_, press_, acc_, xsph_,
-               bforce_, bpos_, nbr_, nbr_n_, halves_, xorder_, stage_, counts_, wet_, start_, partial_, sc_d_, tiles_d_, ctl_d_, spans_d_,
+               bforce_, bpos_, nbr_, nbr_n_, halves_, xorder_, order_, segs_, stage_, counts_, wet_, start_, partial_, sc_d_, tiles_d_, ctl_d_, spans_d_,
                chunks_d_, chunk_first_d_, react_partial_, breact_d_};
   for (void* p : d)
     if (p) cudaFree(p);
@@ -211,12 +216,18 @@ void Engine::free_all() {
   ev_snap_ = nullptr;
   if (rb_d_) cudaFree(rb_d_);
   rb_d_ = nullptr;
-  void* wd[] = {prov_d_, wplanes_d_, pflag_, pnsum_, plist_, pblk_};
+  void* wd[] = {prov_d_,      wplanes_d_,    pflag_,        pnsum_,        plist_,   pblk_,
+                ct_ent_d_[0], ct_ent_d_[1],  ct_ids_d_[0],  ct_ids_d_[1],  ct_start_d_[0],
+                ct_start_d_[1], ct_pl_d_[0], ct_pl_d_[1]};
   for (void* p : wd)
     if (p) cudaFree(p);
   prov_d_ = nullptr;
   wplanes_d_ = nullptr;
   pflag_ = plist_ = pblk_ = nullptr;
+  for (int k = 0; k < 2; ++k) {
+    ct_ent_d_[k] = ct_ids_d_[k] = ct_start_d_[k] = nullptr;
+    ct_pl_d_[k] = nullptr;
+  }
   pnsum_ = nullptr;
   if (blocal_) cudaFree(blocal_);
   if (poses_d_) cudaFree(poses_d_);
@@ -264,6 +275,9 @@ void Engine::set_tuning(const Tuning& t) {
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_f, k_e_force<256>, 256, 0);
   }
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_b, k_e_bforce, 128, 0);
+  int occ_s = 1;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_s, k_e_density_seg<kSegWarps>, kSegWarps * 32, 0);
+  grid_seg_ = sms * std::max(1, occ_s);
   cudaGetLastError();
   // waves == 0: one block per tile (the grid is sized from the tile count at launch)
   grid_density_ = sms * std::max(1, occ_d) * (int)tuning_.waves;
@@ -461,6 +475,20 @@ vxl_status Engine::remove_scenes(const std::vector<uint32_t>& indices) {
     prov_first_st_.clear();  // restaged below, after the slots have moved
     prov_count_st_.clear();
   }
+  for (int side = 0; side < 2; ++side) {  // contact tables follow their scenes
+    if (ct_ids_h_[side].empty()) continue;
+    std::vector<std::vector<uint32_t>> ki, ks;
+    std::vector<std::vector<float>> kpl;
+    for (uint32_t q = 0; q < drop.size(); ++q)
+      if (!drop[q] && q < ct_ids_h_[side].size()) {
+        ki.push_back(ct_ids_h_[side][q]);
+        ks.push_back(ct_start_h_[side][q]);
+        kpl.push_back(ct_pl_h_[side][q]);
+      }
+    ct_ids_h_[side].swap(ki);
+    ct_start_h_[side].swap(ks);
+    ct_pl_h_[side].swap(kpl);
+  }
   if (!rigid_.empty()) {  // coupled bodies follow their scenes
     std::vector<std::vector<vxl_sph_rigid_body>> keep_rigid;
     for (uint32_t q = 0; q < drop.size(); ++q)
@@ -652,6 +680,126 @@ vxl_status Engine::step_coupled_async(float dt_tick, uint32_t rigid_substeps, co
 
 // ---------------------------------------------------------------- provider walls
 
+bool Engine::scene_has_table(uint32_t q) const {
+  for (int side = 0; side < 2; ++side)
+    if (q < ct_ids_h_[side].size() && !ct_ids_h_[side][q].empty()) return true;
+  return false;
+}
+
+ContactTableDev Engine::ctab(int side) const {
+  return ContactTableDev{ct_ent_d_[side], ct_start_d_[side], ct_pl_d_[side]};
+}
+
+// The contact tables of one side of a scene, as the reference's GPU tier uploads them per
+// tick (WallStage::upload, crates/vxl-phys-gpu/src/pipeline/walls.rs:100-121).
+vxl_status Engine::set_wall_contacts(uint32_t q, uint32_t side, const uint32_t* ids, const uint32_t* start,
+                                     uint32_t n, const float* planes, uint32_t nplanes) {
+  if (q >= scenes_.size()) return set_error(VXL_INVALID_ARGUMENT, "scene index out of range");
+  if (side > 1u) return set_error(VXL_INVALID_ARGUMENT, "side must be 0 (mirror) or 1 (projection)");
+  if (n && (!ids || !start)) return set_error(VXL_NULL_POINTER, "ids/start is NULL with entries");
+  if (nplanes && !planes) return set_error(VXL_NULL_POINTER, "planes is NULL");
+  const SceneInfo& si = scenes_[q];
+  if (n) {
+    if (start[0] != 0u || start[n] != nplanes) return set_error(VXL_SIZE_MISMATCH, "start must run from 0 to n_planes");
+    for (uint32_t e = 0; e < n; ++e) {
+      if (ids[e] >= si.nf) return set_error(VXL_INVALID_ARGUMENT, "contact id is not a fluid particle");
+      if (e && ids[e] <= ids[e - 1]) return set_error(VXL_INVALID_ARGUMENT, "contact ids must ascend");
+      if (start[e + 1] < start[e] || start[e + 1] - start[e] > kMaxWallPlanes)
+        return set_error(VXL_INVALID_ARGUMENT, "each entry holds 0..8 planes");
+    }
+    for (uint64_t k = 0; k < 6ull * nplanes; ++k)
+      if (!std::isfinite(planes[k])) return set_error(VXL_INVALID_ARGUMENT, "planes must be finite");
+  } else if (nplanes) {
+    return set_error(VXL_SIZE_MISMATCH, "planes without entries");
+  }
+  CU(cudaSetDevice(device_));
+  prof_collect();
+  for (int k = 0; k < 2; ++k)
+    if (ct_ids_h_[k].size() < scenes_.size()) {
+      ct_ids_h_[k].resize(scenes_.size());
+      ct_start_h_[k].resize(scenes_.size());
+      ct_pl_h_[k].resize(scenes_.size());
+    }
+  const bool had = scene_has_table(q);
+  ct_ids_h_[side][q].assign(ids, ids + n);
+  ct_start_h_[side][q].assign(start, start + (n ? n + 1 : 0));
+  ct_pl_h_[side][q].assign(planes, planes + 6ull * nplanes);
+  if (had != scene_has_table(q)) return stage_walls();  // the scene's provider list changes
+  return upload_tables();
+}
+
+// All scenes' contact tables to the device (stream-ordered before the next tick); device
+// arrays grow by doubling, and a tick graph that holds their old addresses is dropped.
+vxl_status Engine::upload_tables() {
+  bool any = false;
+  for (int side = 0; side < 2; ++side)
+    for (const auto& v : ct_ids_h_[side]) any = any || !v.empty();
+  if (!any && !ct_ent_d_[0]) return VXL_OK;
+  bool moved = false;
+  for (int side = 0; side < 2; ++side) {
+    std::vector<uint32_t> gids, gstart(1, 0u);
+    std::vector<float4> gpl;
+    for (uint32_t q = 0; q < scenes_.size() && q < ct_ids_h_[side].size(); ++q) {
+      const auto& ids = ct_ids_h_[side][q];
+      const auto& st = ct_start_h_[side][q];
+      const auto& pl = ct_pl_h_[side][q];
+      for (size_t e = 0; e < ids.size(); ++e) {
+        gids.push_back((uint32_t)scenes_[q].base + ids[e]);
+        for (uint32_t k = st[e]; k < st[e + 1]; ++k) {
+          const float* c = &pl[6ull * k];
+          gpl.push_back(make_float4(c[0], c[1], c[2], 0.0f));
+          gpl.push_back(make_float4(c[3], c[4], c[5], 0.0f));
+        }
+        gstart.push_back((uint32_t)(gpl.size() / 2));
+      }
+    }
+    if (!ct_ent_d_[side]) {
+      vxl_status s = dalloc(&ct_ent_d_[side], slot_cap_);
+      if (s != VXL_OK) return s;
+      moved = true;
+    }
+    if (gids.size() + 1 > ct_ids_cap_[side]) {
+      const uint64_t cap = std::max<uint64_t>(2 * ct_ids_cap_[side], gids.size() + 1);
+      if (ct_ids_d_[side]) cudaFree(ct_ids_d_[side]);
+      if (ct_start_d_[side]) cudaFree(ct_start_d_[side]);
+      ct_ids_d_[side] = ct_start_d_[side] = nullptr;
+      ct_ids_cap_[side] = 0;
+      vxl_status s = dalloc(&ct_ids_d_[side], cap);
+      if (s == VXL_OK) s = dalloc(&ct_start_d_[side], cap);
+      if (s != VXL_OK) return s;
+      ct_ids_cap_[side] = cap;
+      moved = true;
+    }
+    if (gpl.size() + 2 > ct_pl_cap_[side]) {
+      const uint64_t cap = std::max<uint64_t>(2 * ct_pl_cap_[side], gpl.size() + 2);
+      if (ct_pl_d_[side]) cudaFree(ct_pl_d_[side]);
+      ct_pl_d_[side] = nullptr;
+      ct_pl_cap_[side] = 0;
+      vxl_status s = dalloc(&ct_pl_d_[side], cap);
+      if (s != VXL_OK) return s;
+      ct_pl_cap_[side] = cap;
+      moved = true;
+    }
+    CU(cudaMemsetAsync(ct_ent_d_[side], 0, std::max<uint64_t>(used_, 1) * 4, stream_));
+    if (!gids.empty()) {
+      CU(cudaMemcpyAsync(ct_ids_d_[side], gids.data(), gids.size() * 4, cudaMemcpyHostToDevice, stream_));
+      CU(cudaMemcpyAsync(ct_start_d_[side], gstart.data(), gstart.size() * 4, cudaMemcpyHostToDevice, stream_));
+      if (!gpl.empty())
+        CU(cudaMemcpyAsync(ct_pl_d_[side], gpl.data(), gpl.size() * 16, cudaMemcpyHostToDevice, stream_));
+      k_e_ctab_scatter<<<blocks_for(gids.size()), kThreads, 0, stream_>>>(ct_ids_d_[side], (uint32_t)gids.size(),
+                                                                          ct_ent_d_[side]);
+      CU(cudaGetLastError());
+    }
+  }
+  // the host vectors are freed on return: wait until the pageable copies have been taken
+  CU(cudaStreamSynchronize(stream_));
+  if (moved && graph_) {
+    cudaGraphExecDestroy(graph_);
+    graph_ = nullptr;
+  }
+  return VXL_OK;
+}
+
 vxl_status Engine::set_providers(uint32_t q, const vxl_sph_provider* pr, uint32_t n, const vxl_sph_wall_plane* planes,
                                  uint32_t nplanes) {
   if (q >= scenes_.size()) return set_error(VXL_INVALID_ARGUMENT, "scene index out of range");
@@ -698,7 +846,11 @@ vxl_status Engine::stage_walls() {
   std::vector<WallPlaneDev> hw;
   prov_first_st_.assign(scenes_.size(), 0u);
   prov_count_st_.assign(scenes_.size(), 0u);
-  for (uint32_t q = 0; q < scenes_.size() && q < prov_h_.size(); ++q) {
+  if (prov_h_.size() < scenes_.size()) {
+    prov_h_.resize(scenes_.size());
+    wplanes_h_.resize(scenes_.size());
+  }
+  for (uint32_t q = 0; q < scenes_.size(); ++q) {
     prov_first_st_[q] = (uint32_t)hp.size();
     prov_count_st_[q] = (uint32_t)prov_h_[q].size();
     const uint32_t wbase = (uint32_t)hw.size();
@@ -725,6 +877,12 @@ vxl_status Engine::stage_walls() {
       d.bmaxy = p.bounds_max[1];
       d.bmaxz = p.bounds_max[2];
       hp.push_back(d);
+    }
+    if (scene_has_table(q)) {  // the contact tables come after the analytic providers
+      ProviderDev d{};
+      d.kind = kProviderTable;
+      hp.push_back(d);
+      ++prov_count_st_[q];
     }
   }
   walls_any_ = !hp.empty();
@@ -754,6 +912,10 @@ vxl_status Engine::stage_walls() {
     if (s != VXL_OK) return s;
   }
   if (pflag_) CU(cudaMemset(pflag_, 0, slot_cap_ * sizeof(uint32_t)));
+  {
+    vxl_status s = upload_tables();
+    if (s != VXL_OK) return s;
+  }
   std::vector<float> dts(scenes_.size());
   for (uint32_t q = 0; q < scenes_.size(); ++q) dts[q] = sc_h_[q].dt;
   vxl_status s = push_scene_records(dts);
@@ -976,6 +1138,50 @@ vxl_status Engine::export_grid(uint32_t q, uint32_t* items, uint32_t* start, uin
   return VXL_OK;
 }
 
+vxl_status Engine::export_neighbors(uint32_t q, uint64_t* offsets, uint64_t offsets_len, uint32_t* entries,
+                                    uint64_t entries_cap, uint64_t* total) {
+  if (q >= scenes_.size()) return set_error(VXL_INVALID_ARGUMENT, "scene index out of range");
+  if (!offsets) return set_error(VXL_NULL_POINTER, "offsets is NULL");
+  if (!ran_substep_) return set_error(VXL_NOT_READY, "no substep has run yet");
+  const SceneInfo& si = scenes_[q];
+  const uint32_t n = si.nf + si.nb;
+  if (offsets_len != (uint64_t)n + 1) return set_error(VXL_SIZE_MISMATCH, "offsets must hold n_total + 1 entries");
+  CU(cudaSetDevice(device_));
+  uint32_t* cnt = (uint32_t*)stage_;
+  std::vector<uint32_t> counts(n);
+  if (n) {
+    k_e_export_nbr_counts<<<blocks_for(n), kThreads, 0, stream_>>>(nbr_n_, orig_, si.base, n, cnt);
+    CU(cudaGetLastError());
+    CU(cudaMemcpyAsync(counts.data(), cnt, (size_t)n * 4, cudaMemcpyDeviceToHost, stream_));
+    CU(cudaStreamSynchronize(stream_));
+  }
+  uint64_t acc = 0;
+  for (uint32_t i = 0; i < n; ++i) {
+    offsets[i] = acc;
+    acc += counts[i];
+  }
+  offsets[n] = acc;
+  if (total) *total = acc;
+  if (!entries || acc == 0) return VXL_OK;
+  if (entries_cap < acc) return set_error(VXL_SIZE_MISMATCH, "entries buffer smaller than the list total");
+  unsigned long long* off_d = nullptr;
+  uint32_t* ent_d = nullptr;
+  cudaError_t ce = cudaMalloc(&off_d, ((size_t)n + 1) * 8);
+  if (ce == cudaSuccess) ce = cudaMalloc(&ent_d, (size_t)acc * 4);
+  if (ce == cudaSuccess) ce = cudaMemcpyAsync(off_d, offsets, ((size_t)n + 1) * 8, cudaMemcpyHostToDevice, stream_);
+  if (ce == cudaSuccess) {
+    k_e_export_nbr_entries<<<blocks_for(n), kThreads, 0, stream_>>>(
+        (const float4*)pos_[1], start_, sc_d_, q, orig_, nbr_, nbr_n_, nbr_cap_, (uint32_t)slot_cap_, off_d, ent_d);
+    ce = cudaGetLastError();
+  }
+  if (ce == cudaSuccess) ce = cudaMemcpyAsync(entries, ent_d, (size_t)acc * 4, cudaMemcpyDeviceToHost, stream_);
+  if (ce == cudaSuccess) ce = cudaStreamSynchronize(stream_);
+  cudaFree(off_d);
+  cudaFree(ent_d);
+  if (ce != cudaSuccess) return set_error(VXL_CUDA_ERROR, std::string("neighbour export: ") + cudaGetErrorString(ce));
+  return VXL_OK;
+}
+
 vxl_status Engine::bounds(uint32_t q, float lo[3], float hi[3]) {
   if (q >= scenes_.size()) return set_error(VXL_INVALID_ARGUMENT, "scene index out of range");
   CU(cudaSetDevice(device_));
@@ -1192,7 +1398,10 @@ void Engine::enqueue_substep(bool with_reactions) {
   LAUNCH(KID_CANON, k_e_canon<<<148 * 8, 256, 0, st>>>((const uint2*)items_, start_, ctl_d_, p0, v0, (float4*)pos_[1],
                                                        (float4*)vel_[1], orig_, slot_of_));
   LAUNCH(KID_HALFMASK, k_e_halfmask<<<key_blocks, kThreads, 0, st>>>(p1, sc_d_, tiles_d_, ntiles_, ctl_d_, halves_));
-  LAUNCH(KID_HALFMASK, k_e_xorder<<<148 * 8, kThreads, 0, st>>>(start_, ctl_d_, halves_, xorder_));
+  if (walls_any_) LAUNCH(KID_HALFMASK, k_e_xorder<<<148 * 8, kThreads, 0, st>>>(start_, ctl_d_, halves_, xorder_));
+  else
+    LAUNCH(KID_GROUPS, k_e_groups<<<key_blocks, 256, 0, st>>>(p1, sc_d_, tiles_d_, ntiles_, ctl_d_, order_,
+                                                              (uint2*)segs_));
   const uint32_t stride = (uint32_t)slot_cap_;
   const bool rec = record_;
   const uint32_t per_tile = std::max<uint32_t>(ntiles_, 1);
@@ -1203,19 +1412,15 @@ void Engine::enqueue_substep(bool with_reactions) {
     if (tuning_.block == 128)
       LAUNCH(KID_DENSITY, k_e_density<128, true><<<gd, 128, 0, st>>>(
                               p1, start_, sc_d_, tiles_d_, ntiles_, ctl_d_, halves_, (float2*)rc_, press_, nbr_, nbr_n_,
-                              nbr_cap_, stride, wet_, xorder_, prov_d_, wplanes_d_));
+                              nbr_cap_, stride, wet_, xorder_, prov_d_, wplanes_d_, orig_, ctab(0)));
     else
       LAUNCH(KID_DENSITY, k_e_density<256, true><<<gd, 256, 0, st>>>(
                               p1, start_, sc_d_, tiles_d_, ntiles_, ctl_d_, halves_, (float2*)rc_, press_, nbr_, nbr_n_,
-                              nbr_cap_, stride, wet_, xorder_, prov_d_, wplanes_d_));
-  } else if (tuning_.block == 128) {
-    LAUNCH(KID_DENSITY, k_e_density<128><<<gd, 128, 0, st>>>(p1, start_, sc_d_, tiles_d_, ntiles_, ctl_d_, halves_,
-                                                             (float2*)rc_, press_, nbr_, nbr_n_, nbr_cap_, stride, wet_,
-                                                             xorder_));
+                              nbr_cap_, stride, wet_, xorder_, prov_d_, wplanes_d_, orig_, ctab(0)));
   } else {
-    LAUNCH(KID_DENSITY, k_e_density<256><<<gd, 256, 0, st>>>(p1, start_, sc_d_, tiles_d_, ntiles_, ctl_d_, halves_,
-                                                             (float2*)rc_, press_, nbr_, nbr_n_, nbr_cap_, stride, wet_,
-                                                             xorder_));
+    LAUNCH(KID_DENSITY, k_e_density_seg<kSegWarps><<<grid_seg_, kSegWarps * 32, 0, st>>>(
+                            p1, start_, sc_d_, ctl_d_, halves_, order_, (const uint2*)segs_, (float2*)rc_, press_, nbr_,
+                            nbr_n_, nbr_cap_, stride, wet_));
   }
   // Reaction branch on the side stream: it reads only the sorted buffer, the densities and
   // the lists, so it runs beside the force pass (which writes the other buffer).
@@ -1261,7 +1466,7 @@ void Engine::enqueue_substep(bool with_reactions) {
     const uint32_t nblk = std::max<uint32_t>((nref + kPushedChunk - 1) / kPushedChunk, 1);
     LAUNCH(KID_WALLS, k_e_wall_project<<<key_blocks, kThreads, 0, st>>>(
                           (float4*)pos_[0], (float4*)vel_[0], sc_d_, tiles_d_, ntiles_, ctl_d_, prov_d_, wplanes_d_,
-                          orig_, pflag_, (float4*)pnsum_));
+                          orig_, pflag_, (float4*)pnsum_, ctab(1)));
     LAUNCH(KID_WALLS, k_e_pushed_count<<<nblk, kThreads, 0, st>>>(pflag_, nref, ctl_d_, pblk_));
     LAUNCH(KID_WALLS, k_e_pushed_emit<<<nblk, kThreads, 0, st>>>(pflag_, nref, pblk_, ctl_d_, plist_));
     LAUNCH(KID_WALLS, k_e_separate_check<<<148 * 2, kThreads, 0, st>>>((const float4*)pos_[0], sc_d_, plist_,

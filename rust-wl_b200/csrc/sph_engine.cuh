@@ -38,6 +38,9 @@
 #ifndef VXL_FORCE_THREADS_PER_SM
 #define VXL_FORCE_THREADS_PER_SM 1280
 #endif
+#ifndef VXL_DENSITY_SEG_THREADS_PER_SM
+#define VXL_DENSITY_SEG_THREADS_PER_SM 1536
+#endif
 
 
 namespace vxl {
@@ -119,7 +122,7 @@ struct EngineCtl {
 // closer than 0.2 h", "the separation moved a particle".
 enum WorkId : int {
   kWorkDensity = 0, kWorkForce = 1, kWorkBforce = 2, kWorkScan = 3,
-  kWorkPushed = 4, kWorkTrigger = 5, kWorkMoved = 6
+  kWorkPushed = 4, kWorkTrigger = 5, kWorkMoved = 6, kWorkSegs = 7
 };
 
 // Provider walls (analytic ProviderColliders queried on the device). A plane of a FACES
@@ -131,6 +134,15 @@ struct WallPlaneDev {
   uint32_t pad0, pad1;
 };
 
+// One side (mirror or projection) of the contact tables: ent[global reference index] =
+// entry + 1 (0: no planes), entry e owning planes [start[e], start[e + 1]), each plane two
+// float4 (contact point, outward normal).
+struct ContactTableDev {
+  const uint32_t* ent;
+  const uint32_t* start;
+  const float4* planes;
+};
+
 struct ProviderDev {
   uint32_t kind, first, count, has_bounds;
   float bminx, bminy, bminz, bmaxx, bmaxy, bmaxz;
@@ -138,6 +150,10 @@ struct ProviderDev {
 };
 
 constexpr uint32_t kProviderFaces = 0u, kProviderConvex = 1u;
+// A contact table (any ProviderColliders, gathered on the host once per tick, as the
+// reference's GPU tier does: crates/vxl-phys-gpu/src/pipeline/walls.rs:143-215) is one more
+// provider of the scene, after its analytic ones, queried by particle.
+constexpr uint32_t kProviderTable = 2u;
 constexpr uint32_t kMaxWallPlanes = 8;     // mirror planes per particle (fluid_density.rs:110)
 constexpr uint32_t kPushedChunk = 4096;    // reference indices per block of the pushed-list passes
 
@@ -954,6 +970,329 @@ __device__ __forceinline__ void walk27_half(const GridBox& g, const uint32_t* __
   }
 }
 
+// ---------------------------------------------------------------- grouped density walk
+//
+// Particles of one cell reach the same neighbour cells; when the cell budget has doubled
+// the bins to 2h or more, particles of one octant of a cell (the same half along x, y and
+// z) also reach the same half-cells. The grouped density pass lets eight lanes of a warp
+// share one stream of candidates: k_e_groups orders each 256-slot chunk of a tile by
+// octant (a stable counting sort, so the slots of an octant stay ascending) into
+// order[], then cuts the runs of equal (cell, octant) into segments of at most
+// kSegLanes positions, appended to segs[] as (first position in order[], count |
+// scene << 4); ctl->work[kWorkSegs] counts them. The order of segments in segs[] is
+// immaterial: each particle's sums are formed by one lane alone.
+
+constexpr uint32_t kSegLanes = 8;   // lanes (particles) per segment; four segments per warp
+constexpr uint32_t kSegQueue = 64;  // candidate ring per segment (pending never exceeds 7 + 32)
+
+__global__ void __launch_bounds__(256) k_e_groups(const float4* __restrict__ pos, const SceneDev* __restrict__ sc,
+                                                  const TileDev* __restrict__ tiles, uint32_t ntiles, EngineCtl* ctl,
+                                                  uint32_t* __restrict__ order, uint2* __restrict__ segs) {
+  if (ctl->err & kErrCellCap) return;
+  __shared__ uint32_t s_cnt[8][8];  // [octant][warp]: slots per octant in each warp
+  __shared__ uint32_t s_cell[256], s_oct[256];
+  __shared__ uint32_t s_last[8], s_nseg[8], s_segbase;
+  const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const uint32_t lt = (1u << lane) - 1u;
+  for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const TileDev td = tiles[t];
+    const GridBox g = sc[td.scene].g;
+    const bool half = g.bin >= 2.0f * sc[td.scene].k.h;
+    const float hb = g.bin * 0.5f;
+    for (uint32_t c0 = 0; c0 < td.count; c0 += 256) {
+      const uint32_t n = min(256u, td.count - c0);
+      const uint32_t i = threadIdx.x;
+      const bool valid = i < n;
+      uint32_t cell = 0, oct = 0;
+      if (valid) {
+        const float4 p = pos[td.first + c0 + i];
+        uint32_t cx, cy, cz;
+        bin_of(g, p.x, p.y, p.z, cx, cy, cz);
+        cell = (cx * g.ny + cy) * g.nz + cz;
+        if (half)
+          oct = (p.x >= g.minx + (float)cx * g.bin + hb ? 1u : 0u) | (p.y >= g.miny + (float)cy * g.bin + hb ? 2u : 0u) |
+                (p.z >= g.minz + (float)cz * g.bin + hb ? 4u : 0u);
+      }
+      uint32_t rank = 0;
+#pragma unroll
+      for (uint32_t o = 0; o < 8; ++o) {
+        const uint32_t b = __ballot_sync(0xffffffffu, valid && oct == o);
+        if (lane == 0) s_cnt[o][w] = __popc(b);
+        if (valid && oct == o) rank = __popc(b & lt);
+      }
+      __syncthreads();
+      if (w == 0) {  // exclusive scan of the 64 counts in (octant, warp) order
+        const uint32_t a = s_cnt[lane >> 2][(lane & 3) * 2], b = s_cnt[lane >> 2][(lane & 3) * 2 + 1];
+        uint32_t v = a + b;
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+          const uint32_t u = __shfl_up_sync(0xffffffffu, v, off);
+          if ((int)lane >= off) v += u;
+        }
+        const uint32_t ex = v - a - b;
+        s_cnt[lane >> 2][(lane & 3) * 2] = ex;
+        s_cnt[lane >> 2][(lane & 3) * 2 + 1] = ex + a;
+      }
+      __syncthreads();
+      if (valid) {
+        const uint32_t q = s_cnt[oct][w] + rank;
+        order[td.first + c0 + q] = td.first + c0 + i;
+        s_cell[q] = cell;
+        s_oct[q] = oct;
+      }
+      __syncthreads();
+      // runs of equal (cell, octant) in the new order, cut into segments of kSegLanes
+      const bool head = valid && (i == 0 || s_cell[i] != s_cell[i - 1] || s_oct[i] != s_oct[i - 1]);
+      const uint32_t hbal = __ballot_sync(0xffffffffu, head);
+      if (lane == 0) s_last[w] = hbal ? w * 32 + 31 - __clz(hbal) : 0xffffffffu;
+      __syncthreads();
+      uint32_t run0 = 0;
+      const uint32_t le = hbal & (0xffffffffu >> (31 - lane));
+      if (le) {
+        run0 = w * 32 + 31 - __clz(le);
+      } else {
+        for (int k = (int)w - 1; k >= 0; --k)
+          if (s_last[k] != 0xffffffffu) {
+            run0 = s_last[k];
+            break;
+          }
+      }
+      const bool shead = valid && ((i - run0) % kSegLanes == 0u);
+      uint32_t cnt = 0;
+      if (shead) {
+        cnt = 1;
+        while (cnt < kSegLanes && i + cnt < n && s_cell[i + cnt] == s_cell[i] && s_oct[i + cnt] == s_oct[i]) ++cnt;
+      }
+      const uint32_t sb = __ballot_sync(0xffffffffu, shead);
+      if (lane == 0) s_nseg[w] = __popc(sb);
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        uint32_t tot = 0;
+        for (int k = 0; k < 8; ++k) {
+          const uint32_t v = s_nseg[k];
+          s_nseg[k] = tot;
+          tot += v;
+        }
+        s_segbase = atomicAdd(&ctl->work[kWorkSegs], tot);
+      }
+      __syncthreads();
+      if (shead) segs[s_segbase + s_nseg[w] + __popc(sb & lt)] = make_uint2(td.first + c0 + i, cnt | (td.scene << 4));
+      __syncthreads();
+    }
+  }
+}
+
+// Density (poly6 with self term) + Tait EOS over the segments of k_e_groups: the same
+// sums as k_e_density (crates/vxl-phys-fluid/src/fluid_density.rs:17-70) for scenes
+// without provider walls. Lanes 8k..8k+7 of a warp hold the particles of one segment,
+// which share their cell. The segment's cells are the union of its lanes' culled 27-cell
+// sets (and, at 2h bins, of their reachable half-cells) — for each lane a superset of its
+// own walk that adds only particles farther than h — taken in the reference's (dz, dy, dx)
+// order and, inside a cell, in ascending slot order (crates/vxl-phys-fluid/src/grid.rs:
+// 115-155). The segment's eight lanes append the candidate slots to a ring in shared
+// memory (each lane four bits of a 32-slot window), load eight of them at a time into a
+// staging row, and every lane then tests its own particle against the row in order, so
+// each lane accepts exactly its walk's neighbours in its walk's order: the sums, the EOS
+// and the recorded neighbour list are those of k_e_density, bit for bit. Segments of one
+// warp advance in lock step, eight candidates per round.
+template <int kWarps>
+__global__ void __launch_bounds__(kWarps * 32, VXL_DENSITY_SEG_THREADS_PER_SM / (kWarps * 32)) k_e_density_seg(
+    const float4* __restrict__ pos, const uint32_t* __restrict__ start, const SceneDev* __restrict__ sc,
+    const EngineCtl* __restrict__ ctl, const uint32_t* __restrict__ halves, const uint32_t* __restrict__ order,
+    const uint2* __restrict__ segs, float2* __restrict__ rc, float* __restrict__ press_out, uint32_t* __restrict__ nbr,
+    uint32_t* __restrict__ nbr_n, uint32_t cap, uint32_t stride, const uint32_t* __restrict__ wet) {
+  if (ctl->err & kErrCellCap) return;
+  __shared__ uint32_t s_queue[kWarps][4][kSegQueue];
+  __shared__ float4 s_pos[kWarps][4 * (kSegLanes + 1)];  // rows padded by one: segments hit different banks
+  __shared__ uint32_t s_j[kWarps][4 * (kSegLanes + 1)];
+  const uint32_t nseg = ctl->work[kWorkSegs];
+  const uint32_t epoch = ctl->epoch;
+  const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const uint32_t seg = lane >> 3, sl = lane & 7u;
+  uint32_t* queue = s_queue[w][seg];
+  float4* stp = &s_pos[w][seg * (kSegLanes + 1)];
+  uint32_t* stj = &s_j[w][seg * (kSegLanes + 1)];
+  const uint32_t nwarps = gridDim.x * kWarps;
+  for (uint32_t g0 = (blockIdx.x * kWarps + w) * 4; g0 < nseg; g0 += nwarps * 4) {
+    const uint32_t sid = g0 + seg;
+    const uint2 rec = sid < nseg ? segs[sid] : make_uint2(0u, 0u);
+    const uint32_t nseg_lanes = rec.y & 15u;
+    const bool act = sl < nseg_lanes;
+    const SceneDev& S = sc[rec.y >> 4];
+    const GridBox g = S.g;
+    const float h = S.k.h, h2 = S.k.h2, k6 = S.k.k6;
+    const bool half = halves != nullptr && g.bin >= 2.0f * h;
+    uint32_t s = 0;
+    float4 pi = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    uint32_t cx = 0, cy = 0, cz = 0;
+    if (act) {
+      s = order[rec.x + sl];
+      pi = pos[s];
+      bin_of(g, pi.x, pi.y, pi.z, cx, cy, cz);
+    }
+    const bool fluid_i = pi.w > 0.0f;
+    // this lane's cells: in the grid and not farther than h (conservatively, as walk27),
+    // and at 2h bins with some reachable half along every axis (as walk27_half)
+    uint32_t cm = 0, bxs = 0, bys = 0, bzs = 0;
+    if (act) {
+      const float lx = g.minx + (float)cx * g.bin, ly = g.miny + (float)cy * g.bin, lz = g.minz + (float)cz * g.bin;
+      const float gxl = fmaxf(pi.x - lx, 0.0f), gxr = fmaxf(lx + g.bin - pi.x, 0.0f);
+      const float gyl = fmaxf(pi.y - ly, 0.0f), gyr = fmaxf(ly + g.bin - pi.y, 0.0f);
+      const float gzl = fmaxf(pi.z - lz, 0.0f), gzr = fmaxf(lz + g.bin - pi.z, 0.0f);
+      const float reach = h + g.bin * (1.0f / 1024.0f);
+      const float reach2 = reach * reach;
+      if (half) {
+        bxs = half_reach_bits(pi.x, lx, g.bin, reach, cx + 1 == g.nx);
+        bys = half_reach_bits(pi.y, ly, g.bin, reach, cy + 1 == g.ny);
+        bzs = half_reach_bits(pi.z, lz, g.bin, reach, cz + 1 == g.nz);
+      } else {
+        bxs = bys = bzs = 63u;
+      }
+#pragma unroll
+      for (int dz = -1; dz <= 1; ++dz) {
+        const bool zok = (dz < 0 ? cz > 0 : (dz > 0 ? cz + 1 < g.nz : true)) && ((bzs >> (2 * (dz + 1))) & 3u);
+        const float gz = dz < 0 ? gzl : (dz > 0 ? gzr : 0.0f);
+        const float dz2 = gz * gz;
+#pragma unroll
+        for (int dy = -1; dy <= 1; ++dy) {
+          const bool yok = (dy < 0 ? cy > 0 : (dy > 0 ? cy + 1 < g.ny : true)) && ((bys >> (2 * (dy + 1))) & 3u);
+          const float gy = dy < 0 ? gyl : (dy > 0 ? gyr : 0.0f);
+          const float dyz2 = dz2 + gy * gy;
+#pragma unroll
+          for (int dx = -1; dx <= 1; ++dx) {
+            const bool xok = (dx < 0 ? cx > 0 : (dx > 0 ? cx + 1 < g.nx : true)) && ((bxs >> (2 * (dx + 1))) & 3u);
+            const float gx = dx < 0 ? gxl : (dx > 0 ? gxr : 0.0f);
+            if (zok && yok && xok && !(dyz2 + gx * gx > reach2)) cm |= 1u << ((dz + 1) * 9 + (dy + 1) * 3 + (dx + 1));
+          }
+        }
+      }
+    }
+    // A segment of boundary particles only sums fluid neighbours: with no fluid in its
+    // cell's 27 cells (none marked wet this substep) it has nothing to walk. The segment's
+    // lanes share the cell, so they test the 27 cells together.
+    const uint32_t seg_mask = 0xffu << (8 * seg);
+    const bool seg_fluid = (__ballot_sync(0xffffffffu, act && fluid_i) & seg_mask) != 0u;
+    const uint32_t lead = seg * 8;
+    const uint32_t ccx = __shfl_sync(0xffffffffu, cx, lead), ccy = __shfl_sync(0xffffffffu, cy, lead),
+                   ccz = __shfl_sync(0xffffffffu, cz, lead);
+    bool wet_seen = seg_fluid;
+    if (!seg_fluid && nseg_lanes) {
+      const uint32_t* wc = wet + S.cell_off;
+      for (uint32_t d = sl; d < 27u; d += 8u) {
+        const int dz = (int)(d / 9) - 1, dy = (int)((d / 3) % 3) - 1, dx = (int)(d % 3) - 1;
+        const int x = (int)ccx + dx, y = (int)ccy + dy, z = (int)ccz + dz;
+        if (x >= 0 && x < (int)g.nx && y >= 0 && y < (int)g.ny && z >= 0 && z < (int)g.nz &&
+            wc[((uint32_t)x * g.ny + (uint32_t)y) * g.nz + (uint32_t)z] == epoch)
+          wet_seen = true;
+      }
+    }
+    const bool seg_wet = (__ballot_sync(0xffffffffu, wet_seen) & seg_mask) != 0u;
+    if (!seg_wet) cm = 0;
+#pragma unroll
+    for (uint32_t o = 1; o < 8; o <<= 1) {
+      cm |= __shfl_xor_sync(0xffffffffu, cm, o);
+      bxs |= __shfl_xor_sync(0xffffffffu, bxs, o);
+      bys |= __shfl_xor_sync(0xffffffffu, bys, o);
+      bzs |= __shfl_xor_sync(0xffffffffu, bzs, o);
+    }
+    const uint32_t nz = g.nz, nyz = g.ny * g.nz;
+    const uint32_t centre = (ccx * g.ny + ccy) * g.nz + ccz;
+    const uint32_t* cst = start + S.cell_off;
+    float sum = fluid_i ? S.k.w0 : 0.0f;
+    float sum_b = 0.0f;
+    uint32_t cnt = 0;
+    uint32_t* wp = nbr + s;  // next list entry: nbr[cnt * stride + s]
+    // segment walk state (equal on the segment's lanes)
+    uint32_t ucm = cm, blk = 0, jb = 0, je = 0, xs = 3, ys = 3, zs = 3, qh = 0, qt = 0;
+    for (;;) {
+      while (qt - qh < kSegLanes) {
+        if (blk >= je) {
+          if (!ucm) break;
+          const uint32_t d = __ffs(ucm) - 1;
+          ucm &= ucm - 1u;
+          const uint32_t dzp = d / 9, dyp = (d / 3) % 3, dxp = d % 3;
+          const uint32_t idx = centre + dxp * nyz + dyp * nz + dzp - (nyz + nz + 1u);
+          jb = cst[idx];
+          je = cst[idx + 1];
+          blk = half ? (jb & ~31u) : jb;
+          xs = (bxs >> (2 * dxp)) & 3u;
+          ys = (bys >> (2 * dyp)) & 3u;
+          zs = (bzs >> (2 * dzp)) & 3u;
+          continue;
+        }
+        uint32_t m;
+        if (half) {
+          const uint4 hm = *reinterpret_cast<const uint4*>(halves + 4 * (blk >> 5));
+          m = half_select(xs, hm.x) & half_select(ys, hm.y) & half_select(zs, hm.z);
+          if (jb > blk) m &= ~0u << (jb - blk);
+          if (je < blk + 32u) m &= (1u << (je - blk)) - 1u;
+        } else {
+          const uint32_t left = je - blk;
+          m = left >= 32u ? ~0u : (1u << left) - 1u;
+        }
+        const uint32_t nib = (m >> (4 * sl)) & 15u;
+        uint32_t at = qt + __popc(m & ((1u << (4 * sl)) - 1u));
+        const uint32_t j4 = blk + 4 * sl;
+        if (nib & 1u) queue[(at++) & (kSegQueue - 1)] = j4;
+        if (nib & 2u) queue[(at++) & (kSegQueue - 1)] = j4 + 1;
+        if (nib & 4u) queue[(at++) & (kSegQueue - 1)] = j4 + 2;
+        if (nib & 8u) queue[at & (kSegQueue - 1)] = j4 + 3;
+        qt += __popc(m);
+        blk += 32u;
+      }
+      const uint32_t nc = min(qt - qh, kSegLanes);
+      if (!__any_sync(0xffffffffu, nc != 0u)) break;
+      __syncwarp();
+      if (sl < nc) {
+        const uint32_t j = queue[(qh + sl) & (kSegQueue - 1)];
+        stj[sl] = j;
+        stp[sl] = pos[j];
+      }
+      __syncwarp();
+#pragma unroll
+      for (uint32_t c = 0; c < kSegLanes; ++c) {
+        if (c < nc) {
+          const uint32_t j = stj[c];
+          const float4 pj = stp[c];
+          if (act && j != s) {
+            const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
+            const float r2 = dx * dx + dy * dy + dz * dz;
+            if (r2 <= h2) {
+              const float tt = h2 - r2;
+              const float wv = k6 * tt * tt * tt;
+              bool keep = true;
+              if (fluid_i) {
+                if (pj.w > 0.0f) sum += wv;
+                else sum_b += (-pj.w) * wv;
+              } else if (pj.w > 0.0f) {
+                sum += pj.w * wv;
+              } else {
+                keep = false;
+              }
+              if (keep) {
+                if (cnt < cap) {
+                  __stcs(wp, j);  // streaming store: the list is read once, by the force pass
+                  wp += stride;
+                }
+                ++cnt;
+              }
+            }
+          }
+        }
+      }
+      qh += nc;
+      __syncwarp();
+    }
+    if (act) {
+      nbr_n[s] = cnt;
+      const float rho = fluid_i ? (S.k.mass * sum + sum_b) : ((-pi.w) * S.k.w0 + sum);
+      const float p = tait(S.k, rho);
+      rc[s] = make_float2(rho, p / (rho * rho));
+      if (press_out) press_out[s] = p;
+    }
+  }
+}
+
 // ---------------------------------------------------------------- provider walls
 // ProviderColliders::bounds prefilter of the fluid passes: skip the provider when p lies
 // outside its bounds expanded by m (fluid_density.rs:90-101, fluid_boundary.rs:60-71).
@@ -967,9 +1306,20 @@ __device__ __forceinline__ bool provider_outside(const ProviderDev& pr, float x,
 // 2 probe, at p with that coordinate set to the plane (crates/vxl-phys-fluid/src/tests.rs:
 // 81-110). CONVEX: the decisive plane (largest n.p - d) when -(n.p - d) >= -probe, at
 // p - n (n.p - d) (crates/vxl-phys-terrain/src/plane_set.rs:60-76, 166-181).
+// TABLE: the particle's planes of the table side in use, in their table order.
 template <class F>
 __device__ __forceinline__ void provider_contacts(const ProviderDev& pr, const WallPlaneDev* __restrict__ pl,
-                                                  float px, float py, float pz, float probe, F&& emit) {
+                                                  const ContactTableDev& ct, uint32_t gref, float px, float py,
+                                                  float pz, float probe, F&& emit) {
+  if (pr.kind == kProviderTable) {
+    const uint32_t e = ct.ent ? ct.ent[gref] : 0u;
+    if (!e) return;
+    for (uint32_t k = ct.start[e - 1], k1 = ct.start[e]; k < k1; ++k) {
+      const float4 a = ct.planes[2 * k], n = ct.planes[2 * k + 1];
+      emit(a.x, a.y, a.z, n.x, n.y, n.z);
+    }
+    return;
+  }
   if (pr.kind == kProviderFaces) {
     for (uint32_t k = pr.first; k < pr.first + pr.count; ++k) {
       const WallPlaneDev f = pl[k];
@@ -1027,7 +1377,8 @@ __global__ void __launch_bounds__(kBlock, VXL_DENSITY_THREADS_PER_SM / kBlock) k
     float2* __restrict__ rc, float* __restrict__ press_out, uint32_t* __restrict__ nbr,
     uint32_t* __restrict__ nbr_n, uint32_t cap, uint32_t stride, const uint32_t* __restrict__ wet,
     const uint32_t* __restrict__ xorder, const ProviderDev* __restrict__ prov = nullptr,
-    const WallPlaneDev* __restrict__ wplanes = nullptr) {
+    const WallPlaneDev* __restrict__ wplanes = nullptr, const uint32_t* __restrict__ orig = nullptr,
+    ContactTableDev ctm = ContactTableDev{nullptr, nullptr, nullptr}) {
   if (ctl->err & kErrCellCap) return;
   for (uint32_t t = first_tile(&ctl->work[kWorkDensity], ntiles); t < ntiles; t = following_tile(&ctl->work[kWorkDensity], ntiles)) {
     const TileDev td = tiles[t];
@@ -1054,7 +1405,7 @@ __global__ void __launch_bounds__(kBlock, VXL_DENSITY_THREADS_PER_SM / kBlock) k
         for (uint32_t q = S.prov_first; q < S.prov_first + S.prov_count; ++q) {
           const ProviderDev pr = prov[q];
           if (provider_outside(pr, pi.x, pi.y, pi.z, h)) continue;
-          provider_contacts(pr, wplanes, pi.x, pi.y, pi.z, h,
+          provider_contacts(pr, wplanes, ctm, orig ? orig[s] : 0u, pi.x, pi.y, pi.z, h,
                             [&](float cx_, float cy_, float cz_, float nx_, float ny_, float nz_) {
                               const float sdf = (pi.x - cx_) * nx_ + (pi.y - cy_) * ny_ + (pi.z - cz_) * nz_;
                               if (sdf > 0.0f && sdf < h && np < kMaxWallPlanes) {
@@ -1286,7 +1637,7 @@ __global__ void k_e_wall_project(float4* __restrict__ pos, float4* __restrict__ 
                                  const TileDev* __restrict__ tiles, uint32_t ntiles, const EngineCtl* __restrict__ ctl,
                                  const ProviderDev* __restrict__ prov, const WallPlaneDev* __restrict__ wplanes,
                                  const uint32_t* __restrict__ orig, uint32_t* __restrict__ pflag,
-                                 float4* __restrict__ pnsum) {
+                                 float4* __restrict__ pnsum, ContactTableDev ctp) {
   if (ctl->err & kErrCellCap) return;
   for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
     const TileDev td = tiles[t];
@@ -1312,7 +1663,7 @@ __global__ void k_e_wall_project(float4* __restrict__ pos, float4* __restrict__ 
           for (uint32_t q = S.prov_first; q < S.prov_first + S.prov_count; ++q) {
             const ProviderDev pr = prov[q];
             if (provider_outside(pr, p.x, p.y, p.z, h)) continue;
-            provider_contacts(pr, wplanes, p.x, p.y, p.z, skin,
+            provider_contacts(pr, wplanes, ctp, orig[sl], p.x, p.y, p.z, skin,
                               [&](float cx, float cy, float cz, float nx, float ny, float nz) {
                                 const float sdf = (p.x - cx) * nx + (p.y - cy) * ny + (p.z - cz) * nz;
                                 const float pen = -sdf;
@@ -1917,6 +2268,54 @@ __global__ void k_e_export_bins(const uint32_t* __restrict__ start, const uint32
 }
 
 // One scene's slice of the cell table, rebased to the scene's first slot.
+// Contact table entries by global reference index: ent[ids[e]] = e + 1 (ent zeroed before).
+__global__ void k_e_ctab_scatter(const uint32_t* __restrict__ ids, uint32_t n, uint32_t* __restrict__ ent) {
+  const uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e < n) ent[ids[e]] = e + 1u;
+}
+
+// Neighbour-list export of one scene (last substep): the list count of each slot in the
+// scene's reference order.
+__global__ void k_e_export_nbr_counts(const uint32_t* __restrict__ nbr_n, const uint32_t* __restrict__ orig,
+                                      uint32_t base, uint32_t n, uint32_t* __restrict__ out) {
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < n) out[orig[base + t] - base] = nbr_n[base + t];
+}
+
+// The entries of each slot's list, in its walk order, as scene-local reference indices,
+// at offsets[reference index]: the recorded list, or for a list longer than the cap the
+// same neighbours walked again from the sorted positions and cell table of that substep
+// (the walk the force pass and the boundary gather fall back to).
+__global__ void k_e_export_nbr_entries(const float4* __restrict__ pos, const uint32_t* __restrict__ start,
+                                       const SceneDev* __restrict__ sc, uint32_t q, const uint32_t* __restrict__ orig,
+                                       const uint32_t* __restrict__ nbr, const uint32_t* __restrict__ nbr_n,
+                                       uint32_t cap, uint32_t stride, const unsigned long long* __restrict__ offsets,
+                                       uint32_t* __restrict__ out) {
+  const SceneDev& S = sc[q];
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= S.count) return;
+  const uint32_t s = S.base + t;
+  const uint32_t base = S.base;
+  unsigned long long o = offsets[orig[s] - base];
+  const uint32_t c = nbr_n[s];
+  if (c <= cap) {
+    for (uint32_t k = 0; k < c; ++k) out[o + k] = orig[nbr[(size_t)k * stride + s]] - base;
+    return;
+  }
+  const GridBox g = S.g;
+  const float4 pi = pos[s];
+  const bool fluid_i = pi.w > 0.0f;
+  const float h2 = S.k.h2;
+  uint32_t cx, cy, cz;
+  bin_of(g, pi.x, pi.y, pi.z, cx, cy, cz);
+  walk27<true>(g, start + S.cell_off, pi.x, pi.y, pi.z, cx, cy, cz, S.k.h, [&](uint32_t j) {
+    const float4 pj = pos[j];
+    const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
+    const float r2 = dx * dx + dy * dy + dz * dz;
+    if (r2 <= h2 && (fluid_i || pj.w > 0.0f)) out[o++] = orig[j] - base;
+  }, s);
+}
+
 __global__ void k_e_export_items(const uint32_t* __restrict__ orig, uint32_t base, uint32_t n,
                                  uint32_t* __restrict__ out) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;

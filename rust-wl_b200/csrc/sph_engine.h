@@ -24,6 +24,7 @@ struct SpanChunk;
 struct BodyPoseDev;
 struct RigidBodyDev;
 struct ProviderDev;
+struct ContactTableDev;
 struct WallPlaneDev;
 
 // Launch shape of the particle passes (chosen by the autotuner for batches).
@@ -83,6 +84,8 @@ class Engine {
   vxl_status read_rigid_bodies(uint32_t scene, vxl_sph_rigid_body* out, uint32_t n);
   // Provider walls of a scene (analytic ProviderColliders queried on the device every
   // substep: mirror ghosts in the density, projection and separation after integration).
+  vxl_status set_wall_contacts(uint32_t scene, uint32_t side, const uint32_t* ids, const uint32_t* start,
+                               uint32_t n_entries, const float* planes, uint32_t n_planes);
   vxl_status set_providers(uint32_t scene, const vxl_sph_provider* providers, uint32_t n,
                            const vxl_sph_wall_plane* planes, uint32_t nplanes);
   vxl_status write_state(uint32_t scene, const float* pos, const float* vel);
@@ -92,6 +95,8 @@ class Engine {
   vxl_status request_state();
   vxl_status take_state(float* pos, uint64_t n);
   vxl_status read_fields(uint32_t scene, float* dens, float* press, float* acc, float* xsph, float* bforce);
+  vxl_status export_neighbors(uint32_t scene, uint64_t* offsets, uint64_t offsets_len, uint32_t* entries,
+                              uint64_t entries_cap, uint64_t* total);
   vxl_status export_grid(uint32_t scene, uint32_t* items, uint32_t* start, uint64_t start_cap, uint32_t* bins,
                          vxl_sph_grid_info* info);
   vxl_status bounds(uint32_t scene, float lo[3], float hi[3]);
@@ -169,7 +174,9 @@ class Engine {
   uint32_t* nbr_ = nullptr;
   uint32_t* nbr_n_ = nullptr;
   uint32_t* halves_ = nullptr;  // 4 words per 32 slots: upper-half masks along x, y, z
-  uint32_t* xorder_ = nullptr;  // density thread order at doubled bins (lower x halves first)
+  uint32_t* xorder_ = nullptr;  // density order of the provider-wall variant at doubled bins (lower x halves first)
+  uint32_t* order_ = nullptr;   // grouped density pass: slots of each chunk ordered by octant
+  void* segs_ = nullptr;        // grouped density pass: segments (first position, count | scene << 4)
   float4* blocal_ = nullptr;         // body-frame lattice per boundary slot (reference order), lazily
   BodyPoseDev* poses_d_ = nullptr;   // poses of one scene's bodies (staged per call)
   uint32_t poses_cap_ = 0;
@@ -195,6 +202,20 @@ class Engine {
   std::vector<uint32_t> prov_first_st_, prov_count_st_;  // per scene, as staged on the device
   bool walls_any_ = false;      // some scene has providers (selects the walls kernels)
   vxl_status stage_walls();
+  // contact tables (any ProviderColliders, gathered by the caller once per tick): per side
+  // (0 mirror, 1 projection) and scene, the entries' scene-local fluid ids, their plane
+  // offsets and the planes (point xyz, normal xyz); on the device, all scenes' tables
+  // concatenated with global reference ids
+  std::vector<std::vector<uint32_t>> ct_ids_h_[2], ct_start_h_[2];
+  std::vector<std::vector<float>> ct_pl_h_[2];
+  uint32_t* ct_ent_d_[2] = {nullptr, nullptr};  // per global reference index: entry + 1, 0 = none
+  uint32_t* ct_ids_d_[2] = {nullptr, nullptr};
+  uint32_t* ct_start_d_[2] = {nullptr, nullptr};
+  float4* ct_pl_d_[2] = {nullptr, nullptr};
+  uint64_t ct_ids_cap_[2] = {0, 0}, ct_pl_cap_[2] = {0, 0};
+  bool scene_has_table(uint32_t q) const;
+  vxl_status upload_tables();
+  ContactTableDev ctab(int side) const;
   float* snap_h_ = nullptr;  // pinned, 3 floats per slot
   uint64_t snap_cap_ = 0, snap_n_ = 0;
   cudaEvent_t ev_snap_ = nullptr;
@@ -233,6 +254,7 @@ class Engine {
   bool use_graph_ = true;
   Tuning tuning_;
   int grid_density_ = 0, grid_force_ = 0, grid_bforce_ = 0;
+  int grid_seg_ = 148;  // persistent grid of the grouped density pass (SMs x resident blocks)
   // graph of one tick
   cudaGraphExec_t graph_ = nullptr;
   uint32_t graph_epoch_ = 0;

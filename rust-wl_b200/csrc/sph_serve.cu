@@ -59,6 +59,8 @@ struct vxl_sph_server {
   std::map<uint64_t, Request> req;
   std::deque<uint64_t> queue;
   std::vector<uint64_t> active;  // request id of each engine scene, in scene order
+  uint64_t active_fluid = 0;     // fluid particles of the admitted scenes
+  uint64_t batch_cap = 0;        // admission stops at this many fluid particles per substep (0: none)
   uint64_t next_id = 1;
   std::chrono::steady_clock::time_point t0;
 
@@ -143,23 +145,35 @@ vxl_status vxl_sph_serve_step(vxl_sph_server* s, float dt_tick, vxl_sph_serve_re
     return set_error(VXL_SIZE_MISMATCH, "report header");
   cudaSetDevice(s->e->device());
   uint32_t retired = 0, admitted = 0;
-  // 1. retire finished scenes (copy their state out), compact
+  // 1. retire finished scenes (copy their state out), compact. Every finished scene's
+  // state is read first; requests and budget counters change only once all reads and the
+  // compaction have succeeded, so a failed call can be repeated without counting twice.
   std::vector<uint32_t> drop;
+  std::vector<std::vector<float>> out_pos, out_vel;
   for (uint32_t q = 0; q < s->active.size(); ++q) {
-    Request& r = s->req[s->active[q]];
+    const Request& r = s->req[s->active[q]];
     if (r.ticks_done >= r.ticks_total) {
-      vxl_status st = s->e->read_state(q, r.pos.data(), r.vel.data());
+      out_pos.emplace_back((size_t)3 * (r.nf + r.nb));
+      out_vel.emplace_back((size_t)3 * (r.nf + r.nb));
+      vxl_status st = s->e->read_state(q, out_pos.back().data(), out_vel.back().data());
       if (st != VXL_OK) return st;
-      r.state = kDone;
-      r.done_s = s->now();
-      s->used_slots -= r.nf + r.nb;
-      s->used_cells -= r.cells;
       drop.push_back(q);
     }
   }
   if (!drop.empty()) {
     vxl_status st = s->e->remove_scenes(drop);
     if (st != VXL_OK) return st;
+    const double t = s->now();
+    for (size_t k = 0; k < drop.size(); ++k) {
+      Request& r = s->req[s->active[drop[k]]];
+      r.pos.swap(out_pos[k]);
+      r.vel.swap(out_vel[k]);
+      r.state = kDone;
+      r.done_s = t;
+      s->used_slots -= r.nf + r.nb;
+      s->used_cells -= r.cells;
+      s->active_fluid -= r.nf;
+    }
     std::vector<uint64_t> keep;
     for (uint32_t q = 0; q < s->active.size(); ++q)
       if (std::find(drop.begin(), drop.end(), q) == drop.end()) keep.push_back(s->active[q]);
@@ -170,8 +184,11 @@ vxl_status vxl_sph_serve_step(vxl_sph_server* s, float dt_tick, vxl_sph_serve_re
   for (auto it = s->queue.begin(); it != s->queue.end();) {
     Request& r = s->req[*it];
     const uint64_t nt = r.nf + r.nb;
+    // the batch cap (vxl_sph_serve_set_batch_cap) bounds the fluid particles stepped per
+    // substep; a request larger than the cap is admitted alone
+    const bool under_cap = s->batch_cap == 0 || s->active.empty() || s->active_fluid + r.nf <= s->batch_cap;
     if (s->used_slots + nt <= s->slot_cap && s->used_cells + r.cells <= s->cell_cap &&
-        s->e->scenes().size() < 0xffffffu) {
+        s->e->scenes().size() < 0xffffffu && under_cap) {
       vxl_sph_params p = r.params;
       vxl_status st = s->e->add_scene(p, r.nf, r.nb, r.pos.data(), r.vel.data(), r.pmass.data(), r.id, nullptr);
       if (st == VXL_OUT_OF_MEMORY) {  // scene table full: wait
@@ -188,6 +205,7 @@ vxl_status vxl_sph_serve_step(vxl_sph_server* s, float dt_tick, vxl_sph_serve_re
       r.tick_start_s = r.admit_s;
       s->used_slots += nt;
       s->used_cells += r.cells;
+      s->active_fluid += r.nf;
       s->active.push_back(r.id);
       ++admitted;
       it = s->queue.erase(it);
@@ -225,6 +243,12 @@ vxl_status vxl_sph_serve_step(vxl_sph_server* s, float dt_tick, vxl_sph_serve_re
     rep->particles = particles;
     rep->device_bytes_in_use = s->used_slots * Engine::bytes_per_slot(64) + s->used_cells * Engine::bytes_per_cell();
   }
+  return VXL_OK;
+}
+
+vxl_status vxl_sph_serve_set_batch_cap(vxl_sph_server* s, uint64_t max_fluid_particles) {
+  if (!s) return set_error(VXL_NULL_POINTER, "server is NULL");
+  s->batch_cap = max_fluid_particles;
   return VXL_OK;
 }
 

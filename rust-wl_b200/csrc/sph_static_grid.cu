@@ -30,6 +30,10 @@ constexpr uint32_t kStaticMaxCells = 1u << 19;      // 524,288
 constexpr int kTile = 2048;
 constexpr int kTileThreads = 256;
 constexpr uint32_t kMaxTiles = (kStaticMaxCells + kTile - 1) / kTile;  // 256
+constexpr int kWideThreads = 512;                                          // block of ks_canon_wide
+constexpr uint32_t kWideRank = 2048;  // cells up to this size are ranked in shared memory
+constexpr uint32_t kWideSmemWords = (kStaticMaxParticles + 31) / 32 > kWideRank ? (kStaticMaxParticles + 31) / 32
+                                                                               : kWideRank;  // 64 KB
 
 constexpr size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 constexpr size_t kCountsOff = 0;
@@ -186,7 +190,8 @@ __global__ void ks_place(const uint2* __restrict__ cellrank, const uint32_t* __r
   tmp[start[cr.x] + cr.y] = i;
 }
 
-// One warp per cell: the placed indices of the cell, in ascending order, into items.
+// One warp per cell of at most 32 entries: the placed indices of the cell, in ascending
+// order, into items (each lane ranks its entry against the others).
 __global__ void ks_canon(const uint32_t* __restrict__ tmp, const uint32_t* __restrict__ start,
                          const GridBox* __restrict__ gp, uint32_t* __restrict__ items) {
   const uint32_t total = gp->total;
@@ -194,12 +199,74 @@ __global__ void ks_canon(const uint32_t* __restrict__ tmp, const uint32_t* __res
   const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
   for (uint32_t c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; c < total; c += warps) {
     const uint32_t b = start[c], n = start[c + 1] - b;
-    for (uint32_t e = lane; e < n; e += 32) {
-      const uint32_t key = tmp[b + e];
-      uint32_t rank = 0;
-      for (uint32_t j = 0; j < n; ++j) rank += tmp[b + j] < key ? 1u : 0u;
-      items[b + rank] = key;
+    if (n > 32) continue;  // ks_canon_wide
+    const uint32_t key = lane < (int)n ? tmp[b + lane] : 0xffffffffu;
+    uint32_t rank = 0;
+    for (uint32_t j = 0; j < n; ++j) rank += __shfl_sync(0xffffffffu, key, (int)j) < key ? 1u : 0u;
+    if (lane < (int)n) items[b + rank] = key;
+  }
+}
+
+// Cells of more than 32 entries, one block per cell in turn. Up to kWideRank entries:
+// each thread ranks entries against the cell's keys in shared memory (m^2 / kWideThreads
+// shared reads per thread). More: the cell's indices are distinct values below n, so
+// they are set in a bitmap of n bits in shared memory and read back in ascending order
+// (n / 32 words scanned once, whatever the cell's size).
+__global__ void __launch_bounds__(kWideThreads) ks_canon_wide(const uint32_t* __restrict__ tmp,
+                                                              const uint32_t* __restrict__ start,
+                                                              const GridBox* __restrict__ gp, uint32_t n,
+                                                              uint32_t* __restrict__ items) {
+  extern __shared__ uint32_t sm[];  // kWideSmemWords
+  __shared__ uint32_t s_warp[kWideThreads / 32];
+  const uint32_t total = gp->total;
+  const uint32_t t = threadIdx.x, lane = t & 31, wid = t >> 5;
+  for (uint32_t c = blockIdx.x; c < total; c += gridDim.x) {
+    const uint32_t b = start[c], m = start[c + 1] - b;
+    if (m <= 32) continue;
+    if (m <= kWideRank) {
+      for (uint32_t e = t; e < m; e += kWideThreads) sm[e] = tmp[b + e];
+      __syncthreads();
+      for (uint32_t e = t; e < m; e += kWideThreads) {
+        const uint32_t key = sm[e];
+        uint32_t rank = 0;
+        for (uint32_t j = 0; j < m; ++j) rank += sm[j] < key ? 1u : 0u;
+        items[b + rank] = key;
+      }
+      __syncthreads();
+      continue;
     }
+    const uint32_t words = (n + 31) / 32;
+    for (uint32_t w = t; w < words; w += kWideThreads) sm[w] = 0;
+    __syncthreads();
+    for (uint32_t e = t; e < m; e += kWideThreads) {
+      const uint32_t v = tmp[b + e];
+      atomicOr(&sm[v >> 5], 1u << (v & 31));
+    }
+    __syncthreads();
+    // thread t owns words [w0, w1); exclusive scan of their set bits over the block
+    const uint32_t per = (words + kWideThreads - 1) / kWideThreads;
+    const uint32_t w0 = min(t * per, words), w1 = min(w0 + per, words);
+    uint32_t cnt = 0;
+    for (uint32_t w = w0; w < w1; ++w) cnt += __popc(sm[w]);
+    uint32_t incl = cnt;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, incl, off);
+      if ((int)lane >= off) incl += y;
+    }
+    if (lane == 31) s_warp[wid] = incl;
+    __syncthreads();
+    uint32_t r = incl - cnt;
+    for (uint32_t k = 0; k < wid; ++k) r += s_warp[k];
+    for (uint32_t w = w0; w < w1; ++w) {
+      uint32_t bits = sm[w];
+      while (bits) {
+        const uint32_t bit = (uint32_t)__ffs(bits) - 1u;
+        bits &= bits - 1u;
+        items[b + r++] = w * 32u + bit;
+      }
+    }
+    __syncthreads();
   }
 }
 
@@ -212,6 +279,10 @@ vxl_status scratch_on(int dev, unsigned char** out) {
     cudaError_t e = cudaGetSymbolAddress(&p, g_grid_scratch);
     if (e != cudaSuccess || !p)
       return fail(VXL_CUDA_ERROR, std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(e));
+    e = cudaFuncSetAttribute(ks_canon_wide, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)(kWideSmemWords * sizeof(uint32_t)));
+    if (e != cudaSuccess)
+      return fail(VXL_CUDA_ERROR, std::string("cudaFuncSetAttribute(ks_canon_wide): ") + cudaGetErrorString(e));
     g_scratch_addr[dev] = p;
   }
   *out = (unsigned char*)g_scratch_addr[dev];
@@ -247,7 +318,8 @@ extern "C" vxl_status vxl_sph_build_grid_static(const float* d_pos_xyz, uint32_t
   GridBox* g = (GridBox*)(base + kGridOff);
   const uint32_t nblk = (n + 255) / 256, tiles = (budget + kTile - 1) / kTile;
   // the array keeps the previous call's contents: zero the counts and reset the box
-  cudaMemsetAsync(counts, 0, ((size_t)budget + 1) * 4, s);
+  cudaError_t e = cudaMemsetAsync(counts, 0, ((size_t)budget + 1) * 4, s);
+  if (e != cudaSuccess) return fail(VXL_CUDA_ERROR, std::string("grid build: ") + cudaGetErrorString(e));
   ks_init<<<1, 32, 0, s>>>(box);
   ks_bbox<<<nblk, 256, 0, s>>>(d_pos_xyz, n, box);
   ks_gridbox<<<1, 32, 0, s>>>(box, h, budget, g);
@@ -257,8 +329,11 @@ extern "C" vxl_status vxl_sph_build_grid_static(const float* d_pos_xyz, uint32_t
   ks_scan_final<<<tiles, kTileThreads, 0, s>>>(counts, g, partial, d_start);
   ks_place<<<nblk, 256, 0, s>>>(cellrank, d_start, n, tmp);
   ks_canon<<<148 * 4, 256, 0, s>>>(tmp, d_start, g, d_items);
+  ks_canon_wide<<<148 * 2, kWideThreads, kWideSmemWords * sizeof(uint32_t), s>>>(tmp, d_start, g, n, d_items);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return fail(VXL_CUDA_ERROR, std::string("grid build launch: ") + cudaGetErrorString(e));
   GridBox hg;
-  cudaError_t e = cudaMemcpyAsync(&hg, g, sizeof(GridBox), cudaMemcpyDeviceToHost, s);
+  e = cudaMemcpyAsync(&hg, g, sizeof(GridBox), cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) return fail(VXL_CUDA_ERROR, std::string("grid build: ") + cudaGetErrorString(e));
   info->min[0] = hg.minx;

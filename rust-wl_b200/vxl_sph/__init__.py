@@ -1,8 +1,8 @@
 """Python binding of the B200 WCSPH C ABI (include/vxl_sph.h) through ctypes.
 
 This is the same thin binding a maintainer would add on the caller's side; the
-reference's own caller is Rust (a `FluidStepper` impl over the C ABI, see
-INTEGRATION.md). `GpuFluidStepper` and `PhysGpuBackend` mirror the reference's trait
+reference's own caller is Rust (a `FluidStepper` impl over the C ABI: the crate under
+rust-wl_b200/rust/vxl-phys-gpu-b200). `GpuFluidStepper` and `PhysGpuBackend` mirror the reference's trait
 methods (crates/vxl-phys-core/src/interop.rs:293-316, crates/vxl-phys-gpu/src/lib.rs:20-29)
 so tests read like the reference's own.
 
@@ -233,6 +233,11 @@ SIGNATURES = {
     "vxl_sph_get_stats": (C.c_int, [_H, C.POINTER(Stats)]),
     "vxl_sph_set_stream": (C.c_int, [_H, C.c_void_p]),
     "vxl_sph_set_profile": (C.c_int, [_H, C.c_int]),
+    "vxl_sph_serve_set_batch_cap": (C.c_int, [C.c_void_p, C.c_uint64]),
+    "vxl_sph_set_wall_contacts": (C.c_int, [_H, C.c_uint32, C.c_uint32, _U32P, _U32P, C.c_uint32, _FP,
+                                            C.c_uint32]),
+    "vxl_sph_export_neighbors": (C.c_int, [_H, C.POINTER(C.c_uint64), C.c_uint64, _U32P, C.c_uint64,
+                                           C.POINTER(C.c_uint64)]),
     "vxl_sph_profile_read": (C.c_int, [_H, C.c_uint32, C.POINTER(C.c_char_p), C.POINTER(C.c_double),
                                        C.POINTER(C.c_uint64)]),
     "vxl_sph_build_grid_static": (C.c_int, [C.c_void_p, C.c_uint32, C.c_float, C.c_uint32, C.c_void_p, C.c_void_p,
@@ -466,6 +471,16 @@ class Scene:
         parr, n, warr, nw = providers_arrays(providers)
         _check(self.lib.vxl_sph_set_providers(self._h, scene, parr, n, warr, nw))
 
+    def set_wall_contacts(self, side: int, ids, start, planes, scene: int = 0) -> None:
+        """One side (0 mirror, 1 projection) of the scene's contact tables (vxl_sph_set_wall_contacts)."""
+        ids = np.ascontiguousarray(ids, np.uint32)
+        start = np.ascontiguousarray(start, np.uint32)
+        planes = np.ascontiguousarray(planes, np.float32).reshape(-1, 6)
+        n = ids.shape[0]
+        _check(self.lib.vxl_sph_set_wall_contacts(self._h, scene, side, _u32ptr(ids) if n else None,
+                                                  _u32ptr(start) if n else None, n,
+                                                  _fptr(planes) if planes.shape[0] else None, planes.shape[0]))
+
     def set_spans(self, spans, scene: int = 0) -> None:
         """Spans for ticks that take none (vxl_sph_step_coupled)."""
         arr, n = spans_array(spans)
@@ -547,6 +562,18 @@ class Scene:
         _check(self.lib.vxl_sph_export_grid(self._h, _u32ptr(items), _u32ptr(start), total + 1, _u32ptr(bins),
                                             C.byref(info)))
         return items, start, bins, info
+
+    def export_neighbors(self):
+        """The last substep's neighbour lists in reference index order, as CSR
+        (offsets (n_total + 1,) uint64, entries uint32; vxl_sph_export_neighbors)."""
+        n = self.n_fluid + self.n_boundary
+        offs = np.empty(n + 1, np.uint64)
+        tot = C.c_uint64()
+        op = offs.ctypes.data_as(C.POINTER(C.c_uint64))
+        _check(self.lib.vxl_sph_export_neighbors(self._h, op, n + 1, None, 0, C.byref(tot)))
+        ent = np.empty(max(tot.value, 1), np.uint32)
+        _check(self.lib.vxl_sph_export_neighbors(self._h, op, n + 1, _u32ptr(ent), tot.value, C.byref(tot)))
+        return offs, ent[:tot.value]
 
     def bounds(self):
         lo = np.empty(3, np.float32)
@@ -751,6 +778,10 @@ class Server:
         except Exception:
             pass
 
+    def set_batch_cap(self, max_fluid_particles: int) -> None:
+        """Stop admitting while the admitted scenes hold this many fluid particles (0: no cap)."""
+        _check(self.lib.vxl_sph_serve_set_batch_cap(self._h, int(max_fluid_particles)))
+
     def submit(self, spec, ticks: int) -> int:
         keep: list = []
         d = _desc_of(spec.params, spec.pos, spec.vel, spec.pmass, spec.n_fluid, 0, keep)
@@ -813,10 +844,11 @@ class GpuFluidStepper:
     keeps the tick-averaged reactions.
     """
 
-    def __init__(self, params: Params, n_fluid: int, pos, vel, pmass, device: int = 0):
+    def __init__(self, params: Params, n_fluid: int, pos, vel, pmass, device: int = 0, boundaries=()):
         self.scene = Scene(params, pos, vel, pmass, n_fluid, device)
         self.n_fluid = n_fluid
         self.nb = self.scene.n_boundary
+        self.boundaries = list(boundaries)  # provider ids of the fluid's walls (stepper.rs:27)
         self._reactions: list = []
 
     def step(self, dt_tick: float, n_fluid: int, pos, vel, pmass, spans) -> None:
@@ -842,7 +874,17 @@ class GpuFluidStepper:
             return None
 
     def gather_walls(self, h: float, providers) -> None:
-        # Provider walls are not part of this path (the configs use Akinci walls).
+        """The reference's gather_walls (stepper.rs:118-137): with provider ids registered,
+        read the fluid positions from the device, gather the mirror and projection contact
+        tables on the host and upload them for the next tick's substeps."""
+        if not self.boundaries:
+            return None
+        from . import walls
+        pos, _ = self.scene.read_state()
+        ps = pos[:self.n_fluid]
+        for side in (walls.MIRROR, walls.PROJECT):
+            ids, start, planes = walls.gather_contacts(self.boundaries, h, ps, providers, side)
+            self.scene.set_wall_contacts(side, ids, start, planes)
         return None
 
 

@@ -10,9 +10,13 @@ memory is a fixed array inside the library.
 The check: through the C ABI, the table it builds equals the table the handle-based
 path builds for the same positions (vxl_sph_create + vxl_sph_substep +
 vxl_sph_export_grid, which builds its table from the positions at the start of the
-substep). The tables are integer data, so the tolerance is zero. Two calls in a row,
-on different scenes, show that the shared array's leftover contents do not leak into
-the next call. Sizes past the fixed limit are refused.
+substep) and the oracle's restatement of the reference's UniformGrid::rebuild
+(crates/vxl-phys-fluid/src/grid.rs:29-76). The tables are integer data, so the
+tolerance is zero. Two calls in a row, on different scenes, show that the shared array's
+leftover contents do not leak into the next call. Cells crowded with hundreds to
+thousands of particles sort in bounded time. After the first (set-up) call on the
+device, a call leaves the device's free memory unchanged. Sizes past the fixed limit are
+refused.
 
 The file name sorts last so that a run stopping at the first failure has run every
 other test first; it also passes on its own in a fresh process.
@@ -63,7 +67,7 @@ def _same(a_info, b_info):
             and list(np.float32(a_info.min[:])) == list(np.float32(b_info.min[:])))
 
 
-def test_static_grid_matches_handle_path_two_calls():
+def test_static_grid_matches_handle_path_two_calls(oracle_mod):
     torch = pytest.importorskip("torch")
     import vxl_sph as vxl
     from vxl_sph import build, scenes
@@ -81,6 +85,64 @@ def test_static_grid_matches_handle_path_two_calls():
         assert _same(info_s, info_h), f"call {call}: grid box differs"
         assert np.array_equal(start_s, start_h), f"call {call}: start differs"
         assert np.array_equal(items_s, items_h), f"call {call}: items differ"
+        start_o, items_o, dims_o = oracle_mod.rebuild_grid(spec.pos, h, LIMIT)
+        assert list(dims_o) == list(info_s.dims), f"call {call}: dims differ from the oracle"
+        assert np.array_equal(start_s, start_o), f"call {call}: start differs from the oracle"
+        assert np.array_equal(items_s, items_o), f"call {call}: items differ from the oracle"
+
+
+def test_static_grid_crowded_cells_in_bounded_time(oracle_mod):
+    """One cell of 300, 2,000 and 5,000 particles (the shared-memory rank and the index
+    bitmap), then a cluster of a few crowded cells among sparse ones: each table equals
+    the oracle's, and each call takes well under a second."""
+    import time
+
+    torch = pytest.importorskip("torch")
+    import vxl_sph as vxl
+    vxl.load()
+    rng = np.random.default_rng(5)
+    cases = [rng.uniform(0.0, 0.05, (n, 3)).astype(np.float32) for n in (300, 2000, 5000)]
+    mixed = np.concatenate([rng.uniform(0.0, 0.04, (2500, 3)), rng.uniform(0.3, 0.34, (700, 3)),
+                            rng.uniform(0.0, 2.0, (4000, 3))]).astype(np.float32)
+    cases.append(rng.permutation(mixed))
+    for k, pos in enumerate(cases):
+        _static_table(vxl, torch, pos, 0.1, LIMIT)  # first call of the shape (kernel loading)
+        t0 = time.perf_counter()
+        items_s, start_s, info_s = _static_table(vxl, torch, pos, 0.1, LIMIT)
+        dt = time.perf_counter() - t0
+        start_o, items_o, dims_o = oracle_mod.rebuild_grid(pos, 0.1, LIMIT)
+        assert list(dims_o) == list(info_s.dims), k
+        assert np.array_equal(start_s, start_o), f"case {k}: start differs from the oracle"
+        assert np.array_equal(items_s, items_o), f"case {k}: items differ from the oracle"
+        assert dt < 0.5, f"case {k}: {dt:.3f} s"
+
+
+def test_static_grid_takes_no_device_memory_after_set_up():
+    """After a warm-up call (the set-up on this device), a further call leaves the
+    device's free memory as it was: all its working memory is the fixed array."""
+    torch = pytest.importorskip("torch")
+    import vxl_sph as vxl
+    from vxl_sph import scenes
+    lib = vxl.load()
+    spec = scenes.dam0()
+    n = spec.n_total
+    d_pos = torch.from_numpy(np.ascontiguousarray(spec.pos, np.float32)).cuda()
+    d_items = torch.empty(n, dtype=torch.int32, device="cuda")
+    d_start = torch.empty(LIMIT + 1, dtype=torch.int32, device="cuda")
+    info = vxl.GridInfo()
+    info.hdr = vxl.header(vxl.GridInfo)
+    stream = torch.cuda.current_stream().cuda_stream
+    args = (C.c_void_p(d_pos.data_ptr()), n, float(spec.params.smoothing_radius), LIMIT,
+            C.c_void_p(d_items.data_ptr()), C.c_void_p(d_start.data_ptr()), LIMIT + 1, C.byref(info),
+            C.c_void_p(stream))
+    assert lib.vxl_sph_build_grid_static(*args) == vxl.OK, lib.vxl_sph_last_error()
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    for _ in range(3):
+        assert lib.vxl_sph_build_grid_static(*args) == vxl.OK, lib.vxl_sph_last_error()
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0, (free0, free1)
 
 
 def test_static_grid_rejects_sizes_past_its_limit():
