@@ -93,7 +93,7 @@ uint64_t Engine::bytes_per_slot(uint32_t nbr_cap) {
   // pos, vel (x2), orig, slot_of, cellrank, items, rc, press, acc, xsph, bforce, bpos,
   // neighbour list + count, staging, half masks, density thread orders (walls variant and
   // grouped pass), density segments
-  return 4 * 16 + 4 + 4 + 8 + 8 + 8 + 4 + 16 + 16 + 16 + 16 + (uint64_t)nbr_cap * 4 + 4 + 32 + 1 + 4 + 4 + 8;
+  return 4 * 16 + 4 + 4 + 8 + 8 + 8 + 4 + 16 + 16 + 16 + 16 + (uint64_t)nbr_cap * 2 + 4 + 32 + 1 + 4 + 4 + 8;
 }
 
 uint64_t Engine::bytes_per_cell() { return 12; }  // counts, start, wet

@@ -808,6 +808,44 @@ __device__ __forceinline__ void walk27(const GridBox& g, const uint32_t* __restr
   }
 }
 
+// Compact neighbour-list entries. Every neighbour of a particle in cell (cx, cy, cz) lies in
+// one of the three x-planes x = cx - 1, cx, cx + 1 of its 27 cells, and inside plane x its
+// slot is at least the first slot of cell (x, max(cy - 1, 0), max(cz - 1, 0)) — cell indices
+// grow with x, y, z and the table is sorted by cell — and below the next plane's first
+// slot. A list entry is (plane << 14) | (slot - plane's first slot), 16 bits; a neighbour
+// 16,384 or more slots past its plane's first slot cannot be encoded, and its list is then
+// marked unusable (bit 31 of the count) so that the consumers walk the cells again.
+constexpr uint32_t kListBad = 0x80000000u;
+constexpr uint32_t kListOffBits = 14;
+constexpr uint32_t kListOffMask = (1u << kListOffBits) - 1u;
+
+struct ListPlanes {
+  uint32_t b0, b1, b2;  // first slot of plane cx - 1 (= b1 at the grid's edge), cx, cx + 1 (~0u if none)
+};
+
+__device__ __forceinline__ ListPlanes list_planes(const GridBox& g, const uint32_t* __restrict__ cst, uint32_t cx,
+                                                  uint32_t cy, uint32_t cz) {
+  const uint32_t ylo = cy > 0 ? cy - 1 : 0, zlo = cz > 0 ? cz - 1 : 0;
+  const uint32_t yz = ylo * g.nz + zlo, nyz = g.ny * g.nz;
+  ListPlanes lp;
+  lp.b1 = cst[cx * nyz + yz];
+  lp.b0 = cx > 0 ? cst[(cx - 1) * nyz + yz] : lp.b1;
+  lp.b2 = cx + 1 < g.nx ? cst[(cx + 1) * nyz + yz] : 0xffffffffu;
+  return lp;
+}
+
+// Entry of neighbour slot j, or 0xffffffff if it cannot be encoded.
+__device__ __forceinline__ uint32_t list_encode(const ListPlanes& lp, uint32_t j) {
+  const uint32_t pl = (j >= lp.b1 ? 1u : 0u) + (j >= lp.b2 ? 1u : 0u);
+  const uint32_t off = j - (pl == 0u ? lp.b0 : (pl == 1u ? lp.b1 : lp.b2));
+  return off > kListOffMask ? 0xffffffffu : (pl << kListOffBits) | off;
+}
+
+__device__ __forceinline__ uint32_t list_decode(const ListPlanes& lp, uint32_t e) {
+  const uint32_t pl = e >> kListOffBits;
+  return (pl == 0u ? lp.b0 : (pl == 1u ? lp.b1 : lp.b2)) + (e & kListOffMask);
+}
+
 // Half-cell masks of the sorted slots, for the density walk: for each aligned block of 32
 // slots, halves[4 * (s >> 5) + a] has bit (s & 31) set iff slot s lies at or above the
 // midplane of its own cell along axis a (x, y, z). One thread per slot over tiles;
@@ -1099,7 +1137,7 @@ template <int kWarps>
 __global__ void __launch_bounds__(kWarps * 32, VXL_DENSITY_SEG_THREADS_PER_SM / (kWarps * 32)) k_e_density_seg(
     const float4* __restrict__ pos, const uint32_t* __restrict__ start, const SceneDev* __restrict__ sc,
     const EngineCtl* __restrict__ ctl, const uint32_t* __restrict__ halves, const uint32_t* __restrict__ order,
-    const uint2* __restrict__ segs, float2* __restrict__ rc, float* __restrict__ press_out, uint32_t* __restrict__ nbr,
+    const uint2* __restrict__ segs, float2* __restrict__ rc, float* __restrict__ press_out, uint16_t* __restrict__ nbr,
     uint32_t* __restrict__ nbr_n, uint32_t cap, uint32_t stride, const uint32_t* __restrict__ wet) {
   if (ctl->err & kErrCellCap) return;
   __shared__ uint32_t s_queue[kWarps][4][kSegQueue];
@@ -1200,8 +1238,9 @@ __global__ void __launch_bounds__(kWarps * 32, VXL_DENSITY_SEG_THREADS_PER_SM / 
     const uint32_t* cst = start + S.cell_off;
     float sum = fluid_i ? S.k.w0 : 0.0f;
     float sum_b = 0.0f;
-    uint32_t cnt = 0;
-    uint32_t* wp = nbr + s;  // next list entry: nbr[cnt * stride + s]
+    uint32_t cnt = 0, bad = 0;
+    uint16_t* wp = nbr + s;  // next list entry: nbr[cnt * stride + s]
+    const ListPlanes lp = list_planes(g, cst, ccx, ccy, ccz);
     // segment walk state (equal on the segment's lanes)
     uint32_t ucm = cm, blk = 0, jb = 0, je = 0, xs = 3, ys = 3, zs = 3, qh = 0, qt = 0;
     for (;;) {
@@ -1271,7 +1310,9 @@ __global__ void __launch_bounds__(kWarps * 32, VXL_DENSITY_SEG_THREADS_PER_SM / 
               }
               if (keep) {
                 if (cnt < cap) {
-                  __stcs(wp, j);  // streaming store: the list is read once, by the force pass
+                  const uint32_t e = list_encode(lp, j);
+                  bad |= e >> 31;
+                  __stcs(wp, (unsigned short)e);  // streaming store: the list is read once, by the force pass
                   wp += stride;
                 }
                 ++cnt;
@@ -1284,7 +1325,7 @@ __global__ void __launch_bounds__(kWarps * 32, VXL_DENSITY_SEG_THREADS_PER_SM / 
       __syncwarp();
     }
     if (act) {
-      nbr_n[s] = cnt;
+      nbr_n[s] = cnt | (bad ? kListBad : 0u);
       const float rho = fluid_i ? (S.k.mass * sum + sum_b) : ((-pi.w) * S.k.w0 + sum);
       const float p = tait(S.k, rho);
       rc[s] = make_float2(rho, p / (rho * rho));
@@ -1374,7 +1415,7 @@ template <int kBlock, bool kWalls = false>
 __global__ void __launch_bounds__(kBlock, VXL_DENSITY_THREADS_PER_SM / kBlock) k_e_density(
     const float4* __restrict__ pos, const uint32_t* __restrict__ start, const SceneDev* __restrict__ sc,
     const TileDev* __restrict__ tiles, uint32_t ntiles, EngineCtl* ctl, const uint32_t* __restrict__ halves,
-    float2* __restrict__ rc, float* __restrict__ press_out, uint32_t* __restrict__ nbr,
+    float2* __restrict__ rc, float* __restrict__ press_out, uint16_t* __restrict__ nbr,
     uint32_t* __restrict__ nbr_n, uint32_t cap, uint32_t stride, const uint32_t* __restrict__ wet,
     const uint32_t* __restrict__ xorder, const ProviderDev* __restrict__ prov = nullptr,
     const WallPlaneDev* __restrict__ wplanes = nullptr, const uint32_t* __restrict__ orig = nullptr,
@@ -1397,8 +1438,9 @@ __global__ void __launch_bounds__(kBlock, VXL_DENSITY_THREADS_PER_SM / kBlock) k
       bin_of(g, pi.x, pi.y, pi.z, cx, cy, cz);
       float sum = fluid_i ? w0 : 0.0f;
       float sum_b = 0.0f;
-      uint32_t cnt = 0;
-      uint32_t* wp = nbr + s;  // next list entry: nbr[cnt * stride + s]
+      uint32_t cnt = 0, bad = 0;
+      uint16_t* wp = nbr + s;  // next list entry: nbr[cnt * stride + s]
+      const ListPlanes lp = list_planes(g, cst, cx, cy, cz);
       float wpt[kWalls ? 3 * kMaxWallPlanes : 1], wn[kWalls ? 3 * kMaxWallPlanes : 1];
       uint32_t np = 0;
       if (kWalls && fluid_i) {
@@ -1453,7 +1495,9 @@ __global__ void __launch_bounds__(kBlock, VXL_DENSITY_THREADS_PER_SM / kBlock) k
           }
           if (rec) {
             if (cnt < cap) {
-              __stcs(wp, j);  // streaming store: the list is read once, by the force pass
+              const uint32_t e = list_encode(lp, j);
+              bad |= e >> 31;
+              __stcs(wp, (unsigned short)e);  // streaming store: the list is read once, by the force pass
               wp += stride;
             }
             ++cnt;
@@ -1488,7 +1532,7 @@ __global__ void __launch_bounds__(kBlock, VXL_DENSITY_THREADS_PER_SM / kBlock) k
       } else {
         walk27<true>(g, cst, pi.x, pi.y, pi.z, cx, cy, cz, h, visit, s);
       }
-      nbr_n[s] = cnt;
+      nbr_n[s] = cnt | (bad ? kListBad : 0u);
       const float rho = fluid_i ? (mass * sum + sum_b) : ((-pi.w) * w0 + sum);
       const float p = tait(k, rho);
       rc[s] = make_float2(rho, p / (rho * rho));
@@ -1507,7 +1551,7 @@ __global__ void __launch_bounds__(kBlock, VXL_DENSITY_THREADS_PER_SM / kBlock) k
 template <int kBlock>
 __global__ void __launch_bounds__(kBlock, VXL_FORCE_THREADS_PER_SM / kBlock) k_e_force(
     const float4* __restrict__ pos, const float4* __restrict__ vel, const float2* __restrict__ rc,
-    const uint32_t* __restrict__ start, const uint32_t* __restrict__ nbr, const uint32_t* __restrict__ nbr_n,
+    const uint32_t* __restrict__ start, const uint16_t* __restrict__ nbr, const uint32_t* __restrict__ nbr_n,
     uint32_t cap, uint32_t stride, SceneDev* __restrict__ sc, const TileDev* __restrict__ tiles, uint32_t ntiles,
     EngineCtl* ctl, float4* __restrict__ pos_out, float4* __restrict__ vel_out, float4* __restrict__ acc_out,
     float4* __restrict__ xsph_out) {
@@ -1570,26 +1614,27 @@ __global__ void __launch_bounds__(kBlock, VXL_FORCE_THREADS_PER_SM / kBlock) k_e
             xz = xz + (vj.z - vi.z) * f;
           };
           const uint32_t cnt = nbr_n[s];
+          const GridBox g = S.g;
+          uint32_t cx, cy, cz;
+          bin_of(g, pi.x, pi.y, pi.z, cx, cy, cz);
           if (cnt <= cap) {
             // the next list entry is loaded one neighbour ahead, so each iteration waits on
             // one dependent gather (pos/vel/rc of j) instead of two (measured: 6-8% faster),
             // and the one kListPrefetch ahead is fetched into L2 (the list is not L2-resident)
-            const uint32_t* np = nbr + s;
-            uint32_t jn = cnt ? *np : 0u;
+            const ListPlanes lp = list_planes(g, start + S.cell_off, cx, cy, cz);
+            const uint16_t* np = nbr + s;
+            uint32_t en = cnt ? *np : 0u;
             for (uint32_t q = 0; q < cnt; ++q) {
-              const uint32_t j = jn;
+              const uint32_t j = list_decode(lp, en);
               np += stride;
               if (q + kListPrefetch < cnt)  // the entry kListPrefetch ahead into L2
                 asm volatile("prefetch.global.L2 [%0];" ::"l"(np + (size_t)(kListPrefetch - 1) * stride));
-              if (q + 1 < cnt) jn = *np;
+              if (q + 1 < cnt) en = *np;
               const float4 pj = pos[j];
               const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
               pair(j, pj, dx, dy, dz, dx * dx + dy * dy + dz * dz);
             }
           } else {
-            const GridBox g = S.g;
-            uint32_t cx, cy, cz;
-            bin_of(g, pi.x, pi.y, pi.z, cx, cy, cz);
             walk27<false, true>(g, start + S.cell_off, pi.x, pi.y, pi.z, cx, cy, cz, h, [&](uint32_t j) {
               if (j == s) return;
               const float4 pj = pos[j];
@@ -1913,7 +1958,7 @@ __device__ __forceinline__ float bforce_pair(const SphConst& k, float r2, float 
 // reference index.
 __global__ void __launch_bounds__(128) k_e_bforce(
     const float4* __restrict__ pos, const float4* __restrict__ vel, const float2* __restrict__ rc,
-    const uint32_t* __restrict__ start, const uint32_t* __restrict__ orig, const uint32_t* __restrict__ nbr,
+    const uint32_t* __restrict__ start, const uint32_t* __restrict__ orig, const uint16_t* __restrict__ nbr,
     const uint32_t* __restrict__ nbr_n, uint32_t cap, uint32_t stride, const SceneDev* __restrict__ sc,
     const uint32_t* __restrict__ slot_of, const TileDev* __restrict__ btiles, uint32_t ntiles, EngineCtl* ctl,
     float4* __restrict__ bforce) {
@@ -1958,7 +2003,8 @@ __global__ void __launch_bounds__(128) k_e_bforce(
       };
       const uint32_t cnt = nbr_n[s];
       if (cnt <= cap) {
-        for (uint32_t q = 0; q < cnt; ++q) insert(nbr[(size_t)q * stride + s]);
+        const ListPlanes lp = list_planes(g, cst, cx, cy, cz);
+        for (uint32_t q = 0; q < cnt; ++q) insert(list_decode(lp, nbr[(size_t)q * stride + s]));
       } else {
         walk27<false, true>(g, cst, pj.x, pj.y, pj.z, cx, cy, cz, k.h, [&](uint32_t ii) {
           const float4 p = pos[ii];
@@ -2279,7 +2325,7 @@ __global__ void k_e_ctab_scatter(const uint32_t* __restrict__ ids, uint32_t n, u
 __global__ void k_e_export_nbr_counts(const uint32_t* __restrict__ nbr_n, const uint32_t* __restrict__ orig,
                                       uint32_t base, uint32_t n, uint32_t* __restrict__ out) {
   const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t < n) out[orig[base + t] - base] = nbr_n[base + t];
+  if (t < n) out[orig[base + t] - base] = nbr_n[base + t] & ~kListBad;
 }
 
 // The entries of each slot's list, in its walk order, as scene-local reference indices,
@@ -2288,7 +2334,7 @@ __global__ void k_e_export_nbr_counts(const uint32_t* __restrict__ nbr_n, const 
 // (the walk the force pass and the boundary gather fall back to).
 __global__ void k_e_export_nbr_entries(const float4* __restrict__ pos, const uint32_t* __restrict__ start,
                                        const SceneDev* __restrict__ sc, uint32_t q, const uint32_t* __restrict__ orig,
-                                       const uint32_t* __restrict__ nbr, const uint32_t* __restrict__ nbr_n,
+                                       const uint16_t* __restrict__ nbr, const uint32_t* __restrict__ nbr_n,
                                        uint32_t cap, uint32_t stride, const unsigned long long* __restrict__ offsets,
                                        uint32_t* __restrict__ out) {
   const SceneDev& S = sc[q];
@@ -2298,16 +2344,17 @@ __global__ void k_e_export_nbr_entries(const float4* __restrict__ pos, const uin
   const uint32_t base = S.base;
   unsigned long long o = offsets[orig[s] - base];
   const uint32_t c = nbr_n[s];
-  if (c <= cap) {
-    for (uint32_t k = 0; k < c; ++k) out[o + k] = orig[nbr[(size_t)k * stride + s]] - base;
-    return;
-  }
   const GridBox g = S.g;
   const float4 pi = pos[s];
-  const bool fluid_i = pi.w > 0.0f;
-  const float h2 = S.k.h2;
   uint32_t cx, cy, cz;
   bin_of(g, pi.x, pi.y, pi.z, cx, cy, cz);
+  if (c <= cap) {
+    const ListPlanes lp = list_planes(g, start + S.cell_off, cx, cy, cz);
+    for (uint32_t k = 0; k < c; ++k) out[o + k] = orig[list_decode(lp, nbr[(size_t)k * stride + s])] - base;
+    return;
+  }
+  const bool fluid_i = pi.w > 0.0f;
+  const float h2 = S.k.h2;
   walk27<true>(g, start + S.cell_off, pi.x, pi.y, pi.z, cx, cy, cz, S.k.h, [&](uint32_t j) {
     const float4 pj = pos[j];
     const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;

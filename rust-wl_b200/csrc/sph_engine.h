@@ -171,7 +171,7 @@ class Engine {
   void* xsph_ = nullptr;
   void* bforce_ = nullptr;
   void* bpos_ = nullptr;
-  uint32_t* nbr_ = nullptr;
+  uint16_t* nbr_ = nullptr;  // neighbour lists: 16-bit plane-relative entries, list position major
   uint32_t* nbr_n_ = nullptr;
   uint32_t* halves_ = nullptr;  // 4 words per 32 slots: upper-half masks along x, y, z
   uint32_t* xorder_ = nullptr;  // density order of the provider-wall variant at doubled bins (lower x halves first)
