@@ -148,17 +148,16 @@ def build_scene(workload: str):
     return scenes.CONFIGS[workload]()
 
 
-# The CPU path's bounded sample of each plain workload: one substep of the dam10m tank
-# (walls, 64 boxes, constants and doubled bins as in the workload) holding a 100^3 fluid
-# block instead of 215^3, so that a step of the reference arm takes seconds, not half a
-# minute; dam0 and dam1 are sampled whole.
-SAMPLE_BLOCK = {"dam10m": 100}
-
-
+# The CPU path's bounded sample of each plain workload. dam10m: a 100^3 fluid block in the
+# corner of the dam10m tank, its floor and two corner walls cropped around the block and two
+# marker boxes at the tank's far corners (scenes.dam10m_sample): the same grid and doubled
+# bins as the full scene, a boundary-to-fluid ratio close to its own, 1M fluid particles, so
+# that a step of the reference arm (one substep) takes seconds instead of half a minute.
+# dam0 and dam1 are sampled whole.
 def cpu_sample_spec(workload: str):
     from vxl_sph import scenes
-    if workload in SAMPLE_BLOCK:
-        return scenes.dam10m_block(SAMPLE_BLOCK[workload])
+    if workload == "dam10m":
+        return scenes.dam10m_sample(100)
     return build_scene(workload)
 
 

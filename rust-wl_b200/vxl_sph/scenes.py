@@ -310,6 +310,32 @@ def dam10m_block(n: int = 100, seed: int = 2, boxes: int = 64) -> SceneSpec:
     return dam_break(f"dam10m_block{n}", (n, n, n), 0.005, (2.5, 1.2, 1.2), 120, seed, extra_bodies=extra)
 
 
+def dam10m_sample(n: int = 100, seed: int = 2) -> SceneSpec:
+    """A bounded sample of dam10m for the CPU baseline: an n^3 fluid block in the corner of
+    the dam10m tank with the tank's floor and two corner walls cropped to the block's
+    surroundings, so the boundary-to-fluid ratio is close to the full scene's (0.11), and two
+    small marker boxes at the tank's far corners, so the grid box, and with it the doubled
+    bins, is the full scene's. Same spacing, constants and jitter rule; the boxes of the full
+    scene lie far from the block and are left out."""
+    s = 0.005
+    t = F(2.0 * s)
+    th = t * F(0.5)
+    ext = F((n + 8) * s)  # the block plus a margin of 8 spacings
+    bodies = [
+        Body(0, (ext * F(0.5) + t, th, ext * F(0.5) + t), (ext * F(0.5), -th, ext * F(0.5))),  # floor
+        Body(1, (th, ext * F(0.5), ext * F(0.5) + t), (-th, ext * F(0.5), ext * F(0.5))),      # x = 0 wall
+        Body(3, (ext * F(0.5) + t, ext * F(0.5), th), (ext * F(0.5), ext * F(0.5), -th)),      # z = 0 wall
+        Body(5, (s, s, s), (2.5 + th, 1.2 - s, 1.2 + th)),                                      # far corner markers
+        Body(6, (s, s, s), (2.5 + th, -th, -th)),
+    ]
+    params = baseline_params(s)
+    fluid = jitter(fluid_block((0.0, 0.0, 0.0), (n, n, n), s), s, seed)
+    fill = float((n * s) ** 3 / (2.5 * 1.2 * 1.2))
+    return assemble(f"dam10m_sample{n}", params, fluid, bodies, s, 120,
+                    {"dims": (n, n, n), "tank": (2.5, 1.2, 1.2), "fill": fill, "seed": seed, "bodies": bodies,
+                     "dynamic": [False] * len(bodies)})
+
+
 def small_dam(n=(8, 8, 8), spacing: float = 0.05, tank=(0.8, 0.6, 0.6), seed: int = 3, substeps: int = 4,
               ticks: int = 10, **over) -> SceneSpec:
     """A small tank scene for parity tests (same construction, smaller sizes)."""
