@@ -275,18 +275,26 @@ vxl_status vxl_sph_reactions_all(vxl_sph_handle* h, vxl_sph_reaction* out, uint3
 /* Launch shape of the particle passes: threads per block (128 or 256), slots per tile
  * (a multiple of 128, at least one block) and the scheduling: waves = 0 runs one block
  * per tile, waves = k > 0 runs k x the occupancy limit of persistent blocks that draw
- * tiles from a counter. Default {256, 256, 0}. */
+ * tiles from a counter. density selects the density kernel of scenes without provider
+ * walls: VXL_SPH_DENSITY_WALK (one thread per particle walking its own cells, threads
+ * ordered by cell octant) or VXL_SPH_DENSITY_GROUPED (eight lanes per cell octant sharing
+ * one staged stream of candidates); both give the same results. Default {256, 256, 0,
+ * WALK}. */
+#define VXL_SPH_DENSITY_WALK 0u
+#define VXL_SPH_DENSITY_GROUPED 1u
 typedef struct vxl_sph_tuning {
   vxl_block_header hdr;
   uint32_t block;
   uint32_t tile;
   uint32_t waves;
+  uint32_t density;     /* VXL_SPH_DENSITY_* */
   float ms_per_substep; /* filled by vxl_sph_autotune: device time of the chosen shape */
 } vxl_sph_tuning;
 vxl_status vxl_sph_set_tuning(vxl_sph_handle* h, const vxl_sph_tuning* t);
 vxl_status vxl_sph_get_tuning(vxl_sph_handle* h, vxl_sph_tuning* t);
 /* Autotuner: times every candidate shape on the handle's own scenes (`trials` substeps
- * each, from a snapshot of the state that is restored afterwards) and keeps the fastest.
+ * each, from a snapshot of the state that is restored afterwards) and keeps the fastest;
+ * then times the other density kernel at that shape and keeps the faster.
  * Results are identical for every shape; only the time differs. */
 vxl_status vxl_sph_autotune(vxl_sph_handle* h, float dt_tick, uint32_t trials, vxl_sph_tuning* best);
 

@@ -420,9 +420,11 @@ vxl_status vxl_sph_set_tuning(vxl_sph_handle* h, const vxl_sph_tuning* t) {
   HANDLE_OR_FAIL(h);
   if (!t) return set_error(VXL_NULL_POINTER, "tuning is NULL");
   if (!check_header(t->hdr, sizeof(vxl_sph_tuning))) return set_error(VXL_SIZE_MISMATCH, "tuning header");
-  if ((t->block != 128 && t->block != 256) || t->tile < t->block || t->tile % 128 != 0 || t->waves > 4)
-    return set_error(VXL_INVALID_ARGUMENT, "block must be 128/256, tile a multiple of 128 and >= block, waves 0..4");
-  h->e->set_tuning(vxl::Tuning{t->block, t->tile, t->waves});
+  if ((t->block != 128 && t->block != 256) || t->tile < t->block || t->tile % 128 != 0 || t->waves > 4 ||
+      t->density > 1u)
+    return set_error(VXL_INVALID_ARGUMENT,
+                     "block must be 128/256, tile a multiple of 128 and >= block, waves 0..4, density 0/1");
+  h->e->set_tuning(vxl::Tuning{t->block, t->tile, t->waves, t->density});
   return VXL_OK;
 }
 
@@ -433,6 +435,7 @@ vxl_status vxl_sph_get_tuning(vxl_sph_handle* h, vxl_sph_tuning* t) {
   t->block = h->e->tuning().block;
   t->tile = h->e->tuning().tile;
   t->waves = h->e->tuning().waves;
+  t->density = h->e->tuning().density;
   return VXL_OK;
 }
 
@@ -447,6 +450,7 @@ vxl_status vxl_sph_autotune(vxl_sph_handle* h, float dt_tick, uint32_t trials, v
     best->block = t.block;
     best->tile = t.tile;
     best->waves = t.waves;
+    best->density = t.density;
     best->ms_per_substep = ms;
   }
   return VXL_OK;

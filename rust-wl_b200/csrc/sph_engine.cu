@@ -264,6 +264,7 @@ void Engine::set_tuning(const Tuning& t) {
   if (tuning_.tile < tuning_.block) tuning_.tile = tuning_.block;
   tuning_.tile = (tuning_.tile / 128) * 128;
   if (tuning_.waves > 4) tuning_.waves = 4;
+  if (tuning_.density > 1) tuning_.density = 0;
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device_);
   int occ_d = 1, occ_f = 1, occ_b = 1;
@@ -1398,6 +1399,8 @@ void Engine::enqueue_substep(bool with_reactions) {
   LAUNCH(KID_CANON, k_e_canon<<<148 * 8, 256, 0, st>>>((const uint2*)items_, start_, ctl_d_, p0, v0, (float4*)pos_[1],
                                                        (float4*)vel_[1], orig_, slot_of_));
   LAUNCH(KID_HALFMASK, k_e_halfmask<<<key_blocks, kThreads, 0, st>>>(p1, sc_d_, tiles_d_, ntiles_, ctl_d_, halves_));
+  // thread order of the density pass: x halves first per cell for the provider-wall variant;
+  // otherwise octant-major per 256-slot chunk (and the segments of the grouped kernel)
   if (walls_any_) LAUNCH(KID_HALFMASK, k_e_xorder<<<148 * 8, kThreads, 0, st>>>(start_, ctl_d_, halves_, xorder_));
   else
     LAUNCH(KID_GROUPS, k_e_groups<<<key_blocks, 256, 0, st>>>(p1, sc_d_, tiles_d_, ntiles_, ctl_d_, order_,
@@ -1417,10 +1420,18 @@ void Engine::enqueue_substep(bool with_reactions) {
       LAUNCH(KID_DENSITY, k_e_density<256, true><<<gd, 256, 0, st>>>(
                               p1, start_, sc_d_, tiles_d_, ntiles_, ctl_d_, halves_, (float2*)rc_, press_, nbr_, nbr_n_,
                               nbr_cap_, stride, wet_, xorder_, prov_d_, wplanes_d_, orig_, ctab(0)));
-  } else {
+  } else if (tuning_.density == 1) {
     LAUNCH(KID_DENSITY, k_e_density_seg<kSegWarps><<<grid_seg_, kSegWarps * 32, 0, st>>>(
                             p1, start_, sc_d_, ctl_d_, halves_, order_, (const uint2*)segs_, (float2*)rc_, press_, nbr_,
                             nbr_n_, nbr_cap_, stride, wet_));
+  } else if (tuning_.block == 128) {
+    LAUNCH(KID_DENSITY, k_e_density<128><<<gd, 128, 0, st>>>(p1, start_, sc_d_, tiles_d_, ntiles_, ctl_d_, halves_,
+                                                             (float2*)rc_, press_, nbr_, nbr_n_, nbr_cap_, stride, wet_,
+                                                             order_));
+  } else {
+    LAUNCH(KID_DENSITY, k_e_density<256><<<gd, 256, 0, st>>>(p1, start_, sc_d_, tiles_d_, ntiles_, ctl_d_, halves_,
+                                                             (float2*)rc_, press_, nbr_, nbr_n_, nbr_cap_, stride, wet_,
+                                                             order_));
   }
   // Reaction branch on the side stream: it reads only the sorted buffer, the densities and
   // the lists, so it runs beside the force pass (which writes the other buffer).
@@ -1680,7 +1691,7 @@ vxl_status Engine::autotune(float dt_tick, uint32_t trials, Tuning* best, float*
       for (uint32_t wi = 0; st == VXL_OK && wi < 3; ++wi) {
         st = copy_all(false);
         if (st != VXL_OK) break;
-        set_tuning(Tuning{blocks[bi], blocks[bi] * tile_mult[ti], waves_c[wi]});
+        set_tuning(Tuning{blocks[bi], blocks[bi] * tile_mult[ti], waves_c[wi], was.density});
         enqueue_substep(false);  // warm-up
         cudaEventRecord(e0, stream_);
         for (uint32_t r = 0; r < trials; ++r) enqueue_substep(false);
@@ -1698,6 +1709,31 @@ vxl_status Engine::autotune(float dt_tick, uint32_t trials, Tuning* best, float*
           best_t = tuning_;
         }
       }
+  // the other density kernel at the best shape (provider-wall scenes use their own variant)
+  if (st == VXL_OK && !walls_any_) {
+    Tuning other = best_t;
+    other.density = 1u - best_t.density;
+    st = copy_all(false);
+    if (st == VXL_OK) {
+      set_tuning(other);
+      enqueue_substep(false);
+      cudaEventRecord(e0, stream_);
+      for (uint32_t r = 0; r < trials; ++r) enqueue_substep(false);
+      join_side();
+      cudaEventRecord(e1, stream_);
+      if (cudaStreamSynchronize(stream_) != cudaSuccess) {
+        st = set_error(VXL_CUDA_ERROR, "autotune trial failed");
+      } else {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        ms /= (float)trials;
+        if (ms < best_v) {
+          best_v = ms;
+          best_t = tuning_;
+        }
+      }
+    }
+  }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   if (st == VXL_OK) st = copy_all(false);

@@ -32,6 +32,7 @@ struct Tuning {
   uint32_t block = 256;   // threads per block of the density/force passes (128 or 256)
   uint32_t tile = 256;    // slots per tile (a multiple of 128, at least one block)
   uint32_t waves = 0;     // 0: one block per tile; k > 0: persistent, k x the occupancy limit
+  uint32_t density = 0;   // density kernel without provider walls: 0 per-particle walk, 1 grouped segments
 };
 
 struct SceneInfo {

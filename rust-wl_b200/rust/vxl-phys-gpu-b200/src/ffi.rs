@@ -22,6 +22,8 @@ pub const DEVICE_FAULT_FLAG: u32 = 9;
 
 pub const PROVIDER_FACES: u32 = 0;
 pub const PROVIDER_CONVEX: u32 = 1;
+pub const DENSITY_WALK: u32 = 0;
+pub const DENSITY_GROUPED: u32 = 1;
 pub const WALLS_MIRROR: u32 = 0;
 pub const WALLS_PROJECT: u32 = 1;
 
@@ -117,6 +119,7 @@ pub struct Tuning {
     pub block: u32,
     pub tile: u32,
     pub waves: u32,
+    pub density: u32,
     pub ms_per_substep: f32,
 }
 

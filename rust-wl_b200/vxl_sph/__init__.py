@@ -105,7 +105,7 @@ class Stats(C.Structure):
 
 class Tuning(C.Structure):
     _fields_ = [("hdr", BlockHeader), ("block", C.c_uint32), ("tile", C.c_uint32), ("waves", C.c_uint32),
-                ("ms_per_substep", C.c_float)]
+                ("density", C.c_uint32), ("ms_per_substep", C.c_float)]
 
 
 class RequestStatus(C.Structure):
@@ -712,23 +712,29 @@ class Batch:
                                                   _u32ptr(bins), C.byref(info)))
         return items, start, bins, info
 
-    def set_tuning(self, block: int, tile: int, waves: int = 0):
+    def set_tuning(self, block: int, tile: int, waves: int = 0, density: int | None = None):
+        """Launch shape; density 0 (per-particle walk) or 1 (grouped segments), None keeps it."""
         t = Tuning()
         t.hdr = header(Tuning)
+        if density is None:
+            _check(self.lib.vxl_sph_get_tuning(self._h, C.byref(t)))
         t.block, t.tile, t.waves = block, tile, waves
+        if density is not None:
+            t.density = density
         _check(self.lib.vxl_sph_set_tuning(self._h, C.byref(t)))
 
     def tuning(self):
         t = Tuning()
         t.hdr = header(Tuning)
         _check(self.lib.vxl_sph_get_tuning(self._h, C.byref(t)))
-        return t.block, t.tile, t.waves
+        return t.block, t.tile, t.waves, t.density
 
     def autotune(self, dt_tick: float, trials: int = 3):
         t = Tuning()
         t.hdr = header(Tuning)
         _check(self.lib.vxl_sph_autotune(self._h, dt_tick, trials, C.byref(t)))
-        return {"block": t.block, "tile": t.tile, "waves": t.waves, "ms_per_substep": t.ms_per_substep}
+        return {"block": t.block, "tile": t.tile, "waves": t.waves, "density": ["walk", "grouped"][t.density],
+                "ms_per_substep": t.ms_per_substep}
 
     def set_stream(self, stream_handle: int | None) -> None:
         _check(self.lib.vxl_sph_set_stream(self._h, C.c_void_p(stream_handle or 0)))

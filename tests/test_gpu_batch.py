@@ -57,7 +57,8 @@ def test_batch_equals_oracle_and_plain(vxl, oracle_mod):
         assert np.array_equal(items, og["items"]) and np.array_equal(start, og["start"])
 
 
-@pytest.mark.parametrize("shape", [(128, 128, 0), (256, 1024, 0), (128, 128, 1), (256, 256, 2), (128, 4096, 1), (256, 512, 1)])
+@pytest.mark.parametrize("shape", [(128, 128, 0, 0), (256, 1024, 0, 1), (128, 128, 1, 1), (256, 256, 2, 0),
+                                   (128, 4096, 1, 0), (256, 512, 1, 1)])
 def test_batch_launch_shape_does_not_change_results(vxl, shape):
     specs = _specs()
     ref = vxl.Batch(specs)

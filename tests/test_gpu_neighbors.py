@@ -43,10 +43,14 @@ def _compare_lists(g, o, label):
     return go, ge
 
 
-def _lists_after(vxl, oracle_mod, spec, warm_ticks=0, substeps_before=0):
+DENSITY = [0, 1]  # the per-particle walk and the grouped (segment) density kernel
+
+
+def _lists_after(vxl, oracle_mod, spec, warm_ticks=0, substeps_before=0, density=0):
     """GPU and oracle from identical state; optionally advanced together; then the oracle's
     lists from its current positions and the GPU's lists of its next substep."""
     g = vxl.Scene(spec.params, spec.pos, spec.vel, spec.pmass, spec.n_fluid)
+    g.set_tuning(256, 256, 0, density)
     o = oracle_mod.OracleSystem.from_scene(spec, threads=_threads())
     dt_tick = float(F32(1) / F32(60))
     for _ in range(warm_ticks):
@@ -61,35 +65,39 @@ def _lists_after(vxl, oracle_mod, spec, warm_ticks=0, substeps_before=0):
     return g, o
 
 
-def test_neighbor_lists_dam0_bit_exact(vxl, oracle_mod):
+@pytest.mark.parametrize("density", DENSITY)
+def test_neighbor_lists_dam0_bit_exact(vxl, oracle_mod, density):
     from vxl_sph import scenes
     spec = scenes.dam0()
-    g, o = _lists_after(vxl, oracle_mod, spec)
+    g, o = _lists_after(vxl, oracle_mod, spec, density=density)
     offs, ent = _compare_lists(g, o, "dam0")
     counts = np.diff(offs.astype(np.int64))
     assert counts[:spec.n_fluid].mean() > 20 and ent.size > 0
 
 
-def test_neighbor_lists_flowing_state(vxl, oracle_mod):
+@pytest.mark.parametrize("density", DENSITY)
+def test_neighbor_lists_flowing_state(vxl, oracle_mod, density):
     """After two ticks of the dam break (particles moved, cells reordered)."""
     from vxl_sph import scenes
     spec = scenes.dam0()
-    g, o = _lists_after(vxl, oracle_mod, spec, warm_ticks=2, substeps_before=3)
+    g, o = _lists_after(vxl, oracle_mod, spec, warm_ticks=2, substeps_before=3, density=density)
     _compare_lists(g, o, "dam0 after 2 ticks + 3 substeps")
 
 
-def test_neighbor_lists_doubled_bins(vxl, oracle_mod):
-    """The 10M tank's grid rule with a 100^3 block: the budget doubles the bins to 2h, so the
-    density pass culls half-cells and groups particles by octant."""
+@pytest.mark.parametrize("density", DENSITY)
+def test_neighbor_lists_doubled_bins(vxl, oracle_mod, density):
+    """The 10M tank's grid rule with a 40^3 block: the budget doubles the bins to 2h, so the
+    density pass culls half-cells and orders or groups particles by octant."""
     from vxl_sph import scenes
     spec = scenes.dam10m_block(40)
-    g, o = _lists_after(vxl, oracle_mod, spec)
+    g, o = _lists_after(vxl, oracle_mod, spec, density=density)
     _, _, _, info = g.export_grid()
     assert info.bin >= 2 * spec.params.smoothing_radius * 0.999
     _compare_lists(g, o, "dam10m tank, 40^3 block")
 
 
-def test_neighbor_lists_longer_than_the_recorded_cap(vxl, oracle_mod):
+@pytest.mark.parametrize("density", DENSITY)
+def test_neighbor_lists_longer_than_the_recorded_cap(vxl, oracle_mod, density):
     """h = 3 s: about 110 neighbours per particle, past the 64 recorded entries, so every
     interior list is walked again; boundary particles keep only their fluid neighbours."""
     from vxl_sph import scenes
@@ -97,7 +105,7 @@ def test_neighbor_lists_longer_than_the_recorded_cap(vxl, oracle_mod):
     params = scenes.baseline_params(s, substeps=4, smoothing_radius=3 * s)
     fluid = scenes.jitter(scenes.fluid_block((0.0, 0.0, 0.0), (14, 12, 14), s), s, 5)
     spec = scenes.assemble("wide", params, fluid, scenes.tank_bodies((0.4, 0.4, 0.4), 2 * s), s, 2)
-    g, o = _lists_after(vxl, oracle_mod, spec)
+    g, o = _lists_after(vxl, oracle_mod, spec, density=density)
     offs, _ = _compare_lists(g, o, "h = 3 s")
     assert np.diff(offs.astype(np.int64)).max() > 64
 
@@ -113,27 +121,30 @@ def test_neighbor_lists_before_any_substep_is_not_ready(vxl):
 
 def test_dam10m_substep_bit_exact(vxl, oracle_mod):
     """The 10M configuration, one substep from identical state (doubled bins, walls, 64
-    boxes, the configuration's constants): every per-particle quantity bit for bit."""
+    boxes, the configuration's constants): every per-particle quantity bit for bit, with
+    either density kernel."""
     from vxl_sph import scenes
     spec = scenes.dam10m()
     assert spec.n_fluid == 9938375 and len(spec.spans) == 69
-    g = vxl.Scene(spec.params, spec.pos, spec.vel, spec.pmass, spec.n_fluid)
     o = oracle_mod.OracleSystem.from_scene(spec, threads=_threads())
-    g.set_record(True)
     dt = f32_dt(spec.params.substeps)
-    g.substep(dt)
     o.substep(dt)
-    _, _, _, info = g.export_grid()
-    assert info.bin >= 2 * spec.params.smoothing_radius * 0.999, "the cell budget doubles the bins"
-    compare_grid(g, o, "dam10m")
-    dens, press, acc, xsph, bf = g.read_fields()
     r = o.read_f32()
     nf = spec.n_fluid
-    assert_bits(dens, r["dens"], "density")
-    assert_bits(press, r["press"], "pressure")
-    assert_bits(acc[:nf], r["acc"][:nf], "acceleration")
-    assert_bits(xsph[:nf], r["xsph"][:nf], "xsph")
-    assert_bits(bf, r["bforce"][nf:], "boundary reaction per particle")
-    compare_state(g, o, "dam10m after one substep")
+    for density in DENSITY:
+        g = vxl.Scene(spec.params, spec.pos, spec.vel, spec.pmass, spec.n_fluid)
+        g.set_tuning(256, 256, 0, density)
+        g.set_record(True)
+        g.substep(dt)
+        _, _, _, info = g.export_grid()
+        assert info.bin >= 2 * spec.params.smoothing_radius * 0.999, "the cell budget doubles the bins"
+        compare_grid(g, o, f"dam10m density kernel {density}")
+        dens, press, acc, xsph, bf = g.read_fields()
+        assert_bits(dens, r["dens"], "density")
+        assert_bits(press, r["press"], "pressure")
+        assert_bits(acc[:nf], r["acc"][:nf], "acceleration")
+        assert_bits(xsph[:nf], r["xsph"][:nf], "xsph")
+        assert_bits(bf, r["bforce"][nf:], "boundary reaction per particle")
+        compare_state(g, o, f"dam10m after one substep, density kernel {density}")
+        g.close()
     o.close()
-    g.close()

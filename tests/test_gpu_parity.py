@@ -78,11 +78,14 @@ def test_backend_available(vxl):
     assert b.available() and b.name() == "b200-cuda-wcsph"
 
 
-def test_single_substep_bit_exact(vxl, oracle_mod):
-    """One substep from identical state: table, rho, p, a, xsph, bforce, pos, vel."""
+@pytest.mark.parametrize("density", [0, 1])
+def test_single_substep_bit_exact(vxl, oracle_mod, density):
+    """One substep from identical state: table, rho, p, a, xsph, bforce, pos, vel (with the
+    per-particle walk and with the grouped density kernel)."""
     from vxl_sph import scenes
     spec = scenes.small_dam(n=(10, 12, 9), spacing=0.05, tank=(0.8, 0.7, 0.6))
     g, o = pair(vxl, oracle_mod, spec)
+    g.set_tuning(256, 256, 0, density)
     g.set_record(True)
     dt = f32_dt(spec.params.substeps)
     g.substep(dt)
@@ -231,22 +234,28 @@ def _custom(vxl, pos, vel=None, h=0.1, spacing=0.05, max_bins=0, boundary=None, 
 
 
 def _run_both(vxl, oracle_mod, spec, substeps=1):
-    g, o = pair(vxl, oracle_mod, spec)
-    g.set_record(True)
+    """The oracle and the GPU with each density kernel (per-particle walk, grouped segments)
+    from identical state, `substeps` substeps, everything bit for bit."""
+    o = oracle_mod.OracleSystem.from_scene(spec, threads=8)
     dt = f32_dt(4)
     for _ in range(substeps):
-        g.substep(dt)
         o.substep(dt)
-    compare_grid(g, o)
-    dens, press, acc, xsph, bf = g.read_fields()
     r = o.read_f32()
     nf = spec.n_fluid
-    assert_bits(dens, r["dens"], "density")
-    assert_bits(acc[:nf], r["acc"][:nf], "acc")
-    assert_bits(xsph[:nf], r["xsph"][:nf], "xsph")
-    if spec.n_boundary:
-        assert_bits(bf, r["bforce"][nf:], "bforce")
-    compare_state(g, o)
+    for density in (0, 1):
+        g = vxl.Scene(spec.params, spec.pos, spec.vel, spec.pmass, spec.n_fluid)
+        g.set_tuning(256, 256, 0, density)
+        g.set_record(True)
+        for _ in range(substeps):
+            g.substep(dt)
+        compare_grid(g, o, f"density kernel {density}")
+        dens, press, acc, xsph, bf = g.read_fields()
+        assert_bits(dens, r["dens"], f"density (kernel {density})")
+        assert_bits(acc[:nf], r["acc"][:nf], f"acc (kernel {density})")
+        assert_bits(xsph[:nf], r["xsph"][:nf], f"xsph (kernel {density})")
+        if spec.n_boundary:
+            assert_bits(bf, r["bforce"][nf:], f"bforce (kernel {density})")
+        compare_state(g, o, f"density kernel {density}")
     return g, o
 
 
