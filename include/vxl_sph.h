@@ -294,7 +294,7 @@ vxl_status vxl_sph_set_tuning(vxl_sph_handle* h, const vxl_sph_tuning* t);
 vxl_status vxl_sph_get_tuning(vxl_sph_handle* h, vxl_sph_tuning* t);
 /* Autotuner: times every candidate shape on the handle's own scenes (`trials` substeps
  * each, from a snapshot of the state that is restored afterwards) and keeps the fastest;
- * then times the other density kernel at that shape and keeps the faster.
+ * then times the other density kernels at that shape and keeps the fastest.
  * Results are identical for every shape; only the time differs. */
 vxl_status vxl_sph_autotune(vxl_sph_handle* h, float dt_tick, uint32_t trials, vxl_sph_tuning* best);
 

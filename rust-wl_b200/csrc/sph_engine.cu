@@ -1402,10 +1402,20 @@ void Engine::enqueue_substep(bool with_reactions) {
   // thread order of the density pass: x halves first per cell for the provider-wall variant;
   // otherwise octant-major per 256-slot chunk (and the segments of the grouped kernel)
   if (walls_any_) LAUNCH(KID_HALFMASK, k_e_xorder<<<148 * 8, kThreads, 0, st>>>(start_, ctl_d_, halves_, xorder_));
+#ifdef VXL_WALK_XORDER
+  else if (tuning_.density == 0) {
+    LAUNCH(KID_HALFMASK, k_e_xorder<<<148 * 8, kThreads, 0, st>>>(start_, ctl_d_, halves_, xorder_));
+  }
+#endif
   else
     LAUNCH(KID_GROUPS, k_e_groups<<<key_blocks, 256, 0, st>>>(p1, sc_d_, tiles_d_, ntiles_, ctl_d_, order_,
                                                               (uint2*)segs_));
   const uint32_t stride = (uint32_t)slot_cap_;
+#ifdef VXL_WALK_XORDER
+  const uint32_t* walk_order = xorder_;
+#else
+  const uint32_t* walk_order = order_;
+#endif
   const bool rec = record_;
   const uint32_t per_tile = std::max<uint32_t>(ntiles_, 1);
   const uint32_t gd = grid_density_ ? (uint32_t)grid_density_ : per_tile;
@@ -1427,11 +1437,11 @@ void Engine::enqueue_substep(bool with_reactions) {
   } else if (tuning_.block == 128) {
     LAUNCH(KID_DENSITY, k_e_density<128><<<gd, 128, 0, st>>>(p1, start_, sc_d_, tiles_d_, ntiles_, ctl_d_, halves_,
                                                              (float2*)rc_, press_, nbr_, nbr_n_, nbr_cap_, stride, wet_,
-                                                             order_));
+                                                             walk_order));
   } else {
     LAUNCH(KID_DENSITY, k_e_density<256><<<gd, 256, 0, st>>>(p1, start_, sc_d_, tiles_d_, ntiles_, ctl_d_, halves_,
                                                              (float2*)rc_, press_, nbr_, nbr_n_, nbr_cap_, stride, wet_,
-                                                             order_));
+                                                             walk_order));
   }
   // Reaction branch on the side stream: it reads only the sorted buffer, the densities and
   // the lists, so it runs beside the force pass (which writes the other buffer).
@@ -1709,29 +1719,29 @@ vxl_status Engine::autotune(float dt_tick, uint32_t trials, Tuning* best, float*
           best_t = tuning_;
         }
       }
-  // the other density kernel at the best shape (provider-wall scenes use their own variant)
-  if (st == VXL_OK && !walls_any_) {
+  // the other density kernels at the best shape (provider-wall scenes use their own variant)
+  for (uint32_t dv = 0; st == VXL_OK && !walls_any_ && dv < 2; ++dv) {
+    if (dv == best_t.density) continue;
     Tuning other = best_t;
-    other.density = 1u - best_t.density;
+    other.density = dv;
     st = copy_all(false);
-    if (st == VXL_OK) {
-      set_tuning(other);
-      enqueue_substep(false);
-      cudaEventRecord(e0, stream_);
-      for (uint32_t r = 0; r < trials; ++r) enqueue_substep(false);
-      join_side();
-      cudaEventRecord(e1, stream_);
-      if (cudaStreamSynchronize(stream_) != cudaSuccess) {
-        st = set_error(VXL_CUDA_ERROR, "autotune trial failed");
-      } else {
-        float ms = 0.f;
-        cudaEventElapsedTime(&ms, e0, e1);
-        ms /= (float)trials;
-        if (ms < best_v) {
-          best_v = ms;
-          best_t = tuning_;
-        }
-      }
+    if (st != VXL_OK) break;
+    set_tuning(other);
+    enqueue_substep(false);
+    cudaEventRecord(e0, stream_);
+    for (uint32_t r = 0; r < trials; ++r) enqueue_substep(false);
+    join_side();
+    cudaEventRecord(e1, stream_);
+    if (cudaStreamSynchronize(stream_) != cudaSuccess) {
+      st = set_error(VXL_CUDA_ERROR, "autotune trial failed");
+      break;
+    }
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    ms /= (float)trials;
+    if (ms < best_v) {
+      best_v = ms;
+      best_t = tuning_;
     }
   }
   cudaEventDestroy(e0);

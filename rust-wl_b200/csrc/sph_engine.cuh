@@ -39,7 +39,7 @@
 #define VXL_FORCE_THREADS_PER_SM 1280
 #endif
 #ifndef VXL_DENSITY_SEG_THREADS_PER_SM
-#define VXL_DENSITY_SEG_THREADS_PER_SM 1536
+#define VXL_DENSITY_SEG_THREADS_PER_SM 1024  // 64 registers, no spills: 11.4 vs 15.0 ms at 1536 on dam10m
 #endif
 
 
@@ -1008,6 +1008,112 @@ __device__ __forceinline__ void walk27_half(const GridBox& g, const uint32_t* __
   }
 }
 
+// walk27 / walk27_half handing the candidates over kN at a time, in the same order:
+// f(js, n) with js[0..n) valid (the others repeat js[0]); before a cell's candidates,
+// fc(plane, end) with the cell's x-plane (dx + 1) and its end slot. A batch never spans two
+// cells (or two 32-slot windows), so n < kN only at a window's or cell's end.
+template <int kN, class FC, class F>
+__device__ __forceinline__ void walk27_n(const GridBox& g, const uint32_t* __restrict__ start, float px, float py,
+                                         float pz, uint32_t cx, uint32_t cy, uint32_t cz, float h, FC&& fc, F&& f) {
+  const float lx = g.minx + (float)cx * g.bin, ly = g.miny + (float)cy * g.bin, lz = g.minz + (float)cz * g.bin;
+  const float gxl = fmaxf(px - lx, 0.0f), gxr = fmaxf(lx + g.bin - px, 0.0f);
+  const float gyl = fmaxf(py - ly, 0.0f), gyr = fmaxf(ly + g.bin - py, 0.0f);
+  const float gzl = fmaxf(pz - lz, 0.0f), gzr = fmaxf(lz + g.bin - pz, 0.0f);
+  const float reach = h + g.bin * (1.0f / 1024.0f);
+  const float reach2 = reach * reach;
+  for (int dz = -1; dz <= 1; ++dz) {
+    const int z = (int)cz + dz;
+    if (z < 0 || z >= (int)g.nz) continue;
+    const float gz = dz < 0 ? gzl : (dz > 0 ? gzr : 0.0f);
+    const float dz2 = gz * gz;
+    for (int dy = -1; dy <= 1; ++dy) {
+      const int y = (int)cy + dy;
+      if (y < 0 || y >= (int)g.ny) continue;
+      const float gy = dy < 0 ? gyl : (dy > 0 ? gyr : 0.0f);
+      const float dyz2 = dz2 + gy * gy;
+      for (int dx = -1; dx <= 1; ++dx) {
+        const int x = (int)cx + dx;
+        if (x < 0 || x >= (int)g.nx) continue;
+        const float gx = dx < 0 ? gxl : (dx > 0 ? gxr : 0.0f);
+        if (dyz2 + gx * gx > reach2) continue;
+        const uint32_t idx = ((uint32_t)x * g.ny + (uint32_t)y) * g.nz + (uint32_t)z;
+        const uint32_t j1 = start[idx + 1];
+        fc((uint32_t)(dx + 1), j1);
+        for (uint32_t j = start[idx]; j < j1; j += kN) {
+          const uint32_t n = min(j1 - j, (uint32_t)kN);
+          uint32_t js[kN];
+#pragma unroll
+          for (int t = 0; t < kN; ++t) js[t] = (uint32_t)t < n ? j + t : j;
+          f(js, n);
+        }
+      }
+    }
+  }
+}
+
+template <int kN, class FC, class F>
+__device__ __forceinline__ void walk27_half_n(const GridBox& g, const uint32_t* __restrict__ start,
+                                              const uint32_t* __restrict__ halves, float px, float py, float pz,
+                                              uint32_t cx, uint32_t cy, uint32_t cz, float h, FC&& fc, F&& f) {
+  const float B = g.bin;
+  const float lx = g.minx + (float)cx * B, ly = g.miny + (float)cy * B, lz = g.minz + (float)cz * B;
+  const float gxl = fmaxf(px - lx, 0.0f), gxr = fmaxf(lx + B - px, 0.0f);
+  const float gyl = fmaxf(py - ly, 0.0f), gyr = fmaxf(ly + B - py, 0.0f);
+  const float gzl = fmaxf(pz - lz, 0.0f), gzr = fmaxf(lz + B - pz, 0.0f);
+  const float reach = h + B * (1.0f / 1024.0f);
+  const float reach2 = reach * reach;
+  const uint32_t bxs = half_reach_bits(px, lx, B, reach, cx + 1 == g.nx);
+  const uint32_t bys = half_reach_bits(py, ly, B, reach, cy + 1 == g.ny);
+  const uint32_t bzs = half_reach_bits(pz, lz, B, reach, cz + 1 == g.nz);
+  for (int dz = -1; dz <= 1; ++dz) {
+    const int z = (int)cz + dz;
+    if (z < 0 || z >= (int)g.nz) continue;
+    const float gz = dz < 0 ? gzl : (dz > 0 ? gzr : 0.0f);
+    const float dz2 = gz * gz;
+    const uint32_t zsel = (bzs >> (2 * (dz + 1))) & 3u;
+    for (int dy = -1; dy <= 1; ++dy) {
+      const int y = (int)cy + dy;
+      if (y < 0 || y >= (int)g.ny) continue;
+      const float gy = dy < 0 ? gyl : (dy > 0 ? gyr : 0.0f);
+      const float dyz2 = dz2 + gy * gy;
+      const uint32_t ysel = (bys >> (2 * (dy + 1))) & 3u;
+      for (int dx = -1; dx <= 1; ++dx) {
+        const int x = (int)cx + dx;
+        if (x < 0 || x >= (int)g.nx) continue;
+        const float gx = dx < 0 ? gxl : (dx > 0 ? gxr : 0.0f);
+        if (dyz2 + gx * gx > reach2) continue;
+        const uint32_t xsel = (bxs >> (2 * (dx + 1))) & 3u;
+        if (!xsel || !ysel || !zsel) continue;
+        const uint32_t idx = ((uint32_t)x * g.ny + (uint32_t)y) * g.nz + (uint32_t)z;
+        const uint32_t j0 = start[idx], j1 = start[idx + 1];
+        fc((uint32_t)(dx + 1), j1);
+        for (uint32_t base = j0 & ~31u; base < j1; base += 32) {
+          const uint4 hm = *reinterpret_cast<const uint4*>(halves + 4 * (base >> 5));
+          uint32_t m = half_select(xsel, hm.x) & half_select(ysel, hm.y) & half_select(zsel, hm.z);
+          if (j0 > base) m &= ~0u << (j0 - base);
+          if (j1 < base + 32) m &= (1u << (j1 - base)) - 1u;
+          while (m) {
+            uint32_t js[kN];
+            uint32_t n = 0;
+            js[0] = base + (uint32_t)(__ffs(m) - 1);
+#pragma unroll
+            for (int t = 0; t < kN; ++t) {
+              if (m) {
+                js[t] = base + (uint32_t)(__ffs(m) - 1);
+                m &= m - 1u;
+                ++n;
+              } else {
+                js[t] = js[0];
+              }
+            }
+            f(js, n);
+          }
+        }
+      }
+    }
+  }
+}
+
 // ---------------------------------------------------------------- grouped density walk
 //
 // Particles of one cell reach the same neighbour cells; when the cell budget has doubled
@@ -1524,13 +1630,59 @@ __global__ void __launch_bounds__(kBlock, VXL_DENSITY_THREADS_PER_SM / kBlock) k
           }
         }
       }
+      // Without provider walls: the same test and sums as `visit`, with the list entry
+      // formed from the walked cell's plane offset (kadd, set by cellhook before each cell).
+      uint32_t kadd = 0;
+      auto visit1 = [&](const uint32_t (&js)[1], uint32_t) {
+        const uint32_t j = js[0];
+        if (j == s) return;
+        const float4 pj = pos[j];
+        const float ddx = pi.x - pj.x, ddy = pi.y - pj.y, ddz = pi.z - pj.z;
+        const float r2 = ddx * ddx + ddy * ddy + ddz * ddz;
+        if (r2 <= h2) {
+          const float tt = h2 - r2;
+          const float w = k6 * tt * tt * tt;
+          bool rec = true;
+          if (fluid_i) {
+            if (pj.w > 0.0f) sum += w;
+            else sum_b += (-pj.w) * w;
+          } else if (pj.w > 0.0f) {
+            sum += pj.w * w;
+          } else {
+            rec = false;
+          }
+          if (rec) {
+            if (cnt < cap) {
+              __stcs(wp, (unsigned short)(j + kadd));  // streaming store: read once, by the force pass
+              wp += stride;
+            }
+            ++cnt;
+          }
+        }
+      };
+      // list entries of the cell about to be walked: (plane << 14) + slot - plane's first slot,
+      // the plane's first slot being that of cell (cx + pl - 1, max(cy - 1, 0), max(cz - 1, 0));
+      // a cell reaching 2^14 slots past it marks the list unusable (consumers walk again)
+      auto cellhook = [&](uint32_t pl, uint32_t jend) {
+        const uint32_t pb = cst[(cx + pl - 1u) * (g.ny * g.nz) + (cy > 0 ? cy - 1 : 0) * g.nz + (cz > 0 ? cz - 1 : 0)];
+        kadd = (pl << kListOffBits) - pb;
+        bad |= (jend > pb && jend - 1u - pb > kListOffMask) ? 1u : 0u;
+      };
       if (dry) {
       } else if (half_walk) {
-        walk27_half(g, cst, halves, pi.x, pi.y, pi.z, cx, cy, cz, h, [&](uint32_t j) {
-          if (j != s) visit(j);
-        });
+        if constexpr (kWalls) {
+          walk27_half(g, cst, halves, pi.x, pi.y, pi.z, cx, cy, cz, h, [&](uint32_t j) {
+            if (j != s) visit(j);
+          });
+        } else {
+          walk27_half_n<1>(g, cst, halves, pi.x, pi.y, pi.z, cx, cy, cz, h, cellhook, visit1);
+        }
       } else {
-        walk27<true>(g, cst, pi.x, pi.y, pi.z, cx, cy, cz, h, visit, s);
+        if constexpr (kWalls) {
+          walk27<true>(g, cst, pi.x, pi.y, pi.z, cx, cy, cz, h, visit, s);
+        } else {
+          walk27_n<1>(g, cst, pi.x, pi.y, pi.z, cx, cy, cz, h, cellhook, visit1);
+        }
       }
       nbr_n[s] = cnt | (bad ? kListBad : 0u);
       const float rho = fluid_i ? (mass * sum + sum_b) : ((-pi.w) * w0 + sum);

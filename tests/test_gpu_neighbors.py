@@ -43,7 +43,7 @@ def _compare_lists(g, o, label):
     return go, ge
 
 
-DENSITY = [0, 1]  # the per-particle walk and the grouped (segment) density kernel
+DENSITY = [0, 1]  # density kernels: per-particle walk, grouped segments
 
 
 def _lists_after(vxl, oracle_mod, spec, warm_ticks=0, substeps_before=0, density=0):

@@ -80,8 +80,8 @@ def test_backend_available(vxl):
 
 @pytest.mark.parametrize("density", [0, 1])
 def test_single_substep_bit_exact(vxl, oracle_mod, density):
-    """One substep from identical state: table, rho, p, a, xsph, bforce, pos, vel (with the
-    per-particle walk and with the grouped density kernel)."""
+    """One substep from identical state: table, rho, p, a, xsph, bforce, pos, vel (with each
+    density kernel)."""
     from vxl_sph import scenes
     spec = scenes.small_dam(n=(10, 12, 9), spacing=0.05, tank=(0.8, 0.7, 0.6))
     g, o = pair(vxl, oracle_mod, spec)
