@@ -1402,20 +1402,11 @@ void Engine::enqueue_substep(bool with_reactions) {
   // thread order of the density pass: x halves first per cell for the provider-wall variant;
   // otherwise octant-major per 256-slot chunk (and the segments of the grouped kernel)
   if (walls_any_) LAUNCH(KID_HALFMASK, k_e_xorder<<<148 * 8, kThreads, 0, st>>>(start_, ctl_d_, halves_, xorder_));
-#ifdef VXL_WALK_XORDER
-  else if (tuning_.density == 0) {
-    LAUNCH(KID_HALFMASK, k_e_xorder<<<148 * 8, kThreads, 0, st>>>(start_, ctl_d_, halves_, xorder_));
-  }
-#endif
   else
     LAUNCH(KID_GROUPS, k_e_groups<<<key_blocks, 256, 0, st>>>(p1, sc_d_, tiles_d_, ntiles_, ctl_d_, order_,
                                                               (uint2*)segs_));
   const uint32_t stride = (uint32_t)slot_cap_;
-#ifdef VXL_WALK_XORDER
-  const uint32_t* walk_order = xorder_;
-#else
   const uint32_t* walk_order = order_;
-#endif
   const bool rec = record_;
   const uint32_t per_tile = std::max<uint32_t>(ntiles_, 1);
   const uint32_t gd = grid_density_ ? (uint32_t)grid_density_ : per_tile;
