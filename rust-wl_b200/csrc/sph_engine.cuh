@@ -1087,10 +1087,16 @@ __device__ __forceinline__ void walk27_half_n(const GridBox& g, const uint32_t* 
         const uint32_t idx = ((uint32_t)x * g.ny + (uint32_t)y) * g.nz + (uint32_t)z;
         const uint32_t j0 = start[idx], j1 = start[idx + 1];
         fc((uint32_t)(dx + 1), j1);
-        for (uint32_t base = j0 & ~31u; base < j1; base += 32) {
-          const uint4 hm = *reinterpret_cast<const uint4*>(halves + 4 * (base >> 5));
-          uint32_t m = half_select(xsel, hm.x) & half_select(ysel, hm.y) & half_select(zsel, hm.z);
-          if (j0 > base) m &= ~0u << (j0 - base);
+        // windows of 32 slots from the cell's own first slot, the half masks read across two
+        // aligned words: lanes of one octant in different cells of similar contents then
+        // take the same number of trips through each window
+        for (uint32_t base = j0; base < j1; base += 32) {
+          const uint32_t sh = base & 31u;
+          const uint4 lo = *reinterpret_cast<const uint4*>(halves + 4 * (base >> 5));
+          const uint4 hi = *reinterpret_cast<const uint4*>(halves + 4 * (base >> 5) + 4);
+          const uint32_t ux = __funnelshift_r(lo.x, hi.x, sh), uy = __funnelshift_r(lo.y, hi.y, sh),
+                         uz = __funnelshift_r(lo.z, hi.z, sh);
+          uint32_t m = half_select(xsel, ux) & half_select(ysel, uy) & half_select(zsel, uz);
           if (j1 < base + 32) m &= (1u << (j1 - base)) - 1u;
           while (m) {
             uint32_t js[kN];
