@@ -1400,11 +1400,11 @@ void Engine::enqueue_substep(bool with_reactions) {
                                                        (float4*)vel_[1], orig_, slot_of_));
   LAUNCH(KID_HALFMASK, k_e_halfmask<<<key_blocks, kThreads, 0, st>>>(p1, sc_d_, tiles_d_, ntiles_, ctl_d_, halves_));
   // thread order of the density pass: x halves first per cell for the provider-wall variant;
-  // otherwise octant-major per 256-slot chunk (and the segments of the grouped kernel)
+  // otherwise octant-major per chunk of a tile (and the segments of the grouped kernel)
   if (walls_any_) LAUNCH(KID_HALFMASK, k_e_xorder<<<148 * 8, kThreads, 0, st>>>(start_, ctl_d_, halves_, xorder_));
   else
-    LAUNCH(KID_GROUPS, k_e_groups<<<key_blocks, 256, 0, st>>>(p1, sc_d_, tiles_d_, ntiles_, ctl_d_, order_,
-                                                              (uint2*)segs_));
+    LAUNCH(KID_GROUPS, k_e_groups<<<key_blocks, kGroupChunk, 0, st>>>(p1, sc_d_, tiles_d_, ntiles_, ctl_d_, order_,
+                                                                      (uint2*)segs_));
   const uint32_t stride = (uint32_t)slot_cap_;
   const uint32_t* walk_order = order_;
   const bool rec = record_;

@@ -1008,13 +1008,13 @@ __device__ __forceinline__ void walk27_half(const GridBox& g, const uint32_t* __
   }
 }
 
-// walk27 / walk27_half handing the candidates over kN at a time, in the same order:
-// f(js, n) with js[0..n) valid (the others repeat js[0]); before a cell's candidates,
-// fc(plane, end) with the cell's x-plane (dx + 1) and its end slot. A batch never spans two
-// cells (or two 32-slot windows), so n < kN only at a window's or cell's end.
-template <int kN, class FC, class F>
-__device__ __forceinline__ void walk27_n(const GridBox& g, const uint32_t* __restrict__ start, float px, float py,
-                                         float pz, uint32_t cx, uint32_t cy, uint32_t cz, float h, FC&& fc, F&& f) {
+// walk27 / walk27_half with a hook per cell and the slot `skip` left out: f(j) for every
+// candidate in the same order; before a cell's candidates, fc(plane, end) with the cell's
+// x-plane (dx + 1) and its end slot.
+template <class FC, class F>
+__device__ __forceinline__ void walk27_c(const GridBox& g, const uint32_t* __restrict__ start, float px, float py,
+                                         float pz, uint32_t cx, uint32_t cy, uint32_t cz, float h, uint32_t skip,
+                                         FC&& fc, F&& f) {
   const float lx = g.minx + (float)cx * g.bin, ly = g.miny + (float)cy * g.bin, lz = g.minz + (float)cz * g.bin;
   const float gxl = fmaxf(px - lx, 0.0f), gxr = fmaxf(lx + g.bin - px, 0.0f);
   const float gyl = fmaxf(py - ly, 0.0f), gyr = fmaxf(ly + g.bin - py, 0.0f);
@@ -1039,22 +1039,18 @@ __device__ __forceinline__ void walk27_n(const GridBox& g, const uint32_t* __res
         const uint32_t idx = ((uint32_t)x * g.ny + (uint32_t)y) * g.nz + (uint32_t)z;
         const uint32_t j1 = start[idx + 1];
         fc((uint32_t)(dx + 1), j1);
-        for (uint32_t j = start[idx]; j < j1; j += kN) {
-          const uint32_t n = min(j1 - j, (uint32_t)kN);
-          uint32_t js[kN];
-#pragma unroll
-          for (int t = 0; t < kN; ++t) js[t] = (uint32_t)t < n ? j + t : j;
-          f(js, n);
-        }
+        for (uint32_t j = start[idx]; j < j1; ++j)
+          if (j != skip) f(j);
       }
     }
   }
 }
 
-template <int kN, class FC, class F>
-__device__ __forceinline__ void walk27_half_n(const GridBox& g, const uint32_t* __restrict__ start,
+template <class FC, class F>
+__device__ __forceinline__ void walk27_half_c(const GridBox& g, const uint32_t* __restrict__ start,
                                               const uint32_t* __restrict__ halves, float px, float py, float pz,
-                                              uint32_t cx, uint32_t cy, uint32_t cz, float h, FC&& fc, F&& f) {
+                                              uint32_t cx, uint32_t cy, uint32_t cz, float h, uint32_t skip,
+                                              FC&& fc, F&& f) {
   const float B = g.bin;
   const float lx = g.minx + (float)cx * B, ly = g.miny + (float)cy * B, lz = g.minz + (float)cz * B;
   const float gxl = fmaxf(px - lx, 0.0f), gxr = fmaxf(lx + B - px, 0.0f);
@@ -1098,21 +1094,10 @@ __device__ __forceinline__ void walk27_half_n(const GridBox& g, const uint32_t* 
                          uz = __funnelshift_r(lo.z, hi.z, sh);
           uint32_t m = half_select(xsel, ux) & half_select(ysel, uy) & half_select(zsel, uz);
           if (j1 < base + 32) m &= (1u << (j1 - base)) - 1u;
+          if (skip - base < 32u) m &= ~(1u << (skip - base));  // once per window, not per candidate
           while (m) {
-            uint32_t js[kN];
-            uint32_t n = 0;
-            js[0] = base + (uint32_t)(__ffs(m) - 1);
-#pragma unroll
-            for (int t = 0; t < kN; ++t) {
-              if (m) {
-                js[t] = base + (uint32_t)(__ffs(m) - 1);
-                m &= m - 1u;
-                ++n;
-              } else {
-                js[t] = js[0];
-              }
-            }
-            f(js, n);
+            f(base + (uint32_t)(__ffs(m) - 1));
+            m &= m - 1u;
           }
         }
       }
@@ -1125,23 +1110,39 @@ __device__ __forceinline__ void walk27_half_n(const GridBox& g, const uint32_t* 
 // Particles of one cell reach the same neighbour cells; when the cell budget has doubled
 // the bins to 2h or more, particles of one octant of a cell (the same half along x, y and
 // z) also reach the same half-cells. The grouped density pass lets eight lanes of a warp
-// share one stream of candidates: k_e_groups orders each 256-slot chunk of a tile by
-// octant (a stable counting sort, so the slots of an octant stay ascending) into
-// order[], then cuts the runs of equal (cell, octant) into segments of at most
-// kSegLanes positions, appended to segs[] as (first position in order[], count |
+// share one stream of candidates: k_e_groups orders each chunk of a tile (up to
+// kGroupChunk slots) by octant (a stable counting sort, so the slots of an octant stay
+// ascending) into order[], then cuts the runs of equal (cell, octant) into segments of at
+// most kSegLanes positions, appended to segs[] as (first position in order[], count |
 // scene << 4); ctl->work[kWorkSegs] counts them. The order of segments in segs[] is
 // immaterial: each particle's sums are formed by one lane alone.
+//
+// The per-particle walk runs in order[] too: a warp whose lanes share one octant walks one
+// culled cell set. Octants follow one another in Gray-code order (0 1 3 2 6 7 5 4), so a
+// warp that straddles two octants walks the union of two sets that differ along one axis
+// only (12 cells instead of 8; up to 27 for octants apart in all three). A chunk holds 8
+// octant runs, 7 boundaries over kGroupChunk / 32 warps; chunks of 512 slots (tiles of 512)
+// let fewer warps straddle, but cost the grouping pass about as much as they save.
 
 constexpr uint32_t kSegLanes = 8;   // lanes (particles) per segment; four segments per warp
 constexpr uint32_t kSegQueue = 64;  // candidate ring per segment (pending never exceeds 7 + 32)
+#ifndef VXL_GROUP_CHUNK
+#define VXL_GROUP_CHUNK 256
+#endif
+constexpr uint32_t kGroupChunk = VXL_GROUP_CHUNK;  // slots per chunk = threads per block
+static_assert(kGroupChunk % 128 == 0 && kGroupChunk <= 1024, "chunk: 128..1024 slots, whole warps");
 
-__global__ void __launch_bounds__(256) k_e_groups(const float4* __restrict__ pos, const SceneDev* __restrict__ sc,
-                                                  const TileDev* __restrict__ tiles, uint32_t ntiles, EngineCtl* ctl,
-                                                  uint32_t* __restrict__ order, uint2* __restrict__ segs) {
+__device__ __forceinline__ uint32_t octant_rank(uint32_t oct) { return oct ^ (oct >> 1) ^ (oct >> 2); }
+
+__global__ void __launch_bounds__(kGroupChunk) k_e_groups(const float4* __restrict__ pos, const SceneDev* __restrict__ sc,
+                                                          const TileDev* __restrict__ tiles, uint32_t ntiles, EngineCtl* ctl,
+                                                          uint32_t* __restrict__ order, uint2* __restrict__ segs) {
   if (ctl->err & kErrCellCap) return;
-  __shared__ uint32_t s_cnt[8][8];  // [octant][warp]: slots per octant in each warp
-  __shared__ uint32_t s_cell[256], s_oct[256];
-  __shared__ uint32_t s_last[8], s_nseg[8], s_segbase;
+  constexpr uint32_t kW = kGroupChunk / 32;  // warps
+  constexpr uint32_t kV = 8 * kW / 32;       // (rank, warp) counts per lane of the scan
+  __shared__ uint32_t s_cnt[8 * kW];         // [octant rank][warp]: slots per octant in each warp
+  __shared__ uint32_t s_cell[kGroupChunk], s_oct[kGroupChunk];
+  __shared__ uint32_t s_last[kW], s_nseg[kW], s_segbase;
   const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const uint32_t lt = (1u << lane) - 1u;
   for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
@@ -1149,8 +1150,8 @@ __global__ void __launch_bounds__(256) k_e_groups(const float4* __restrict__ pos
     const GridBox g = sc[td.scene].g;
     const bool half = g.bin >= 2.0f * sc[td.scene].k.h;
     const float hb = g.bin * 0.5f;
-    for (uint32_t c0 = 0; c0 < td.count; c0 += 256) {
-      const uint32_t n = min(256u, td.count - c0);
+    for (uint32_t c0 = 0; c0 < td.count; c0 += kGroupChunk) {
+      const uint32_t n = min(kGroupChunk, td.count - c0);
       const uint32_t i = threadIdx.x;
       const bool valid = i < n;
       uint32_t cell = 0, oct = 0;
@@ -1163,29 +1164,38 @@ __global__ void __launch_bounds__(256) k_e_groups(const float4* __restrict__ pos
           oct = (p.x >= g.minx + (float)cx * g.bin + hb ? 1u : 0u) | (p.y >= g.miny + (float)cy * g.bin + hb ? 2u : 0u) |
                 (p.z >= g.minz + (float)cz * g.bin + hb ? 4u : 0u);
       }
+      const uint32_t key = octant_rank(oct);
       uint32_t rank = 0;
 #pragma unroll
       for (uint32_t o = 0; o < 8; ++o) {
-        const uint32_t b = __ballot_sync(0xffffffffu, valid && oct == o);
-        if (lane == 0) s_cnt[o][w] = __popc(b);
-        if (valid && oct == o) rank = __popc(b & lt);
+        const uint32_t b = __ballot_sync(0xffffffffu, valid && key == o);
+        if (lane == 0) s_cnt[o * kW + w] = __popc(b);
+        if (valid && key == o) rank = __popc(b & lt);
       }
       __syncthreads();
-      if (w == 0) {  // exclusive scan of the 64 counts in (octant, warp) order
-        const uint32_t a = s_cnt[lane >> 2][(lane & 3) * 2], b = s_cnt[lane >> 2][(lane & 3) * 2 + 1];
-        uint32_t v = a + b;
+      if (w == 0) {  // exclusive scan of the 8 * kW counts in (rank, warp) order
+        uint32_t v[kV], tot = 0;
+#pragma unroll
+        for (uint32_t k = 0; k < kV; ++k) {
+          v[k] = s_cnt[lane * kV + k];
+          tot += v[k];
+        }
+        uint32_t incl = tot;
 #pragma unroll
         for (int off = 1; off < 32; off <<= 1) {
-          const uint32_t u = __shfl_up_sync(0xffffffffu, v, off);
-          if ((int)lane >= off) v += u;
+          const uint32_t u = __shfl_up_sync(0xffffffffu, incl, off);
+          if ((int)lane >= off) incl += u;
         }
-        const uint32_t ex = v - a - b;
-        s_cnt[lane >> 2][(lane & 3) * 2] = ex;
-        s_cnt[lane >> 2][(lane & 3) * 2 + 1] = ex + a;
+        uint32_t ex = incl - tot;
+#pragma unroll
+        for (uint32_t k = 0; k < kV; ++k) {
+          s_cnt[lane * kV + k] = ex;
+          ex += v[k];
+        }
       }
       __syncthreads();
       if (valid) {
-        const uint32_t q = s_cnt[oct][w] + rank;
+        const uint32_t q = s_cnt[key * kW + w] + rank;
         order[td.first + c0 + q] = td.first + c0 + i;
         s_cell[q] = cell;
         s_oct[q] = oct;
@@ -1218,7 +1228,7 @@ __global__ void __launch_bounds__(256) k_e_groups(const float4* __restrict__ pos
       __syncthreads();
       if (threadIdx.x == 0) {
         uint32_t tot = 0;
-        for (int k = 0; k < 8; ++k) {
+        for (uint32_t k = 0; k < kW; ++k) {
           const uint32_t v = s_nseg[k];
           s_nseg[k] = tot;
           tot += v;
@@ -1639,9 +1649,7 @@ __global__ void __launch_bounds__(kBlock, VXL_DENSITY_THREADS_PER_SM / kBlock) k
       // Without provider walls: the same test and sums as `visit`, with the list entry
       // formed from the walked cell's plane offset (kadd, set by cellhook before each cell).
       uint32_t kadd = 0;
-      auto visit1 = [&](const uint32_t (&js)[1], uint32_t) {
-        const uint32_t j = js[0];
-        if (j == s) return;
+      auto visit1 = [&](uint32_t j) {  // j != s (the walks skip it)
         const float4 pj = pos[j];
         const float ddx = pi.x - pj.x, ddy = pi.y - pj.y, ddz = pi.z - pj.z;
         const float r2 = ddx * ddx + ddy * ddy + ddz * ddz;
@@ -1681,13 +1689,13 @@ __global__ void __launch_bounds__(kBlock, VXL_DENSITY_THREADS_PER_SM / kBlock) k
             if (j != s) visit(j);
           });
         } else {
-          walk27_half_n<1>(g, cst, halves, pi.x, pi.y, pi.z, cx, cy, cz, h, cellhook, visit1);
+          walk27_half_c(g, cst, halves, pi.x, pi.y, pi.z, cx, cy, cz, h, s, cellhook, visit1);
         }
       } else {
         if constexpr (kWalls) {
           walk27<true>(g, cst, pi.x, pi.y, pi.z, cx, cy, cz, h, visit, s);
         } else {
-          walk27_n<1>(g, cst, pi.x, pi.y, pi.z, cx, cy, cz, h, cellhook, visit1);
+          walk27_c(g, cst, pi.x, pi.y, pi.z, cx, cy, cz, h, s, cellhook, visit1);
         }
       }
       nbr_n[s] = cnt | (bad ? kListBad : 0u);
