@@ -445,11 +445,14 @@ def run_ours(args) -> None:
     sb["achieved_gbs"] = sb["bytes"] / (sb["ms"] / 1e3) / 1e9
     sb["frac"] = sb["achieved_gbs"] / peak
 
-    # e2e: the drop-in call pattern of FluidStepper::step through the C ABI, pinned host
-    # buffers. The backend owns the fluid state, so a step uploads the boundary segment
-    # (the reference's per-tick upload, crates/vxl-phys-gpu/src/pipeline/coupling.rs:20-50),
-    # steps one tick (the per-body reactions come back) and reads every position back (what
-    # a renderer or the host-side copy takes).
+    # e2e: the drop-in call pattern of the GPU tier's FluidStepper::step through the C ABI,
+    # pinned host buffers. The backend owns the fluid state, so a step uploads the boundary
+    # segment (the reference's per-tick upload, crates/vxl-phys-gpu/src/pipeline/coupling.rs:
+    # 20-50), enqueues the tick, takes the previous tick's positions while this one runs
+    # (the tier's deferred readback: Packet::run_deferred + take_deferred_state,
+    # crates/vxl-phys-gpu/src/pipeline.rs:603-609, pipeline/readback.rs:229-262), waits for
+    # this tick's per-body reactions and requests its positions. Every timed step's positions
+    # reach the host inside the timed region (the last one after the loop).
     nf, nb = spec.n_fluid, spec.n_boundary
     pin_bp = torch.empty((max(nb, 1), 3), dtype=torch.float32, pin_memory=True).numpy()[:nb]
     pin_bv = torch.empty((max(nb, 1), 3), dtype=torch.float32, pin_memory=True).numpy()[:nb]
@@ -458,28 +461,34 @@ def run_ours(args) -> None:
     pin_bv[:] = spec.vel[nf:]
     scene.set_profile(False)
 
-    def e2e_step():
-        if nb:
-            scene.upload_boundary(pin_bp, pin_bv)
-        scene.step_tick(dt_tick, spec.spans)
-        vxl_sph._check(scene.lib.vxl_sph_read_state(scene._h, vxl_sph._fptr(pin_p), None))
+    def e2e_steps(k: int) -> None:
+        for q in range(k):
+            if nb:
+                scene.upload_boundary(pin_bp, pin_bv)
+            scene.step_tick_async(dt_tick, spec.spans)
+            if q:
+                scene.take_state(pin_p)
+            scene.sync()
+            scene.request_state()
+        if k:
+            scene.take_state(pin_p)
 
     scene.write_state(spec.pos, spec.vel)
-    for _ in range(2):
-        e2e_step()
+    e2e_steps(2)
     scene.write_state(spec.pos, spec.vel)  # the timed steps start from the initial state too
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
     t0 = time.perf_counter()
-    for _ in range(args.steps):
-        e2e_step()
+    e2e_steps(args.steps)
     e2e_s = placement.max_over_ranks(time.perf_counter() - t0, dist, f"cuda:{local}")
     nspans = len(spec.spans)
     e2e = {"value": updates / e2e_s, "unit": UNIT, "h2d_bytes_per_step": nb * 24 + nspans * 24,
            "d2h_bytes_per_step": spec.n_total * 12 + nspans * 28,
-           "api": "vxl_sph_upload_boundary (boundary segment) + vxl_sph_step_tick (spans in, reactions out) + "
-                  "vxl_sph_read_state (positions), pinned host buffers: the FluidStepper::step pattern"}
+           "api": "vxl_sph_upload_boundary (boundary segment) + vxl_sph_step_tick_async (spans in) + "
+                  "vxl_sph_take_state (the previous tick's positions) + vxl_sph_sync (reactions out) + "
+                  "vxl_sph_request_state, pinned host buffers: the GPU tier's FluidStepper::step pattern "
+                  "with its deferred readback"}
 
     mix = {}
     if world == 1 and spec.meta.get("dynamic") and any(spec.meta["dynamic"]) and not args.no_coupled:

@@ -304,7 +304,9 @@ vxl_status vxl_sph_autotune(vxl_sph_handle* h, float dt_tick, uint32_t trials, v
  * after whatever is already enqueued on the handle's stream (e.g. vxl_sph_step_tick_async),
  * a copy of every particle's position (reference order; for a batch, scene after scene) into
  * a pinned buffer the handle owns and returns without waiting; take waits for that copy and
- * writes it out. The host's wait overlaps the tick: renderers draw the previous tick. */
+ * writes it out. The device-to-host copy runs on a stream of its own, so work enqueued after
+ * the request (the next tick) does not wait for it, and the host's wait overlaps the tick:
+ * renderers draw the previous tick. A second request waits for a copy not yet taken. */
 vxl_status vxl_sph_request_state(vxl_sph_handle* h);
 /* n: every particle of the handle (the sum over its scenes), as at the request. */
 vxl_status vxl_sph_take_state(vxl_sph_handle* h, float* pos_xyz, uint64_t n);

@@ -212,8 +212,14 @@ void Engine::free_all() {
     if (p) cudaFreeHost(p);
   if (snap_h_) cudaFreeHost(snap_h_);
   snap_h_ = nullptr;
+  if (snap_d_) cudaFree(snap_d_);
+  snap_d_ = nullptr;
   if (ev_snap_) cudaEventDestroy(ev_snap_);
   ev_snap_ = nullptr;
+  if (ev_snap_ready_) cudaEventDestroy(ev_snap_ready_);
+  ev_snap_ready_ = nullptr;
+  if (snap_stream_) cudaStreamDestroy(snap_stream_);
+  snap_stream_ = nullptr;
   if (rb_d_) cudaFree(rb_d_);
   rb_d_ = nullptr;
   void* wd[] = {prov_d_,      wplanes_d_,    pflag_,        pnsum_,        plist_,   pblk_,
@@ -1020,25 +1026,38 @@ vxl_status Engine::read_state(uint32_t q, float* pos, float* vel) {
 vxl_status Engine::request_state() {
   CU(cudaSetDevice(device_));
   const uint64_t n = used_;
+  if (!ev_snap_) CU(cudaEventCreateWithFlags(&ev_snap_, cudaEventDisableTiming));
+  if (!ev_snap_ready_) CU(cudaEventCreateWithFlags(&ev_snap_ready_, cudaEventDisableTiming));
+  if (!snap_stream_) CU(cudaStreamCreateWithFlags(&snap_stream_, cudaStreamNonBlocking));
+  if (snap_pending_) {  // a copy not yet taken still reads snap_d_ and writes snap_h_
+    CU(cudaEventSynchronize(ev_snap_));
+    snap_pending_ = false;
+  }
   if (n > snap_cap_) {
-    if (snap_pending_) {
-      cudaEventSynchronize(ev_snap_);
-      snap_pending_ = false;
-    }
     if (snap_h_) cudaFreeHost(snap_h_);
+    if (snap_d_) cudaFree(snap_d_);
     snap_h_ = nullptr;
+    snap_d_ = nullptr;
     snap_cap_ = 0;
     CU(cudaMallocHost((void**)&snap_h_, n * 12));
+    if (cudaMalloc((void**)&snap_d_, n * 12) != cudaSuccess) {
+      cudaGetLastError();
+      return set_error(VXL_OUT_OF_MEMORY, "no device memory for the state copy");
+    }
     snap_cap_ = n;
   }
-  if (!ev_snap_) CU(cudaEventCreateWithFlags(&ev_snap_, cudaEventDisableTiming));
+  // the positions in reference order are gathered behind the enqueued work on the handle's
+  // stream; the device-to-host copy then runs on a stream of its own, so the next tick's
+  // kernels do not wait for it
   if (n) {
-    k_e_read_scene<<<blocks_for(n), kThreads, 0, stream_>>>((const float4*)pos_[0], nullptr, orig_, stage_,
+    k_e_read_scene<<<blocks_for(n), kThreads, 0, stream_>>>((const float4*)pos_[0], nullptr, orig_, snap_d_,
                                                              nullptr, 0u, (uint32_t)n);
     CU(cudaGetLastError());
-    CU(cudaMemcpyAsync(snap_h_, stage_, n * 12, cudaMemcpyDeviceToHost, stream_));
   }
-  CU(cudaEventRecord(ev_snap_, stream_));
+  CU(cudaEventRecord(ev_snap_ready_, stream_));
+  CU(cudaStreamWaitEvent(snap_stream_, ev_snap_ready_, 0));
+  if (n) CU(cudaMemcpyAsync(snap_h_, snap_d_, n * 12, cudaMemcpyDeviceToHost, snap_stream_));
+  CU(cudaEventRecord(ev_snap_, snap_stream_));
   snap_n_ = n;
   snap_pending_ = true;
   return VXL_OK;

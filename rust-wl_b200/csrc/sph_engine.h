@@ -218,8 +218,10 @@ class Engine {
   vxl_status upload_tables();
   ContactTableDev ctab(int side) const;
   float* snap_h_ = nullptr;  // pinned, 3 floats per slot
+  float* snap_d_ = nullptr;  // device copy in reference order, the source of the host copy
   uint64_t snap_cap_ = 0, snap_n_ = 0;
-  cudaEvent_t ev_snap_ = nullptr;
+  cudaEvent_t ev_snap_ = nullptr, ev_snap_ready_ = nullptr;
+  cudaStream_t snap_stream_ = nullptr;  // the host copy runs here, beside the next tick's kernels
   bool snap_pending_ = false;
   float* stage_ = nullptr;  // 8 floats per slot: staging for host transfers
   // cells (cell_cap_ + 1)
