@@ -631,6 +631,26 @@ __device__ __forceinline__ void canon_cell(uint32_t b, uint32_t n, int lane, uin
       orig[dst] = it.x;
       slot_of[it.x] = dst;
     }
+  } else if (n <= (uint32_t)kCanonSmem / 2) {
+    // keys and source slots both staged, so the cell's entries are read from memory once
+    uint32_t* sslot = skeys + kCanonSmem / 2;
+    for (uint32_t e = lane; e < n; e += 32) {
+      const uint2 it = items[b + e];
+      skeys[e] = it.x;
+      sslot[e] = it.y;
+    }
+    __syncwarp();
+    for (uint32_t e = lane; e < n; e += 32) {
+      const uint32_t key = skeys[e], src = sslot[e];
+      uint32_t rank = 0;
+      for (uint32_t j = 0; j < n; ++j) rank += (skeys[j] < key) ? 1u : 0u;
+      const uint32_t dst = b + rank;
+      pos_out[dst] = pos_in[src];
+      vel_out[dst] = vel_in[src];
+      orig[dst] = key;
+      slot_of[key] = dst;
+    }
+    __syncwarp();
   } else if (n <= (uint32_t)kCanonSmem) {
     for (uint32_t e = lane; e < n; e += 32) skeys[e] = items[b + e].x;
     __syncwarp();

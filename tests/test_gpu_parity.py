@@ -264,9 +264,10 @@ def test_single_particle(vxl, oracle_mod):
 
 
 def test_one_crowded_cell_canon_paths(vxl, oracle_mod):
-    """Cells of > 32 and > 1024 particles take the shared-memory and global sort paths."""
+    """Cells of > 32, > 512 and > 1024 particles take the shared-memory sort paths (keys and
+    source slots staged; keys only) and the global one."""
     rng = np.random.default_rng(7)
-    for n in (200, 1500):
+    for n in (200, 800, 1500):
         pos = rng.uniform(0.0, 0.08, (n, 3)).astype(F32)
         _run_both(vxl, oracle_mod, _custom(vxl, pos, h=0.1), substeps=2)
 
