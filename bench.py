@@ -876,6 +876,9 @@ def run_ncu_case(args) -> None:
     else:
         spec = build_scene(args.workload)
     scene = vxl_sph.Scene(spec.params, spec.pos, spec.vel, spec.pmass, spec.n_fluid)
+    if args.ncu_density >= 0:
+        block, tile, waves, _ = scene.tuning()
+        scene.set_tuning(block, tile, waves, args.ncu_density)
     for _ in range(max(args.warmup, 1)):
         scene.step_tick(dt_tick, spec.spans)
     scene.close()
@@ -915,6 +918,8 @@ def main():
     ap.add_argument("--no-coupled", action="store_true", help="skip the coupled-bodies line of scenes with boxes")
     ap.add_argument("--cpu-threads", type=int, default=0, help="reference arm: host threads (default: all)")
     ap.add_argument("--ncu-case", action="store_true", help="build + warm-up ticks only (for ncu captures)")
+    ap.add_argument("--ncu-density", type=int, default=-1,
+                    help="ncu case: density kernel (0 walk, 1 grouped; default: the handle's)")
     ap.add_argument("--ncu-block", type=int, default=0,
                     help="ncu case of dam10m: an N^3 fluid block in the same tank (bins still doubled)")
     args = ap.parse_args()
