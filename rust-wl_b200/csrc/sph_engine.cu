@@ -1417,13 +1417,16 @@ void Engine::enqueue_substep(bool with_reactions) {
                                                                ntiles_, ctl_d_, (uint2*)items_));
   LAUNCH(KID_CANON, k_e_canon<<<148 * 8, 256, 0, st>>>((const uint2*)items_, start_, ctl_d_, p0, v0, (float4*)pos_[1],
                                                        (float4*)vel_[1], orig_, slot_of_));
-  LAUNCH(KID_HALFMASK, k_e_halfmask<<<key_blocks, kThreads, 0, st>>>(p1, sc_d_, tiles_d_, ntiles_, ctl_d_, halves_));
-  // thread order of the density pass: x halves first per cell for the provider-wall variant;
-  // otherwise octant-major per chunk of a tile (and the segments of the grouped kernel)
-  if (walls_any_) LAUNCH(KID_HALFMASK, k_e_xorder<<<148 * 8, kThreads, 0, st>>>(start_, ctl_d_, halves_, xorder_));
-  else
+  // half-cell masks and the thread order of the density pass: for the provider-wall variant
+  // the masks, then x halves first per cell; otherwise the masks with the octant-major order
+  // per chunk of a tile (and the segments of the grouped kernel) in one pass
+  if (walls_any_) {
+    LAUNCH(KID_HALFMASK, k_e_halfmask<<<key_blocks, kThreads, 0, st>>>(p1, sc_d_, tiles_d_, ntiles_, ctl_d_, halves_));
+    LAUNCH(KID_HALFMASK, k_e_xorder<<<148 * 8, kThreads, 0, st>>>(start_, ctl_d_, halves_, xorder_));
+  } else {
     LAUNCH(KID_GROUPS, k_e_groups<<<key_blocks, kGroupChunk, 0, st>>>(p1, sc_d_, tiles_d_, ntiles_, ctl_d_, order_,
-                                                                      (uint2*)segs_));
+                                                                      (uint2*)segs_, halves_));
+  }
   const uint32_t stride = (uint32_t)slot_cap_;
   const uint32_t* walk_order = order_;
   const bool rec = record_;

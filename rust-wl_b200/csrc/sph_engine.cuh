@@ -1156,7 +1156,8 @@ __device__ __forceinline__ uint32_t octant_rank(uint32_t oct) { return oct ^ (oc
 
 __global__ void __launch_bounds__(kGroupChunk) k_e_groups(const float4* __restrict__ pos, const SceneDev* __restrict__ sc,
                                                           const TileDev* __restrict__ tiles, uint32_t ntiles, EngineCtl* ctl,
-                                                          uint32_t* __restrict__ order, uint2* __restrict__ segs) {
+                                                          uint32_t* __restrict__ order, uint2* __restrict__ segs,
+                                                          uint32_t* __restrict__ halves) {
   if (ctl->err & kErrCellCap) return;
   constexpr uint32_t kW = kGroupChunk / 32;  // warps
   constexpr uint32_t kV = 8 * kW / 32;       // (rank, warp) counts per lane of the scan
@@ -1165,24 +1166,56 @@ __global__ void __launch_bounds__(kGroupChunk) k_e_groups(const float4* __restri
   __shared__ uint32_t s_last[kW], s_nseg[kW], s_segbase;
   const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const uint32_t lt = (1u << lane) - 1u;
-  for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
-    const TileDev td = tiles[t];
+  // the block's chunks one after another, each one's positions loaded while the previous
+  // one is sorted
+  uint32_t t = blockIdx.x, c1 = 0;
+  TileDev tn = t < ntiles ? tiles[t] : TileDev{};
+  float4 pn = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  if (t < ntiles && threadIdx.x < tn.count) pn = pos[tn.first + threadIdx.x];
+  while (t < ntiles) {  // uniform over the block
+    const TileDev td = tn;
+    const uint32_t c0 = c1;
+    const float4 p = pn;
+    c1 += kGroupChunk;
+    if (c1 >= tn.count) {
+      t += gridDim.x;
+      c1 = 0;
+      if (t < ntiles) tn = tiles[t];
+    }
+    if (t < ntiles && c1 + threadIdx.x < tn.count) pn = pos[tn.first + c1 + threadIdx.x];
     const GridBox g = sc[td.scene].g;
     const bool half = g.bin >= 2.0f * sc[td.scene].k.h;
     const float hb = g.bin * 0.5f;
-    for (uint32_t c0 = 0; c0 < td.count; c0 += kGroupChunk) {
+    {
       const uint32_t n = min(kGroupChunk, td.count - c0);
       const uint32_t i = threadIdx.x;
       const bool valid = i < n;
       uint32_t cell = 0, oct = 0;
       if (valid) {
-        const float4 p = pos[td.first + c0 + i];
         uint32_t cx, cy, cz;
         bin_of(g, p.x, p.y, p.z, cx, cy, cz);
         cell = (cx * g.ny + cy) * g.nz + cz;
         if (half)
           oct = (p.x >= g.minx + (float)cx * g.bin + hb ? 1u : 0u) | (p.y >= g.miny + (float)cy * g.bin + hb ? 2u : 0u) |
                 (p.z >= g.minz + (float)cz * g.bin + hb ? 4u : 0u);
+      }
+      // the half-cell masks of the density walk (what k_e_halfmask writes for the scenes
+      // with provider walls): bit (s & 31) of halves[4 (s >> 5) + a] for the upper half
+      if (half) {
+        const uint32_t active = __ballot_sync(0xffffffffu, valid);
+        if (valid) {
+          const uint32_t s = td.first + c0 + i;
+          const uint32_t blk = s >> 5, bit = 1u << (s & 31);
+          const uint32_t peers = __match_any_sync(active, blk);
+          const uint32_t mx = __reduce_or_sync(peers, (oct & 1u) ? bit : 0u);
+          const uint32_t my = __reduce_or_sync(peers, (oct & 2u) ? bit : 0u);
+          const uint32_t mz = __reduce_or_sync(peers, (oct & 4u) ? bit : 0u);
+          if (lane == __ffs(peers) - 1) {
+            if (mx) atomicOr(&halves[4 * blk], mx);
+            if (my) atomicOr(&halves[4 * blk + 1], my);
+            if (mz) atomicOr(&halves[4 * blk + 2], mz);
+          }
+        }
       }
       const uint32_t key = octant_rank(oct);
       uint32_t rank = 0;
