@@ -1709,16 +1709,14 @@ __global__ void __launch_bounds__(kBlock, VXL_DENSITY_THREADS_PER_SM / kBlock) k
         if (r2 <= h2) {
           const float tt = h2 - r2;
           const float w = k6 * tt * tt * tt;
-          bool rec = true;
-          if (fluid_i) {
-            if (pj.w > 0.0f) sum += w;
-            else sum_b += (-pj.w) * w;
-          } else if (pj.w > 0.0f) {
-            sum += pj.w * w;
-          } else {
-            rec = false;
-          }
-          if (rec) {
+          // the neighbour's class selected, not branched on (the same sums: an unselected
+          // term is not added)
+          const bool fj = pj.w > 0.0f;
+          const float tf = fluid_i ? w : pj.w * w;
+          const float tb = (-pj.w) * w;
+          sum = fj ? sum + tf : sum;
+          sum_b = (fluid_i && !fj) ? sum_b + tb : sum_b;
+          if (fj || fluid_i) {
             if (cnt < cap) {
               __stcs(wp, (unsigned short)(j + kadd));  // streaming store: read once, by the force pass
               wp += stride;
