@@ -42,7 +42,7 @@ UNIT = "particle-updates/s"
 FALLBACK_HBM_GBS = 6650.0
 # Kernels launched on the handle's second stream beside k_force: their event-timed spans
 # include waiting for SMs that k_force holds, so they are not costs and are listed apart.
-SIDE_STREAM = ("k_bforce", "k_react_chunks", "k_react_spans")
+SIDE_STREAM = ("k_bforce", "k_react_long", "k_react_spans")
 
 # Algorithmic bytes per launch of each substep kernel (per particle unless noted), the
 # per-unit figures of the byte model B = 116 N_t + 72 N_f + 40 N_b + 8 C per substep:

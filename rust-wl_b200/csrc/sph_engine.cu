@@ -33,12 +33,12 @@ inline uint32_t blocks_for(uint64_t n, int t = kThreads) { return (uint32_t)((n 
 
 enum KernelId : int {
   KID_CELLOFF, KID_KEYS, KID_SCAN_PARTIAL, KID_SCAN_FINAL, KID_PLACE, KID_CANON,
-  KID_DENSITY, KID_FORCE, KID_BFORCE, KID_REACT_CHUNKS, KID_REACT_SPANS, KID_SCALE, KID_HALFMASK, KID_WALLS,
+  KID_DENSITY, KID_FORCE, KID_BFORCE, KID_REACT_LONG, KID_REACT_SPANS, KID_SCALE, KID_HALFMASK, KID_WALLS,
   KID_GROUPS, KID_COUNT
 };
 const char* const kKernelNames[KID_COUNT] = {
     "k_celloff", "k_keys", "k_scan_partial", "k_scan_final", "k_place", "k_canon",
-    "k_density", "k_force", "k_bforce", "k_react_chunks", "k_react_spans", "k_scale", "k_halfmask", "k_walls",
+    "k_density", "k_force", "k_bforce", "k_react_long", "k_react_spans", "k_scale", "k_halfmask", "k_walls",
     "k_groups"};
 constexpr int kSegWarps = 8;  // warps per block of the grouped density pass
 
@@ -129,6 +129,9 @@ vxl_status Engine::create(int device, uint64_t slot_cap, uint64_t cell_cap, uint
   if (ce == cudaSuccess) ce = cudaStreamCreateWithFlags(&e->side_, cudaStreamNonBlocking);
   if (ce == cudaSuccess) ce = cudaEventCreateWithFlags(&e->ev_fork_, cudaEventDisableTiming);
   if (ce == cudaSuccess) ce = cudaEventCreateWithFlags(&e->ev_join_, cudaEventDisableTiming);
+  if (ce == cudaSuccess) ce = cudaStreamCreateWithFlags(&e->react_, cudaStreamNonBlocking);
+  if (ce == cudaSuccess) ce = cudaEventCreateWithFlags(&e->ev_rfork_, cudaEventDisableTiming);
+  if (ce == cudaSuccess) ce = cudaEventCreateWithFlags(&e->ev_rjoin_, cudaEventDisableTiming);
   if (ce != cudaSuccess) {
     cudaGetLastError();
     delete e;  // the destructor releases tiles_h_
@@ -204,10 +207,10 @@ void Engine::free_all() {
   graph_ = nullptr;
   void* d[] = {pos_[0], pos_[1], vel_[0], vel_[1], orig_, slot_of_, cellrank_, items_, rc_, press_, acc_, xsph_,
                bforce_, bpos_, nbr_, nbr_n_, halves_, xorder_, order_, segs_, stage_, counts_, wet_, start_, partial_, sc_d_, tiles_d_, ctl_d_, spans_d_,
-               chunks_d_, chunk_first_d_, react_partial_, breact_d_};
+               chunks_d_, breact_d_};
   for (void* p : d)
     if (p) cudaFree(p);
-  void* hp[] = {sc_h_, ctl_h_, spans_h_, chunks_h_, chunk_first_h_, breact_h_};
+  void* hp[] = {sc_h_, ctl_h_, spans_h_, chunks_h_, breact_h_};
   for (void* p : hp)
     if (p) cudaFreeHost(p);
   if (snap_h_) cudaFreeHost(snap_h_);
@@ -248,12 +251,18 @@ void Engine::free_all() {
   if (ev_fork_) cudaEventDestroy(ev_fork_);
   if (ev_join_) cudaEventDestroy(ev_join_);
   ev_fork_ = ev_join_ = nullptr;
+  if (react_) cudaStreamDestroy(react_);
+  react_ = nullptr;
+  if (ev_rfork_) cudaEventDestroy(ev_rfork_);
+  if (ev_rjoin_) cudaEventDestroy(ev_rjoin_);
+  ev_rfork_ = ev_rjoin_ = nullptr;
 }
 
 Engine::~Engine() {
   cudaSetDevice(device_);
   if (stream_) cudaStreamSynchronize(stream_);
   if (side_) cudaStreamSynchronize(side_);
+  if (react_) cudaStreamSynchronize(react_);
   free_all();
   delete tiles_h_;
 }
@@ -848,7 +857,8 @@ vxl_status Engine::set_providers(uint32_t q, const vxl_sph_provider* pr, uint32_
 vxl_status Engine::stage_walls() {
   CU(cudaStreamSynchronize(stream_));
   if (side_) CU(cudaStreamSynchronize(side_));
-  side_pending_ = false;
+  if (react_) CU(cudaStreamSynchronize(react_));
+  side_pending_ = react_pending_ = false;
   std::vector<ProviderDev> hp;
   std::vector<WallPlaneDev> hw;
   prov_first_st_.assign(scenes_.size(), 0u);
@@ -1241,7 +1251,6 @@ vxl_status Engine::stage_spans() {
   CU(cudaStreamSynchronize(stream_));
   std::vector<SpanDev> sp;
   std::vector<SpanChunk> ch;
-  std::vector<uint32_t> first;
   span_scene_.clear();
   for (uint32_t q = 0; q < scenes_.size() && q < spans_local_.size(); ++q)
     for (const vxl_sph_span& s : spans_local_[q]) {
@@ -1256,38 +1265,31 @@ vxl_status Engine::stage_spans() {
           }
       sp.push_back(SpanDev{s.body, s.origin[0], s.origin[1], s.origin[2], gs, ge, rigid});
       span_scene_.push_back(q);
-      first.push_back((uint32_t)ch.size());
-      if (ge - gs > kReactExactSpan)  // larger spans take the two-level reduction
-        for (uint32_t b = gs; b < ge; b += kReactChunk) ch.push_back(SpanChunk{idx, b, std::min(ge, b + kReactChunk), 0u});
+      if (ge - gs > kReactExactSpan) ch.push_back(SpanChunk{idx, gs, ge, 0u});  // a block of its own
     }
-  first.push_back((uint32_t)ch.size());
   const uint32_t ns = (uint32_t)sp.size(), nc = (uint32_t)ch.size();
   if (!spans_h_ || ns > spans_cap_ || nc > chunks_cap_) {
-    void* d[] = {spans_d_, chunks_d_, chunk_first_d_, react_partial_, breact_d_};
+    void* d[] = {spans_d_, chunks_d_, breact_d_};
     for (void* p : d)
       if (p) cudaFree(p);
-    void* hp[] = {spans_h_, chunks_h_, chunk_first_h_, breact_h_};
+    void* hp[] = {spans_h_, chunks_h_, breact_h_};
     for (void* p : hp)
       if (p) cudaFreeHost(p);
-    spans_d_ = nullptr; chunks_d_ = nullptr; chunk_first_d_ = nullptr; react_partial_ = nullptr; breact_d_ = nullptr;
-    spans_h_ = nullptr; chunks_h_ = nullptr; chunk_first_h_ = nullptr; breact_h_ = nullptr;
+    spans_d_ = nullptr; chunks_d_ = nullptr; breact_d_ = nullptr;
+    spans_h_ = nullptr; chunks_h_ = nullptr; breact_h_ = nullptr;
     const uint32_t cap = std::max<uint32_t>(ns, 64), ccap = std::max<uint32_t>(nc, 256);
     vxl_status s;
     if ((s = dalloc(&spans_d_, cap)) != VXL_OK) return s;
     if ((s = dalloc(&chunks_d_, ccap)) != VXL_OK) return s;
-    if ((s = dalloc(&chunk_first_d_, (size_t)cap + 1)) != VXL_OK) return s;
-    if ((s = dalloc(&react_partial_, (size_t)ccap * 6)) != VXL_OK) return s;
     if ((s = dalloc(&breact_d_, (size_t)cap * 6)) != VXL_OK) return s;
     CU(cudaMallocHost((void**)&spans_h_, cap * sizeof(SpanDev)));
     CU(cudaMallocHost((void**)&chunks_h_, ccap * sizeof(SpanChunk)));
-    CU(cudaMallocHost((void**)&chunk_first_h_, (cap + 1) * sizeof(uint32_t)));
     CU(cudaMallocHost((void**)&breact_h_, cap * 6 * sizeof(float)));
     spans_cap_ = cap;
     chunks_cap_ = ccap;
   }
   if (ns) std::memcpy(spans_h_, sp.data(), ns * sizeof(SpanDev));
   if (nc) std::memcpy(chunks_h_, ch.data(), nc * sizeof(SpanChunk));
-  std::memcpy(chunk_first_h_, first.data(), first.size() * sizeof(uint32_t));
   nspans_ = ns;
   nchunks_ = nc;
   spans_dirty_ = false;
@@ -1320,10 +1322,18 @@ void Engine::prof_end(int i, cudaStream_t st) {
   if (i >= 0) record_event(prof_ev_[2 * i + 1], st);
 }
 
-void Engine::join_side() {
+void Engine::join_side_only() {
   if (side_pending_) {
     cudaStreamWaitEvent(stream_, ev_join_, 0);
     side_pending_ = false;
+  }
+}
+
+void Engine::join_side() {
+  join_side_only();
+  if (react_pending_) {
+    cudaStreamWaitEvent(stream_, ev_rjoin_, 0);
+    react_pending_ = false;
   }
 }
 
@@ -1404,9 +1414,10 @@ void Engine::enqueue_substep(bool with_reactions) {
   const float4* v0 = (const float4*)vel_[0];
   const float4* p1 = (const float4*)pos_[1];
   const float4* v1 = (const float4*)vel_[1];
-  // The previous substep's reaction branch reads this substep's inputs-to-be (scene grids,
-  // cell table, sorted buffer, permutation, lists, work counters): join it first.
-  join_side();
+  // The previous substep's boundary-force pass reads this substep's inputs-to-be (scene
+  // grids, cell table, sorted buffer, permutation, lists, work counters): join it first.
+  // Its reaction sums read only bforce / bpos and go on beside this substep.
+  join_side_only();
   LAUNCH(KID_CELLOFF, k_e_celloff<<<1, 1024, 0, st>>>(sc_d_, S, ctl_d_, (uint32_t)cell_cap_));
   LAUNCH(KID_KEYS, k_e_keys<<<key_blocks, kThreads, 0, st>>>(p0, sc_d_, tiles_d_, ntiles_, ctl_d_, counts_,
                                                              (uint2*)cellrank_, halves_,
@@ -1463,25 +1474,30 @@ void Engine::enqueue_substep(bool with_reactions) {
   if (bforce || react) {
     cudaEventRecord(ev_fork_, st);
     cudaStreamWaitEvent(side_, ev_fork_, 0);
+    if (react_pending_) {  // the previous substep's sums still read bforce
+      cudaStreamWaitEvent(side_, ev_rjoin_, 0);
+      react_pending_ = false;
+    }
     if (bforce)
       LAUNCH_ON(KID_BFORCE, side_,
                 k_e_bforce<<<gb, 128, 0, side_>>>(p1, v1, (const float2*)rc_, start_, orig_, nbr_, nbr_n_, nbr_cap_,
                                                   stride, sc_d_, slot_of_, tiles_d_ + ntiles_, nbtiles_, ctl_d_,
                                                   (float4*)bforce_));
-    if (react) {
-      if (nchunks_)
-        LAUNCH_ON(KID_REACT_CHUNKS, side_,
-                k_react_chunks<<<nchunks_, kReactThreads, 0, side_>>>((const float4*)bforce_, (const float4*)bpos_,
-                                                                      spans_d_, chunks_d_, rb_d_, ctl_d_,
-                                                                      react_partial_));
-      LAUNCH_ON(KID_REACT_SPANS, side_,
-                k_react_spans<<<(nspans_ + kReactSpanWarps - 1) / kReactSpanWarps, 32 * kReactSpanWarps, 0, side_>>>(react_partial_, chunk_first_d_,
-                                                                         (const float4*)bforce_, (const float4*)bpos_,
-                                                                         spans_d_, rb_d_, ctl_d_,
-                                                                         breact_d_, nspans_));
-    }
     cudaEventRecord(ev_join_, side_);
     side_pending_ = true;
+    if (react) {
+      cudaEventRecord(ev_rfork_, side_);
+      cudaStreamWaitEvent(react_, ev_rfork_, 0);
+      if (nchunks_)  // the long spans (tank walls), a block each
+        LAUNCH_ON(KID_REACT_LONG, react_,
+                  k_react_long<<<nchunks_, kReactThreads, 0, react_>>>((const float4*)bforce_, (const float4*)bpos_,
+                                                                       spans_d_, chunks_d_, rb_d_, ctl_d_, breact_d_));
+      LAUNCH_ON(KID_REACT_SPANS, react_,
+                k_react_spans<<<(nspans_ + kReactSpanWarps - 1) / kReactSpanWarps, 32 * kReactSpanWarps, 0, react_>>>(
+                    (const float4*)bforce_, (const float4*)bpos_, spans_d_, rb_d_, ctl_d_, breact_d_, nspans_));
+      cudaEventRecord(ev_rjoin_, react_);
+      react_pending_ = true;
+    }
   }
   if (tuning_.block == 128)
     LAUNCH(KID_FORCE, k_e_force<128><<<gf, 128, 0, st>>>(
@@ -1518,7 +1534,6 @@ void Engine::enqueue_tick(float /*dt_tick*/) {
   if (nspans_ > 0) {
     cudaMemcpyAsync(spans_d_, spans_h_, nspans_ * sizeof(SpanDev), cudaMemcpyHostToDevice, st);
     if (nchunks_) cudaMemcpyAsync(chunks_d_, chunks_h_, nchunks_ * sizeof(SpanChunk), cudaMemcpyHostToDevice, st);
-    cudaMemcpyAsync(chunk_first_d_, chunk_first_h_, (nspans_ + 1) * sizeof(uint32_t), cudaMemcpyHostToDevice, st);
     cudaMemsetAsync(breact_d_, 0, nspans_ * 6 * sizeof(float), st);
   }
   for (uint32_t s = 0; s < sub; ++s) enqueue_substep(true);

@@ -99,10 +99,11 @@ struct SpanChunk {
   uint32_t span, begin, end, pad;
 };
 
-constexpr uint32_t kReactChunk = 4096;
-// Spans of at most this many particles (bodies, as opposed to tank walls) are summed in
-// index order: the reference's sum, bit for bit.
+// Spans of at most this many particles (bodies) are summed by one warp each; larger ones
+// (tank walls) by one block each. Both add the terms in index order: the reference's sum,
+// bit for bit.
 constexpr uint32_t kReactExactSpan = 8192;
+constexpr uint32_t kReactBatch = 1024;  // terms a block stages per step of a long span
 constexpr int kReactThreads = 256;
 constexpr int kReactSpanWarps = 2;  // spans per block of k_react_spans (one warp each)
 
@@ -2280,10 +2281,8 @@ __global__ void __launch_bounds__(128) k_e_bforce(
 // and form each one's force and torque terms, then lane a (a < 6) adds component a of the
 // 32 terms to its running sum in index order — six independent sequential sums, with the
 // loads of a batch in flight together instead of one at a time. Larger spans (tank walls)
-// take a fixed-shape two-level reduction, deterministic run to run: level 1, one block per
-// chunk of <= kReactChunk consecutive particles (thread t sums t, t + blockDim, ... in
-// order, then a fixed tree); level 2, the span's warp adds its chunk partials in chunk
-// order. Span ranges are global reference indices.
+// take one block each (k_react_long), the same sums in the same order with the next
+// batch's loads overlapping them. Span ranges are global reference indices.
 
 // Torque origin of a span: its coupled rigid body's position, or the origin it was given.
 __device__ __forceinline__ void span_origin(const SpanDev& sp, const RigidBodyDev* __restrict__ rb, float& ox,
@@ -2299,44 +2298,71 @@ __device__ __forceinline__ void span_origin(const SpanDev& sp, const RigidBodyDe
   }
 }
 
-__global__ void __launch_bounds__(kReactThreads) k_react_chunks(const float4* __restrict__ bforce,
-                                                                const float4* __restrict__ bpos,
-                                                                const SpanDev* __restrict__ spans,
-                                                                const SpanChunk* __restrict__ chunks,
-                                                                const RigidBodyDev* __restrict__ rb,
-                                                                const EngineCtl* __restrict__ ctl,
-                                                                float* __restrict__ partial) {
+// A span above kReactExactSpan, one block per span: the block stages the force and torque
+// terms of kReactBatch consecutive particles in shared memory while thread a (a < 6) adds
+// component a of the previous batch to its running sum in index order, so the loads of
+// the next batch are in flight during the sequential sums.
+__global__ void __launch_bounds__(kReactThreads) k_react_long(const float4* __restrict__ bforce,
+                                                              const float4* __restrict__ bpos,
+                                                              const SpanDev* __restrict__ spans,
+                                                              const SpanChunk* __restrict__ longs,
+                                                              const RigidBodyDev* __restrict__ rb,
+                                                              const EngineCtl* __restrict__ ctl,
+                                                              float* __restrict__ breact) {
   if (ctl->err & kErrCellCap) return;
-  const SpanChunk ch = chunks[blockIdx.x];
+  __shared__ float terms[2][6][kReactBatch];
+  const SpanChunk ch = longs[blockIdx.x];
   SpanDev sp = spans[ch.span];
   span_origin(sp, rb, sp.ox, sp.oy, sp.oz);
-  float f[6] = {0, 0, 0, 0, 0, 0};
-  for (uint32_t kk = ch.begin + threadIdx.x; kk < ch.end; kk += kReactThreads) {
-    const float4 fk = bforce[kk];
-    const float4 p = bpos[kk];
-    const float rx = p.x - sp.ox, ry = p.y - sp.oy, rz = p.z - sp.oz;
-    f[0] = f[0] + fk.x;
-    f[1] = f[1] + fk.y;
-    f[2] = f[2] + fk.z;
-    f[3] = f[3] + (ry * fk.z - rz * fk.y);
-    f[4] = f[4] + (rz * fk.x - rx * fk.z);
-    f[5] = f[5] + (rx * fk.y - ry * fk.x);
-  }
-  __shared__ float sh[6][kReactThreads];
-  for (int a = 0; a < 6; ++a) sh[a][threadIdx.x] = f[a];
+  auto stage = [&](uint32_t b0, uint32_t buf) {
+    for (uint32_t t = threadIdx.x; t < kReactBatch; t += kReactThreads) {
+      const uint32_t kk = b0 + t;
+      if (kk < sp.end) {
+        const float4 fk = bforce[kk];
+        const float4 p = bpos[kk];
+        const float rx = p.x - sp.ox, ry = p.y - sp.oy, rz = p.z - sp.oz;
+        terms[buf][0][t] = fk.x;
+        terms[buf][1][t] = fk.y;
+        terms[buf][2][t] = fk.z;
+        terms[buf][3][t] = ry * fk.z - rz * fk.y;
+        terms[buf][4][t] = rz * fk.x - rx * fk.z;
+        terms[buf][5][t] = rx * fk.y - ry * fk.x;
+      }
+    }
+  };
+  float f = 0.0f;  // thread a < 6: component a (force xyz, torque xyz)
+  uint32_t buf = 0;
+  stage(sp.start, 0);
   __syncthreads();
-  for (uint32_t w = kReactThreads / 2; w > 0; w >>= 1) {
-    if (threadIdx.x < w)
-      for (int a = 0; a < 6; ++a) sh[a][threadIdx.x] = sh[a][threadIdx.x] + sh[a][threadIdx.x + w];
+  for (uint32_t b0 = sp.start; b0 < sp.end; b0 += kReactBatch) {
+    if (b0 + kReactBatch < sp.end) stage(b0 + kReactBatch, buf ^ 1u);
+    if (threadIdx.x < 6) {
+      const uint32_t nb = min(kReactBatch, sp.end - b0);
+      const float* tt = terms[buf][threadIdx.x];
+      uint32_t t = 0;
+      for (; t + 16 <= nb; t += 16) {  // 16 terms loaded together, then added one by one
+        float v[16];
+#pragma unroll
+        for (int i = 0; i < 16; i += 4) {
+          const float4 q = *reinterpret_cast<const float4*>(tt + t + i);
+          v[i] = q.x;
+          v[i + 1] = q.y;
+          v[i + 2] = q.z;
+          v[i + 3] = q.w;
+        }
+#pragma unroll
+        for (int i = 0; i < 16; ++i) f = f + v[i];
+      }
+      for (; t < nb; ++t) f = f + tt[t];
+    }
     __syncthreads();
+    buf ^= 1u;
   }
-  if (threadIdx.x < 6) partial[6 * blockIdx.x + threadIdx.x] = sh[threadIdx.x][0];
+  if (threadIdx.x < 6) breact[6 * ch.span + threadIdx.x] = breact[6 * ch.span + threadIdx.x] + f;
 }
 
-// chunk_first[q] .. chunk_first[q + 1]: the chunks of span q (in order; none for a span
-// summed exactly).
-__global__ void k_react_spans(const float* __restrict__ partial, const uint32_t* __restrict__ chunk_first,
-                              const float4* __restrict__ bforce, const float4* __restrict__ bpos,
+// Spans of at most kReactExactSpan particles, one warp each (the others: k_react_long).
+__global__ void k_react_spans(const float4* __restrict__ bforce, const float4* __restrict__ bpos,
                               const SpanDev* __restrict__ spans, const RigidBodyDev* __restrict__ rb,
                               const EngineCtl* __restrict__ ctl, float* __restrict__ breact, uint32_t nspans) {
   if (ctl->err & kErrCellCap) return;
@@ -2346,8 +2372,9 @@ __global__ void k_react_spans(const float* __restrict__ partial, const uint32_t*
   if (q >= nspans) return;  // uniform over the warp
   SpanDev sp = spans[q];
   span_origin(sp, rb, sp.ox, sp.oy, sp.oz);
+  if (sp.end - sp.start > kReactExactSpan) return;  // uniform over the warp
   float f = 0.0f;  // lane a < 6: component a (force xyz, torque xyz)
-  if (sp.end - sp.start <= kReactExactSpan) {
+  {
     for (uint32_t b0 = sp.start; b0 < sp.end; b0 += 32) {
       const uint32_t kk = b0 + lane;
       if (kk < sp.end) {
@@ -2364,12 +2391,18 @@ __global__ void k_react_spans(const float* __restrict__ partial, const uint32_t*
       __syncwarp();
       if (lane < 6) {
         const uint32_t nb = min(32u, sp.end - b0);
-        for (uint32_t t = 0; t < nb; ++t) f = f + terms[w][lane][t];
+        if (nb == 32u) {  // the batch's terms loaded together, then added one by one
+          float v[32];
+#pragma unroll
+          for (int i = 0; i < 32; ++i) v[i] = terms[w][lane][i];
+#pragma unroll
+          for (int i = 0; i < 32; ++i) f = f + v[i];
+        } else {
+          for (uint32_t t = 0; t < nb; ++t) f = f + terms[w][lane][t];
+        }
       }
       __syncwarp();
     }
-  } else if (lane < 6) {
-    for (uint32_t c = chunk_first[q]; c < chunk_first[q + 1]; ++c) f = f + partial[6 * c + lane];
   }
   if (lane < 6) breact[6 * q + lane] = breact[6 * q + lane] + f;
 }

@@ -153,6 +153,12 @@ class Engine {
   cudaStream_t side_ = nullptr;
   cudaEvent_t ev_fork_ = nullptr, ev_join_ = nullptr;
   bool side_pending_ = false;
+  // per-body reaction sums: a third stream, forked after k_e_bforce and joined only where
+  // bforce / bpos / breact change (the next k_e_bforce, the tick's end, host reads)
+  cudaStream_t react_ = nullptr;
+  cudaEvent_t ev_rfork_ = nullptr, ev_rjoin_ = nullptr;
+  bool react_pending_ = false;
+  void join_side_only();
   uint64_t slot_cap_ = 0, cell_cap_ = 0, used_ = 0;
   uint32_t scene_cap_ = 0, nbr_cap_ = 64;
   uint64_t device_bytes_ = 0;
@@ -243,9 +249,6 @@ class Engine {
   SpanDev* spans_h_ = nullptr;  // pinned
   SpanChunk* chunks_d_ = nullptr;
   SpanChunk* chunks_h_ = nullptr;  // pinned
-  uint32_t* chunk_first_d_ = nullptr;
-  uint32_t* chunk_first_h_ = nullptr;  // pinned
-  float* react_partial_ = nullptr;
   float* breact_d_ = nullptr;
   float* breact_h_ = nullptr;  // pinned
   uint32_t nspans_ = 0, nchunks_ = 0, spans_cap_ = 0, chunks_cap_ = 0;

@@ -6,9 +6,8 @@ computes per particle: cell keys, the sort permutation and cell table
 (crates/vxl-phys-fluid/src/grid.rs:29-76), density, pressure, acceleration, XSPH,
 the per-boundary-particle reaction, and the integrated positions and velocities, over
 many substeps. Per-body reactions are summed in index order, like the reference's
-sequential loop (fluid_boundary.rs:10-28), for spans of up to 8,192 particles (bitwise
-equal), and by a fixed tree for larger ones (tank walls), which are compared within a
-stated tolerance (REACTION_RTOL, relative to the sum of |f_k|).
+sequential loop (fluid_boundary.rs:10-28), for every span (bodies and tank walls), and are
+compared bitwise.
 
 The reference's own golden values enter twice: the published CPU grid-table hashes
 are recomputed from tables the GPU built (test_published_hash_through_gpu), and the
@@ -23,8 +22,6 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 GOLDEN = json.loads((Path(__file__).parent / "golden" / "grid_hashes.json").read_text())
-REACTION_RTOL = 1e-5   # |F_gpu - F_cpu| <= REACTION_RTOL * sum_k |f_k| (per span, per axis)
-EXACT_SPAN = 8192      # spans up to this size are summed in index order: bitwise equal
 DENS_RTOL = 1e-5       # per-step tolerance of the f32 fluid step, used where bitwise is not claimed
 F32 = np.float32
 
@@ -125,8 +122,8 @@ def test_fp64_error_equal_for_gpu_and_oracle(vxl, oracle_mod):
 @pytest.mark.parametrize("ticks", [6])
 def test_multi_tick_bit_exact_with_reactions(vxl, oracle_mod, ticks):
     """Whole ticks (4 substeps each) with Akinci tank walls: positions and velocities
-    stay bitwise equal to the oracle tick after tick; per-body reactions are bitwise equal
-    for spans of up to 8,192 particles (summed in index order) and within tolerance above."""
+    stay bitwise equal to the oracle tick after tick; per-body reactions are bitwise equal,
+    the tank walls' spans above 8,192 particles (summed by a block each) included."""
     from vxl_sph import scenes
     spec = scenes.small_dam(n=(10, 12, 9), spacing=0.05, tank=(0.8, 0.7, 0.6))
     g, o = pair(vxl, oracle_mod, spec)
@@ -137,13 +134,8 @@ def test_multi_tick_bit_exact_with_reactions(vxl, oracle_mod, ticks):
         compare_state(g, o, f"tick {t}")
         ro = o.reactions()
         assert [x[0] for x in rg] == [x[0] for x in ro]
-        bf = np.abs(o.read()["bforce"][spec.n_fluid:])
         for (bid, fg, tg), (_, fo, to), (_, _, s0, s1) in zip(rg, ro, spec.spans):
-            if s1 - s0 <= EXACT_SPAN:
-                assert fg.tobytes() == fo.tobytes() and tg.tobytes() == to.tobytes(), (t, bid, fg, fo, tg, to)
-                continue
-            scale = bf[s0 - spec.n_fluid:s1 - spec.n_fluid].sum() + 1e-30
-            assert np.all(np.abs(fg - fo) <= REACTION_RTOL * scale + 1e-6), (t, bid, fg, fo)
+            assert fg.tobytes() == fo.tobytes() and tg.tobytes() == to.tobytes(), (t, bid, s1 - s0, fg, fo, tg, to)
     compare_grid(g, o, "final grid")
 
 
@@ -201,15 +193,21 @@ def test_dam0_ticks_bit_exact(vxl, oracle_mod):
 
 
 def test_dam1_full_size_one_tick_bit_exact(vxl, oracle_mod):
-    """1,000,000 fluid particles at full size: one tick (10 substeps) bitwise equal."""
+    """1,000,000 fluid particles at full size: one tick (10 substeps) bitwise equal, the
+    tank walls' per-body reactions (spans of 42,816-83,216 particles, a block each) too."""
     from vxl_sph import scenes
     spec = scenes.dam1()
+    assert max(e - s for _, _, s, e in spec.spans) > 8192
     g, o = pair(vxl, oracle_mod, spec, threads=16)
     dt_tick = float(F32(1) / F32(60))
-    g.step_tick(dt_tick, spec.spans)
+    rg = g.step_tick(dt_tick, spec.spans)
     o.step(dt_tick)
     compare_state(g, o, "dam1")
     compare_grid(g, o, "dam1")
+    ro = o.reactions()
+    assert [x[0] for x in rg] == [x[0] for x in ro]
+    for (bid, fg, tg), (_, fo, to) in zip(rg, ro):
+        assert fg.tobytes() == fo.tobytes() and tg.tobytes() == to.tobytes(), (bid, fg, fo, tg, to)
 
 
 # ---------------------------------------------------------------- edge cases
