@@ -207,10 +207,10 @@ void Engine::free_all() {
   graph_ = nullptr;
   void* d[] = {pos_[0], pos_[1], vel_[0], vel_[1], orig_, slot_of_, cellrank_, items_, rc_, press_, acc_, xsph_,
                bforce_, bpos_, nbr_, nbr_n_, halves_, xorder_, order_, segs_, stage_, counts_, wet_, start_, partial_, sc_d_, tiles_d_, ctl_d_, spans_d_,
-               chunks_d_, breact_d_};
+               longs_d_, breact_d_};
   for (void* p : d)
     if (p) cudaFree(p);
-  void* hp[] = {sc_h_, ctl_h_, spans_h_, chunks_h_, breact_h_};
+  void* hp[] = {sc_h_, ctl_h_, spans_h_, longs_h_, breact_h_};
   for (void* p : hp)
     if (p) cudaFreeHost(p);
   if (snap_h_) cudaFreeHost(snap_h_);
@@ -1250,7 +1250,7 @@ vxl_status Engine::stage_spans() {
   prof_collect();
   CU(cudaStreamSynchronize(stream_));
   std::vector<SpanDev> sp;
-  std::vector<SpanChunk> ch;
+  std::vector<LongSpan> ch;
   span_scene_.clear();
   for (uint32_t q = 0; q < scenes_.size() && q < spans_local_.size(); ++q)
     for (const vxl_sph_span& s : spans_local_[q]) {
@@ -1265,33 +1265,33 @@ vxl_status Engine::stage_spans() {
           }
       sp.push_back(SpanDev{s.body, s.origin[0], s.origin[1], s.origin[2], gs, ge, rigid});
       span_scene_.push_back(q);
-      if (ge - gs > kReactExactSpan) ch.push_back(SpanChunk{idx, gs, ge, 0u});  // a block of its own
+      if (ge - gs > kReactExactSpan) ch.push_back(LongSpan{idx, gs, ge, 0u});  // a block of its own
     }
   const uint32_t ns = (uint32_t)sp.size(), nc = (uint32_t)ch.size();
-  if (!spans_h_ || ns > spans_cap_ || nc > chunks_cap_) {
-    void* d[] = {spans_d_, chunks_d_, breact_d_};
+  if (!spans_h_ || ns > spans_cap_ || nc > longs_cap_) {
+    void* d[] = {spans_d_, longs_d_, breact_d_};
     for (void* p : d)
       if (p) cudaFree(p);
-    void* hp[] = {spans_h_, chunks_h_, breact_h_};
+    void* hp[] = {spans_h_, longs_h_, breact_h_};
     for (void* p : hp)
       if (p) cudaFreeHost(p);
-    spans_d_ = nullptr; chunks_d_ = nullptr; breact_d_ = nullptr;
-    spans_h_ = nullptr; chunks_h_ = nullptr; breact_h_ = nullptr;
+    spans_d_ = nullptr; longs_d_ = nullptr; breact_d_ = nullptr;
+    spans_h_ = nullptr; longs_h_ = nullptr; breact_h_ = nullptr;
     const uint32_t cap = std::max<uint32_t>(ns, 64), ccap = std::max<uint32_t>(nc, 256);
     vxl_status s;
     if ((s = dalloc(&spans_d_, cap)) != VXL_OK) return s;
-    if ((s = dalloc(&chunks_d_, ccap)) != VXL_OK) return s;
+    if ((s = dalloc(&longs_d_, ccap)) != VXL_OK) return s;
     if ((s = dalloc(&breact_d_, (size_t)cap * 6)) != VXL_OK) return s;
     CU(cudaMallocHost((void**)&spans_h_, cap * sizeof(SpanDev)));
-    CU(cudaMallocHost((void**)&chunks_h_, ccap * sizeof(SpanChunk)));
+    CU(cudaMallocHost((void**)&longs_h_, ccap * sizeof(LongSpan)));
     CU(cudaMallocHost((void**)&breact_h_, cap * 6 * sizeof(float)));
     spans_cap_ = cap;
-    chunks_cap_ = ccap;
+    longs_cap_ = ccap;
   }
   if (ns) std::memcpy(spans_h_, sp.data(), ns * sizeof(SpanDev));
-  if (nc) std::memcpy(chunks_h_, ch.data(), nc * sizeof(SpanChunk));
+  if (nc) std::memcpy(longs_h_, ch.data(), nc * sizeof(LongSpan));
   nspans_ = ns;
-  nchunks_ = nc;
+  nlongs_ = nc;
   spans_dirty_ = false;
   rb_dirty_ = true;              // the bodies' span indices follow the staging
   rb_have_reaction_ = false;     // reactions are indexed by the old staging
@@ -1488,10 +1488,10 @@ void Engine::enqueue_substep(bool with_reactions) {
     if (react) {
       cudaEventRecord(ev_rfork_, side_);
       cudaStreamWaitEvent(react_, ev_rfork_, 0);
-      if (nchunks_)  // the long spans (tank walls), a block each
+      if (nlongs_)  // the long spans (tank walls), a block each
         LAUNCH_ON(KID_REACT_LONG, react_,
-                  k_react_long<<<nchunks_, kReactThreads, 0, react_>>>((const float4*)bforce_, (const float4*)bpos_,
-                                                                       spans_d_, chunks_d_, rb_d_, ctl_d_, breact_d_));
+                  k_react_long<<<nlongs_, kReactThreads, 0, react_>>>((const float4*)bforce_, (const float4*)bpos_,
+                                                                       spans_d_, longs_d_, rb_d_, ctl_d_, breact_d_));
       LAUNCH_ON(KID_REACT_SPANS, react_,
                 k_react_spans<<<(nspans_ + kReactSpanWarps - 1) / kReactSpanWarps, 32 * kReactSpanWarps, 0, react_>>>(
                     (const float4*)bforce_, (const float4*)bpos_, spans_d_, rb_d_, ctl_d_, breact_d_, nspans_));
@@ -1533,7 +1533,7 @@ void Engine::enqueue_tick(float /*dt_tick*/) {
   const uint32_t sub = scenes_.empty() ? 1 : scenes_[0].substeps;
   if (nspans_ > 0) {
     cudaMemcpyAsync(spans_d_, spans_h_, nspans_ * sizeof(SpanDev), cudaMemcpyHostToDevice, st);
-    if (nchunks_) cudaMemcpyAsync(chunks_d_, chunks_h_, nchunks_ * sizeof(SpanChunk), cudaMemcpyHostToDevice, st);
+    if (nlongs_) cudaMemcpyAsync(longs_d_, longs_h_, nlongs_ * sizeof(LongSpan), cudaMemcpyHostToDevice, st);
     cudaMemsetAsync(breact_d_, 0, nspans_ * 6 * sizeof(float), st);
   }
   for (uint32_t s = 0; s < sub; ++s) enqueue_substep(true);

@@ -95,7 +95,7 @@ struct SpanDev {
   uint32_t rigid;  // coupled rigid body whose position is the torque origin (~0u: use ox, oy, oz)
 };
 
-struct SpanChunk {
+struct LongSpan {  // a span above kReactExactSpan, summed by a block of its own
   uint32_t span, begin, end, pad;
 };
 
@@ -2305,13 +2305,13 @@ __device__ __forceinline__ void span_origin(const SpanDev& sp, const RigidBodyDe
 __global__ void __launch_bounds__(kReactThreads) k_react_long(const float4* __restrict__ bforce,
                                                               const float4* __restrict__ bpos,
                                                               const SpanDev* __restrict__ spans,
-                                                              const SpanChunk* __restrict__ longs,
+                                                              const LongSpan* __restrict__ longs,
                                                               const RigidBodyDev* __restrict__ rb,
                                                               const EngineCtl* __restrict__ ctl,
                                                               float* __restrict__ breact) {
   if (ctl->err & kErrCellCap) return;
   __shared__ float terms[2][6][kReactBatch];
-  const SpanChunk ch = longs[blockIdx.x];
+  const LongSpan ch = longs[blockIdx.x];
   SpanDev sp = spans[ch.span];
   span_origin(sp, rb, sp.ox, sp.oy, sp.oz);
   auto stage = [&](uint32_t b0, uint32_t buf) {

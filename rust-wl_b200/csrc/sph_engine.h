@@ -20,7 +20,7 @@ struct SceneDev;
 struct TileDev;
 struct EngineCtl;
 struct SpanDev;
-struct SpanChunk;
+struct LongSpan;
 struct BodyPoseDev;
 struct RigidBodyDev;
 struct ProviderDev;
@@ -247,11 +247,11 @@ class Engine {
   std::vector<std::vector<vxl_sph_span>> spans_local_;
   SpanDev* spans_d_ = nullptr;
   SpanDev* spans_h_ = nullptr;  // pinned
-  SpanChunk* chunks_d_ = nullptr;
-  SpanChunk* chunks_h_ = nullptr;  // pinned
+  LongSpan* longs_d_ = nullptr;
+  LongSpan* longs_h_ = nullptr;  // pinned
   float* breact_d_ = nullptr;
   float* breact_h_ = nullptr;  // pinned
-  uint32_t nspans_ = 0, nchunks_ = 0, spans_cap_ = 0, chunks_cap_ = 0;
+  uint32_t nspans_ = 0, nlongs_ = 0, spans_cap_ = 0, longs_cap_ = 0;
   bool spans_dirty_ = true;
   std::vector<uint32_t> span_scene_;  // scene of each global span (for the results)
 
