@@ -434,9 +434,10 @@ def run_ours(args) -> None:
                             "ms": total_ms / (args.steps * sub)},
                 "profiled_ms_per_tick": sum(prof_step_ms) / args.steps,
                 "timing": "kernel times from a second pass over the same ticks with an event pair around "
-                          "every launch; value from the pass without them. k_bforce and k_react_* run on a "
-                          "second stream beside k_force: their spans include waiting for SMs, so they are "
-                          "listed apart (side_stream_spans_ms_per_substep) and are not costs",
+                          "every launch; value from the pass without them. k_bforce runs on a second stream "
+                          "beside k_force and k_react_* on a third beside the next substep's passes: their "
+                          "spans include waiting for SMs, so they are listed apart "
+                          "(side_stream_spans_ms_per_substep) and are not costs",
                 "kernels_ms_per_substep": {k: v[0] / max(args.steps * sub, 1) for k, v in sorted(prof.items())
                                            if k not in SIDE_STREAM},
                 "side_stream_spans_ms_per_substep": {k: v[0] / max(args.steps * sub, 1)
