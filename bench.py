@@ -79,6 +79,21 @@ def ncu_traffic(kernel: str, workload: str):
     return None
 
 
+def ncu_issue(kernel: str, workload: str):
+    """Issue-slot use of `kernel` on `workload` from the committed ncu summary: the resource
+    that binds the neighbour passes (their DRAM throughput stays below 10%)."""
+    p = ROOT / "profiles" / "roofline_issue.txt"
+    try:
+        for line in p.read_text().splitlines():
+            f = line.split()
+            if len(f) >= 5 and not line.startswith("#") and f[0] == kernel and f[1] == workload:
+                return {"issue_active": float(f[2]), "threads_per_instruction": float(f[3]),
+                        "source": "profiles/" + f[4]}
+    except OSError:
+        pass
+    return None
+
+
 def hbm_peak() -> tuple[float, str]:
     p = ROOT / "MEASURED_PEAKS.json"
     try:
@@ -426,6 +441,7 @@ def run_ours(args) -> None:
     roofline = {"kernel": dom_name, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": (achieved / peak) if achieved else None,
                 "traffic": ncu_traffic(dom_name, spec.name),
+                "issue": ncu_issue(dom_name, spec.name),
                 "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
                 else "fallback 6650 GB/s",
                 "avg_launch_ms": avg_ms, "launches": dom_n, "share": dom_ms / prof_total if prof_total else None,
