@@ -75,3 +75,22 @@ def test_gpus_flag_launches_ranks():
     assert r.returncode == 0, r.stderr[-2000:]
     lines = [json.loads(x) for x in r.stdout.splitlines() if x.startswith("{")]
     assert len(lines) == 1 and lines[0]["n_gpus"] == 2 and lines[0]["impl"] == "reference"
+
+
+def test_roofline_tables_point_at_committed_summaries():
+    """roofline.traffic and roofline.issue come from committed ncu summaries: every row of
+    the two tables parses and names a summary under profiles/, and the headline workload's
+    dominant kernel has both figures."""
+    sys.path.insert(0, str(ROOT))
+    import bench
+    for name, ncols in (("roofline_traffic.txt", 4), ("roofline_issue.txt", 5)):
+        rows = [l.split() for l in (ROOT / "profiles" / name).read_text().splitlines()
+                if l.strip() and not l.startswith("#")]
+        assert rows, name
+        for f in rows:
+            assert len(f) == ncols, (name, f)
+            float(f[2])
+            assert (ROOT / "profiles" / f[-1]).is_file(), (name, f[-1])
+    assert bench.ncu_traffic("k_density", "dam10m") > 0
+    issue = bench.ncu_issue("k_density", "dam10m")
+    assert 0.0 < issue["issue_active"] <= 1.0 and 0.0 < issue["threads_per_instruction"] <= 32.0
